@@ -1,0 +1,465 @@
+"""Input generator for the NRG step: writes the `param` and `data` (version 9)
+files that the reference's C++ back end reads.
+
+The reference produces `data` with its Mathematica front end (initial.m,
+maketable at initial.m:4309-4392), which is not available here.  This module
+restates the parts of that front end that the QS (charge U(1) x spin SU(2))
+workloads need:
+
+* the Wilson chain of a flat band in the Yoshida-Whitaker-Oliveira (Y)
+  discretization, by Lanczos tridiagonalisation of the star Hamiltonian in
+  arbitrary precision (initial.m:2902-2908 band, 3538-3545 Y energies,
+  3055-3164 Lanczos recursion, 4040-4044 table output);
+* the initial cluster (impurity + site f_0 of every channel): Fock-space
+  Hamiltonian, its eigenstates per invariant subspace (Q, SS) with the
+  representative member at S_z = S (initial.m:1664-1668), energies shifted by
+  the ground state and divided by SCALE(0) (initial.m:4104-4124);
+* irreducible matrix elements in the Wigner-Eckart normalisation of
+  initial.m:2089-2104:  <I1||O||I2> = <I1,S1|O_sigma|I2,S2> / CG(S2 S2; 1/2 sigma | S1 S1);
+* the data-file layout of initial.m:4094-4101 (header), 4309-4392 (blocks)
+  and the reader at src/nrg.cc:3323-3401, src/read-input.cc:98-143.
+
+Models: single-impurity Anderson (models.m SIAM variant) and the 1- or
+2-channel Kondo model (models.m:366-377).  Hybridisation and exchange are
+taken literally as given by the caller (V, J); the A_Lambda correction of
+initial.m:1023 is not applied unless the caller folds it into V or J.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+try:
+    import mpmath
+except ImportError:  # pragma: no cover - mpmath ships with the image
+    mpmath = None
+
+
+# ---------------------------------------------------------------------------
+# Wilson chain
+# ---------------------------------------------------------------------------
+
+def scale_factor(N: int, Lambda: float, z: float = 1.0, discretization: str = "Y",
+                 bandrescale: float = 1.0) -> float:
+    """SCALE(N) of src/nrg.cc:491-506 (no substeps)."""
+    if discretization == "Y":
+        s = 0.5 * (1.0 + 1.0 / Lambda)
+    elif discretization in ("C", "Z"):
+        s = (1.0 - 1.0 / Lambda) / math.log(Lambda)
+    else:
+        raise ValueError("unknown discretization " + discretization)
+    return s * Lambda ** (-(N - 1) / 2.0 + 1.0 - z) * bandrescale
+
+
+def wilson_chain_flat(Lambda: float, z: float, Nmax: int, mMAX: int | None = None,
+                      dps: int = 200) -> Tuple[np.ndarray, np.ndarray]:
+    """Chain coefficients xi[0..Nmax], zeta[0..Nmax] of a flat band (D=1) in the
+    Y discretization.
+
+    Star levels (initial.m:2902-2908, 3538-3545): interval edges eps_0 = 1,
+    eps_m = Lambda^(1-z-m); hybridisation weights df_m = eps_m - eps_{m+1}
+    (theta = 2, symmetric); representative energies de_0 = (1+Lambda^-z)/2,
+    de_m = (1+1/Lambda)/2 * Lambda^(1-z-m).  mMAX defaults to
+    max(80, 2*Nmax) as in initial.m:2877.  The Lanczos recursion runs at `dps`
+    decimal digits, since double precision loses orthogonality along the
+    chain (the reference uses 1000 digits, initial.m:2790-2793).
+    """
+    if mpmath is None:
+        raise RuntimeError("mpmath is required for the Wilson chain")
+    if mMAX is None:
+        mMAX = max(80, 2 * Nmax)
+    mp = mpmath.mp
+    old = mp.dps
+    mp.dps = dps
+    try:
+        L = mpmath.mpf(Lambda)
+        Z = mpmath.mpf(z)
+        eps = [mpmath.mpf(1)] + [L ** (1 - Z - m) for m in range(1, mMAX + 2)]
+        df = [eps[m] - eps[m + 1] for m in range(mMAX + 1)]
+        de = [(1 + L ** (-Z)) / 2] + [(1 + 1 / L) / 2 * L ** (1 - Z - m) for m in range(1, mMAX + 1)]
+        theta = mpmath.mpf(2)
+        # Diagonal star Hamiltonian A = diag(+de, -de) with start vector u0.
+        diagA = de + [-x for x in de]
+        u = [mpmath.sqrt(x / theta) for x in df] * 2
+        norm = mpmath.fsum(x * x for x in u)
+        u = [x / mpmath.sqrt(norm) for x in u]  # rescale exactly to one
+        xi, zeta = [], []
+        uprev = [mpmath.mpf(0)] * len(u)
+        xiprev = mpmath.mpf(0)
+        for n in range(Nmax + 1):
+            Au = [a * x for a, x in zip(diagA, u)]
+            zn = mpmath.fsum(a * x for a, x in zip(Au, u))
+            r = [a - zn * x - xiprev * p for a, x, p in zip(Au, u, uprev)]
+            # one step of reorthogonalisation against the previous vectors is
+            # unnecessary at this precision; renormalise as initial.m:3450-3458.
+            xn = mpmath.sqrt(mpmath.fsum(x * x for x in r))
+            zeta.append(zn)
+            xi.append(xn)
+            uprev, u = u, [x / xn for x in r]
+            xiprev = xn
+        return (np.array([float(x) for x in xi]), np.array([float(x) for x in zeta]))
+    finally:
+        mp.dps = old
+
+
+def wilson_closed_form(Lambda: float, Nmax: int) -> np.ndarray:
+    """Wilson's closed form for xi_n (flat band, z=1, infinite star), used as
+    a cross-check of the Lanczos result."""
+    n = np.arange(Nmax + 1, dtype=float)
+    L = Lambda
+    return ((1 + 1 / L) / 2 * (1 - L ** (-n - 1))
+            / np.sqrt((1 - L ** (-2 * n - 1)) * (1 - L ** (-2 * n - 3))) * L ** (-n / 2))
+
+
+# ---------------------------------------------------------------------------
+# Fock space of the initial cluster
+# ---------------------------------------------------------------------------
+
+class Fock:
+    """Dense Fock space of `nmodes` fermionic modes, Jordan-Wigner ordered.
+
+    Mode k is (orbital, spin) with spin 0 = up, 1 = down.  cdag[k] is the
+    creation-operator matrix (2^n x 2^n)."""
+
+    def __init__(self, norb: int):
+        self.norb = norb
+        self.nmodes = 2 * norb
+        dim = 1 << self.nmodes
+        self.dim = dim
+        self.cdag = []
+        states = np.arange(dim)
+        for k in range(self.nmodes):
+            M = np.zeros((dim, dim))
+            for s in states:
+                if not (s >> k) & 1:
+                    t = s | (1 << k)
+                    # sign: number of occupied modes below k
+                    sign = -1.0 if bin(s & ((1 << k) - 1)).count("1") % 2 else 1.0
+                    M[t, s] = sign
+            self.cdag.append(M)
+        self.occ = np.array([[(s >> k) & 1 for k in range(self.nmodes)] for s in states])
+
+    def mode(self, orb: int, spin: int) -> int:
+        return 2 * orb + spin
+
+    def c(self, orb, spin):
+        return self.cdag[self.mode(orb, spin)].T
+
+    def cd(self, orb, spin):
+        return self.cdag[self.mode(orb, spin)]
+
+    def n(self, orb, spin=None):
+        if spin is None:
+            return self.n(orb, 0) + self.n(orb, 1)
+        m = self.cdag[self.mode(orb, spin)]
+        return m @ m.T
+
+    def spin_ops(self, orb):
+        sp = self.cd(orb, 0) @ self.c(orb, 1)
+        sz = 0.5 * (self.n(orb, 0) - self.n(orb, 1))
+        return sp, sp.T, sz
+
+
+@dataclass
+class Subspace:
+    Q: int
+    SS: int
+    energies: np.ndarray            # ascending, absolute units
+    vectors: np.ndarray             # (fock_dim, nstates), representative S_z = S
+
+
+@dataclass
+class ClusterModel:
+    """Initial cluster: Hamiltonian, operators and the site-0 f operators."""
+    fock: Fock
+    H: np.ndarray
+    charge_orbitals: List[int]      # orbitals whose occupancy defines Q
+    f_orbitals: List[int]           # orbital of f_0 for each channel
+    spin_orbitals: List[int]        # orbitals that carry spin
+    basis_mask: np.ndarray          # Fock states that are allowed
+    doublet_ops: Dict[str, int] = field(default_factory=dict)   # name -> orbital (creation op)
+    singlet_ops: Dict[str, np.ndarray] = field(default_factory=dict)
+    triplet_ops: Dict[str, int] = field(default_factory=dict)   # name -> orbital (spin op)
+
+
+def siam_cluster(U: float, eps_d: float, V: float, zeta0: float = 0.0) -> ClusterModel:
+    """Single-impurity Anderson model, impurity d + first chain site f_0:
+    H = eps_d n_d + U n_up n_dn + V sum_s (d^dag_s f_0s + h.c.) + zeta0 (n_f0 - 1)."""
+    F = Fock(2)  # orbital 0 = d, orbital 1 = f0
+    H = eps_d * F.n(0) + U * F.n(0, 0) @ F.n(0, 1)
+    for s in (0, 1):
+        hop = F.cd(0, s) @ F.c(1, s)
+        H = H + V * (hop + hop.T)
+    H = H + zeta0 * (F.n(1) - np.eye(F.dim))
+    m = ClusterModel(F, H, charge_orbitals=[0, 1], f_orbitals=[1], spin_orbitals=[0, 1],
+                     basis_mask=np.ones(F.dim, dtype=bool))
+    m.doublet_ops["A_d"] = 0
+    m.singlet_ops["n_d"] = F.n(0)
+    m.singlet_ops["n_d^2"] = F.n(0) @ F.n(0)
+    m.triplet_ops["SZd"] = 0
+    return m
+
+
+def kondo_cluster(J: List[float]) -> ClusterModel:
+    """Kondo model with len(J) channels: impurity spin (orbital 0, singly
+    occupied) coupled to f_0 of each channel, H = sum_ch J_ch S_d . s_ch
+    (models.m:366-377 for two channels)."""
+    nch = len(J)
+    F = Fock(1 + nch)
+    H = np.zeros((F.dim, F.dim))
+    spd, smd, szd = F.spin_ops(0)
+    for ch in range(nch):
+        sp, sm, sz = F.spin_ops(1 + ch)
+        H = H + J[ch] * (szd @ sz + 0.5 * (spd @ sm + smd @ sp))
+    mask = F.occ[:, 0] + F.occ[:, 1] == 1
+    m = ClusterModel(F, H, charge_orbitals=list(range(1, 1 + nch)),
+                     f_orbitals=list(range(1, 1 + nch)),
+                     spin_orbitals=list(range(1 + nch)), basis_mask=mask)
+    for ch in range(nch):
+        m.doublet_ops["A_f%d" % ch] = 1 + ch
+    m.triplet_ops["SZd"] = 0
+    return m
+
+
+def _total_spin_ops(m: ClusterModel):
+    F = m.fock
+    Sp = np.zeros((F.dim, F.dim))
+    Sz = np.zeros((F.dim, F.dim))
+    for o in m.spin_orbitals:
+        sp, sm, sz = F.spin_ops(o)
+        Sp = Sp + sp
+        Sz = Sz + sz
+    return Sp, Sz
+
+
+def cg_half(S2: float, S1: float) -> float:
+    """Clebsch-Gordan <S2 S2; 1/2 (S1-S2) | S1 S1> (Condon-Shortley)."""
+    if abs(S1 - (S2 + 0.5)) < 1e-12:
+        return 1.0
+    if abs(S1 - (S2 - 0.5)) < 1e-12:
+        return math.sqrt(2 * S2 / (2 * S2 + 1))
+    raise ValueError("not a doublet coupling")
+
+
+def cg_one(S2: float, S1: float) -> float:
+    """<S2 S2; 1 (S1-S2) | S1 S1> for a rank-1 (triplet) operator."""
+    q = S1 - S2
+    if abs(q - 1) < 1e-12:
+        return 1.0
+    if abs(q) < 1e-12:
+        return math.sqrt(S2 / (S2 + 1)) if S2 > 0 else 0.0
+    if abs(q + 1) < 1e-12:
+        return math.sqrt(S2 * (2 * S2 - 1) / ((S2 + 1) * (2 * S2 + 1))) if S2 > 0.5 else 0.0
+    raise ValueError("not a triplet coupling")
+
+
+def decompose(m: ClusterModel, tol: float = 1e-9) -> List[Subspace]:
+    """Eigenstates per invariant subspace (Q, SS); representative S_z = S."""
+    F = m.fock
+    Sp, Sz = _total_spin_ops(m)
+    ncharge = F.occ[:, [2 * o for o in m.charge_orbitals]].sum(1) + \
+        F.occ[:, [2 * o + 1 for o in m.charge_orbitals]].sum(1)
+    Q = ncharge - len(m.charge_orbitals)
+    sz = np.round(np.diag(Sz) * 2).astype(int)  # 2*S_z
+    subs = []
+    for q in sorted(set(Q[m.basis_mask])):
+        for two_s in sorted(set(sz[(Q == q) & m.basis_mask])):
+            if two_s < 0:
+                continue
+            idx = np.where((Q == q) & (sz == two_s) & m.basis_mask)[0]
+            idx_up = np.where((Q == q) & (sz == two_s + 2) & m.basis_mask)[0]
+            if len(idx_up):
+                A = Sp[np.ix_(idx_up, idx)]
+                # null space of S+ within this sector: highest-weight states
+                u, s, vt = np.linalg.svd(A)
+                rank = int((s > tol).sum())
+                B = vt[rank:].T
+            else:
+                B = np.eye(len(idx))
+            if B.shape[1] == 0:
+                continue
+            Hs = B.T @ m.H[np.ix_(idx, idx)] @ B
+            Hs = 0.5 * (Hs + Hs.T)
+            e, w = np.linalg.eigh(Hs)
+            vec = np.zeros((F.dim, B.shape[1]))
+            vec[idx] = B @ w
+            subs.append(Subspace(int(q), int(two_s + 1), e, vec))
+    return subs
+
+
+def _sub_map(subs):
+    return {(s.Q, s.SS): s for s in subs}
+
+
+def reduced_doublet(m: ClusterModel, subs, orb: int):
+    """<I1||a^dag||I2> for pairs with Q1 = Q2+1, |SS1-SS2| = 1 (ireducMatrixSpeedy, QS)."""
+    F = m.fock
+    smap = _sub_map(subs)
+    out = {}
+    for (q2, ss2), s2 in smap.items():
+        for ss1 in (ss2 + 1, ss2 - 1):
+            key1 = (q2 + 1, ss1)
+            if ss1 < 1 or key1 not in smap:
+                continue
+            s1 = smap[key1]
+            S1, S2 = (ss1 - 1) / 2, (ss2 - 1) / 2
+            spin = 0 if S1 > S2 else 1  # sigma = S1 - S2
+            op = F.cd(orb, spin)
+            M = s1.vectors.T @ op @ s2.vectors / cg_half(S2, S1)
+            out[(key1, (q2, ss2))] = M
+    return out
+
+
+def reduced_singlet(m: ClusterModel, subs, op: np.ndarray):
+    smap = _sub_map(subs)
+    out = {}
+    for key, s in smap.items():
+        out[(key, key)] = s.vectors.T @ op @ s.vectors
+    return out
+
+
+def reduced_triplet(m: ClusterModel, subs, orb: int):
+    """<I1||S||I2> for a spin-1 operator, pairs with equal Q and
+    SS1 - SS2 in {0, +-2}; spherical components S_{+1} = -S+/sqrt2, S_0 = Sz,
+    S_{-1} = S-/sqrt2 (initial.m:2549-2570)."""
+    F = m.fock
+    sp, sm, sz = F.spin_ops(orb)
+    smap = _sub_map(subs)
+    out = {}
+    for (q2, ss2), s2 in smap.items():
+        for ss1 in (ss2 + 2, ss2, ss2 - 2):
+            key1 = (q2, ss1)
+            if ss1 < 1 or key1 not in smap:
+                continue
+            S1, S2 = (ss1 - 1) / 2, (ss2 - 1) / 2
+            q = S1 - S2
+            op = {1: -sp / math.sqrt(2), 0: sz, -1: sm / math.sqrt(2)}[int(round(q))]
+            cg = cg_one(S2, S1)
+            if cg == 0.0:
+                continue
+            out[(key1, (q2, ss2))] = smap[key1].vectors.T @ op @ s2.vectors / cg
+    return out
+
+
+# ---------------------------------------------------------------------------
+# data / param writers
+# ---------------------------------------------------------------------------
+
+def _fmt(x: float) -> str:
+    return repr(float(x))
+
+
+def _write_matrix(lines, M):
+    for row in np.atleast_2d(M):
+        lines.append(" ".join(_fmt(v) for v in row))
+
+
+def write_data(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: int,
+               xi: np.ndarray, zeta: np.ndarray, nchannels: int,
+               discretization: str = "Y") -> dict:
+    """Write a version-9 `data` file; returns a summary dict."""
+    subs = decompose(m)
+    gs = min(s.energies[0] for s in subs)
+    sc0 = scale_factor(0, Lambda, z, discretization)
+    lines = ["# Input file for NRG Ljubljana (generated by inputgen.py)",
+             "# symtype QS",
+             "#!9",
+             "# Number of channels, chain sites, subspaces: ",
+             "%d %d %d" % (nchannels, Nmax, len(subs)),
+             "# SCALE " + _fmt(sc0),
+             "# Energies (GS energy subtracted, multiplied by 1/SCALE):"]
+    for s in subs:
+        lines.append("%d %d" % (s.Q, s.SS))
+        lines.append("%d" % len(s.energies))
+        lines.append(" ".join(_fmt((e - gs) / sc0) for e in s.energies))
+    lines.append("# Irreducible matrix elements for Wilson chains:")
+    for ch in range(nchannels):
+        f = reduced_doublet(m, subs, m.f_orbitals[ch])
+        lines.append("f %d 0" % ch)
+        lines.append("%d" % len(f))
+        for (k1, k2), M in f.items():
+            lines.append("%d %d %d %d" % (k1[0], k1[1], k2[0], k2[1]))
+            _write_matrix(lines, M)
+    lines.append("# GS energy in absolute units:")
+    lines.append("e")
+    lines.append(_fmt(gs))
+    lines.append("# Irreducible matrix elements for other operators:")
+    for name, op in m.singlet_ops.items():
+        blocks = reduced_singlet(m, subs, op)
+        lines.append("s" + name)
+        lines.append("%d" % len(blocks))
+        for (k1, k2), M in blocks.items():
+            lines.append("%d %d %d %d" % (k1[0], k1[1], k2[0], k2[1]))
+            _write_matrix(lines, M)
+    for name, orb in m.doublet_ops.items():
+        blocks = reduced_doublet(m, subs, orb)
+        lines.append("d" + name)
+        lines.append("%d" % len(blocks))
+        for (k1, k2), M in blocks.items():
+            lines.append("%d %d %d %d" % (k1[0], k1[1], k2[0], k2[1]))
+            _write_matrix(lines, M)
+    for name, orb in m.triplet_ops.items():
+        blocks = reduced_triplet(m, subs, orb)
+        lines.append("t" + name)
+        lines.append("%d" % len(blocks))
+        for (k1, k2), M in blocks.items():
+            lines.append("%d %d %d %d" % (k1[0], k1[1], k2[0], k2[1]))
+            _write_matrix(lines, M)
+    lines.append("# Discretization tables:")
+    lines.append("z")
+    for ch in range(nchannels):
+        lines.append("%d" % (len(xi) - 1))
+        lines.extend(_fmt(x) for x in xi)
+    for ch in range(nchannels):
+        lines.append("%d" % (len(zeta) - 1))
+        lines.extend(_fmt(x) for x in zeta)
+    lines.append("")
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines))
+    return {"subspaces": len(subs), "gs_energy": gs, "scale0": sc0}
+
+
+def write_param(path: str, params: Dict[str, object]) -> None:
+    with open(path, "w") as fh:
+        fh.write("[param]\n")
+        for k, v in params.items():
+            if isinstance(v, bool):
+                v = "true" if v else "false"
+            fh.write("%s=%s\n" % (k, v))
+
+
+def make_siam(dirpath: str, U: float, eps_d: float, Gamma: float, Lambda: float,
+              Nmax: int, z: float = 1.0, params: Dict[str, object] | None = None,
+              V: float | None = None, dps: int = 200) -> dict:
+    """Generate `data` and `param` for a QS single-impurity Anderson model on a
+    flat band (D=1) in directory `dirpath`.  V defaults to sqrt(2 Gamma/pi)."""
+    os.makedirs(dirpath, exist_ok=True)
+    if V is None:
+        V = math.sqrt(2.0 * Gamma / math.pi)
+    xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps)
+    m = siam_cluster(U, eps_d, V, zeta0=zeta[0])
+    info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, 1)
+    p = {"Lambda": Lambda, "z": z, "discretization": "Y"}
+    if params:
+        p.update(params)
+    write_param(os.path.join(dirpath, "param"), p)
+    info.update({"V": V, "xi": xi, "zeta": zeta})
+    return info
+
+
+def make_kondo(dirpath: str, J: List[float], Lambda: float, Nmax: int, z: float = 1.0,
+               params: Dict[str, object] | None = None, dps: int = 200) -> dict:
+    os.makedirs(dirpath, exist_ok=True)
+    xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps)
+    m = kondo_cluster(J)
+    info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, len(J))
+    p = {"Lambda": Lambda, "z": z, "discretization": "Y"}
+    if params:
+        p.update(params)
+    write_param(os.path.join(dirpath, "param"), p)
+    info.update({"xi": xi, "zeta": zeta})
+    return info

@@ -1,0 +1,146 @@
+"""Known-answer tests that pin the oracle (and the input generator) where the
+reference has no regression tests for the NRG step: Wilson's closed-form
+chain, exact diagonalisation of short chains, the FDM sum rule and the
+density-matrix trace invariants of src/nrg.cc:1176-1181, src/dmnrg.h:588-592."""
+import math
+
+import numpy as np
+import pytest
+
+import inputgen as g
+import nrg_oracle as O
+
+
+def test_wilson_chain_closed_form():
+    xi, zeta = g.wilson_chain_flat(2.0, 1.0, 30)
+    ref = g.wilson_closed_form(2.0, 30)
+    assert np.max(np.abs(xi / ref - 1)) < 1e-14
+    assert np.max(np.abs(zeta)) < 1e-15
+    xi3, _ = g.wilson_chain_flat(3.0, 1.0, 20)
+    assert np.max(np.abs(xi3 / g.wilson_closed_form(3.0, 20) - 1)) < 1e-14
+
+
+def test_wilson_chain_precision_converged():
+    a, _ = g.wilson_chain_flat(2.0, 0.625, 40, dps=150)
+    b, _ = g.wilson_chain_flat(2.0, 0.625, 40, dps=300)
+    assert np.max(np.abs(a / b - 1)) < 1e-15
+
+
+def _chain_H(F, xi, N, first_site=1):
+    H = np.zeros((F.dim, F.dim))
+    for n in range(0, N + 1):
+        for s in (0, 1):
+            h = F.cd(first_site + n, s) @ F.c(first_site + n + 1, s)
+            H += xi[n] * (h + h.T)
+    return H
+
+
+def _nrg_levels(rec):
+    return np.sort(np.concatenate([np.repeat(e.value, I[1]) for I, e in rec.eig.items()]))
+
+
+@pytest.mark.parametrize("U,eps", [(0.3, -0.1), (0.1, -0.05), (0.0, 0.02)])
+def test_siam_energies_match_exact_diagonalisation(tmp_path, U, eps):
+    info = g.make_siam(str(tmp_path), U, eps, 0.05, 2.0, Nmax=3, params={"keep": 100000})
+    o = O.Oracle(str(tmp_path))
+    o.setup()
+    o.sweep1()
+    for N in range(3):
+        F = g.Fock(N + 3)
+        H = eps * F.n(0) + U * F.n(0, 0) @ F.n(0, 1)
+        for s in (0, 1):
+            h = F.cd(0, s) @ F.c(1, s)
+            H += info["V"] * (h + h.T)
+        H += _chain_H(F, info["xi"], N)
+        ev = np.linalg.eigvalsh(H) / O.SCALE(o.P, N + 1)
+        ev -= ev.min()
+        assert np.max(np.abs(np.sort(ev) - _nrg_levels(o.steps[N]))) < 1e-12
+
+
+def test_kondo_energies_match_exact_diagonalisation(tmp_path):
+    J = 0.4
+    info = g.make_kondo(str(tmp_path), [J], 2.5, Nmax=3, params={"keep": 100000})
+    o = O.Oracle(str(tmp_path))
+    o.setup()
+    o.sweep1()
+    for N in range(2):
+        F = g.Fock(N + 3)
+        spd, smd, szd = F.spin_ops(0)
+        sp, sm, sz = F.spin_ops(1)
+        H = J * (szd @ sz + 0.5 * (spd @ sm + smd @ sp)) + _chain_H(F, info["xi"], N)
+        mask = (F.occ[:, 0] + F.occ[:, 1]) == 1
+        ev = np.linalg.eigvalsh(H[np.ix_(mask, mask)]) / O.SCALE(o.P, N + 1)
+        ev -= ev.min()
+        assert np.max(np.abs(np.sort(ev) - _nrg_levels(o.steps[N]))) < 1e-12
+
+
+def test_doublet_recalculation_matches_exact_diagonalisation(tmp_path):
+    U, eps, Gam = 0.3, -0.1, 0.05
+    info = g.make_siam(str(tmp_path), U, eps, Gam, 2.0, Nmax=3,
+                       params={"keep": 100000, "specd": "A_d-A_d"})
+    o = O.Oracle(str(tmp_path))
+    o.setup()
+    o.sweep1()
+    N = 2
+    F = g.Fock(N + 3)
+    H = eps * F.n(0) + U * F.n(0, 0) @ F.n(0, 1)
+    for s in (0, 1):
+        h = F.cd(0, s) @ F.c(1, s)
+        H += info["V"] * (h + h.T)
+    H += _chain_H(F, info["xi"], N)
+    m = g.ClusterModel(F, H, charge_orbitals=list(range(N + 3)), f_orbitals=[N + 2],
+                       spin_orbitals=list(range(N + 3)), basis_mask=np.ones(F.dim, bool))
+    subs = g.decompose(m)
+    red = g.reduced_doublet(m, subs, 0)
+    sc = O.SCALE(o.P, N + 1)
+    E = {(s.Q, s.SS): s.energies / sc for s in subs}
+    gs = min(v.min() for v in E.values())
+    E = {k: v - gs for k, v in E.items()}
+
+    def moments(blocks, En):
+        out = []
+        for a in (0.0, 0.5, 2.0):
+            for k in (0, 1, 2):
+                t = 0.0
+                for (I1, I2), M in blocks.items():
+                    e1 = En[I1][:M.shape[0]]
+                    e2 = En[I2][:M.shape[1]]
+                    t += np.sum(M ** 2 * np.exp(-a * (e1[:, None] + e2[None, :]))
+                                * (e1[:, None] - e2[None, :]) ** k)
+                out.append(t)
+        return np.array(out)
+
+    ref = moments(red, E)
+    got = moments(o.final_ops["d"]["A_d"], {I: e.value for I, e in o.steps[N].eig.items()})
+    assert np.max(np.abs(ref - got) / np.abs(ref)) < 1e-12
+
+
+def test_fdm_sum_rule_with_truncation(tmp_path):
+    g.make_siam(str(tmp_path), 0.2, -0.1, 0.04, 2.0, Nmax=10,
+                params={"keep": 60, "specd": "A_d-A_d", "fdm": True, "T": 1e-3, "bins": 20,
+                        "broaden": False})
+    o = O.Oracle(str(tmp_path))
+    o.run()
+    sp = o.spectra[0]
+    assert abs(sp.pos.w.sum() + sp.neg.w.sum() - 1.0) < 1e-10
+    assert abs(o.wn.sum() - 1.0) < 1e-12
+
+
+def test_dmnrg_density_matrix_traces_and_fdm_agreement(tmp_path):
+    g.make_siam(str(tmp_path), 0.2, -0.1, 0.04, 2.0, Nmax=22,
+                params={"keep": 300, "specd": "A_d-A_d", "dmnrg": True, "fdm": True,
+                        "T": 1e-6, "bins": 10, "broaden": False})
+    o = O.Oracle(str(tmp_path))
+    o.run()
+    for N, rho in o.rho.items():
+        assert abs(o.trace(rho) - 1.0) < 1e-12
+    dm, fdm = o.spectra
+    assert dm.spectype == "DMNRG" and fdm.spectype == "FDM"
+    # FDM satisfies the sum rule exactly; DM-NRG with N/N+2 patching only
+    # approximately, and the two agree decade by decade above the last window.
+    assert abs(fdm.pos.w.sum() + fdm.neg.w.sum() - 1.0) < 1e-10
+    assert abs(dm.pos.w.sum() + dm.neg.w.sum() - 1.0) < 0.05
+    wd = dm.pos.w + dm.neg.w
+    wf = fdm.pos.w + fdm.neg.w
+    for i in range(30, len(wd), 10):
+        assert abs(wd[i:i + 10].sum() - wf[i:i + 10].sum()) < 0.02
