@@ -1,0 +1,86 @@
+/* nrgb.h - C ABI of the B200 NRG step library (libnrgb.so).
+ *
+ * Plain pointers and sizes only.  All matrices are column-major FP64.
+ * Every function returns 0 on success or a nonzero status; the message of the
+ * last failure on a context is available from nrgb_last_error().  The
+ * library never calls exit(); a caller that wants the reference's behaviour
+ * on LAPACK failure (src/portabil.h:130-140 my_error -> exit(1)) maps a
+ * nonzero status to its own error path.
+ *
+ * Seams of the reference that these entry points replace:
+ *   nrgb_syev_batched      dsyev_('V','L',...) per invariant subspace
+ *                          (src/diag.h:9-10, 54-89; called per block from
+ *                          src/nrg.cc:2484-2507), here for a whole step at once.
+ *   nrgb_gemm_grouped_dev  atlas::gemm / cblas dgemm calls of the operator
+ *                          recalculation and density-matrix updates
+ *                          (src/recalc.cc:90-91, 268-272; src/dmnrg.h:382-387).
+ *   nrgb_run               the `nrg` executable's main program for the NRG
+ *                          iteration (src/nrg.cc:3429-3469 start_calculation):
+ *                          reads `param` and `data`, writes `td`, spectra.
+ */
+#ifndef NRGB_H
+#define NRGB_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct nrgb_ctx nrgb_ctx;
+
+/* Context bound to one CUDA device; owns all device memory it allocates. */
+int nrgb_create(int device, nrgb_ctx** out);
+int nrgb_destroy(nrgb_ctx* ctx);
+const char* nrgb_last_error(const nrgb_ctx* ctx);
+const char* nrgb_version(void);
+
+/* Eigen-decomposition of a batch of dense symmetric blocks (host memory).
+ * a[b]: n[b] x n[b] column-major, both triangles filled; on return it holds the
+ *       eigenvectors (column r belongs to w[b][r]), as dsyev('V') does.
+ * w[b]: n[b] eigenvalues in ascending order.
+ * Replaces one dsyev_ call per block (src/diag.h:54-89). */
+int nrgb_syev_batched(nrgb_ctx* ctx, int nblocks, const int* n, double* const* a,
+                      double* const* w);
+
+/* Same on device memory: a_dev[b] is destroyed, z_dev[b] (n x n, must not alias
+ * a_dev[b]) receives the eigenvectors, w_dev[b] the eigenvalues.  Runs on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and returns after
+ * the work completed. */
+int nrgb_syev_batched_dev(nrgb_ctx* ctx, int nblocks, const int* n, double* const* a_dev,
+                          double* const* w_dev, double* const* z_dev, void* stream);
+
+/* One product term of a grouped GEMM:  alpha * op(A) * op(B),
+ * op(A) m x k, op(B) k x n, trans = 0 (as stored) or 1 (transposed). */
+typedef struct {
+  const double* a;
+  const double* b;
+  int lda, ldb, k, trans_a, trans_b;
+  double alpha;
+} nrgb_gemm_term;
+
+/* Output of a grouped GEMM:  C = beta*C + sum of terms[term0 .. term0+nterms). */
+typedef struct {
+  double* c;
+  int ldc, m, n;
+  double beta;
+  int term0, nterms;
+} nrgb_gemm_out;
+
+/* Grouped FP64 GEMM on device pointers (descriptors in host memory). */
+int nrgb_gemm_grouped_dev(nrgb_ctx* ctx, int nout, const nrgb_gemm_out* outs, int nterms,
+                          const nrgb_gemm_term* terms, void* stream);
+
+/* Full NRG run of the QS symmetry on the GPU: reads workdir/param and
+ * workdir/data, writes td, custom, annotated.dat (if requested) and the
+ * spectral-function files into outdir.  stats (may be NULL) receives
+ * [0] wall seconds, [1] eigensolver seconds, [2] recalc seconds,
+ * [3] density-matrix seconds, [4] spectral seconds, [5] kernels launched,
+ * [6] host->device bytes, [7] device->host bytes. */
+int nrgb_run(nrgb_ctx* ctx, const char* workdir, const char* outdir, double* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NRGB_H */

@@ -1,0 +1,204 @@
+// Grouped, segmented-K FP64 GEMM on the DMMA tensor-core path (sm_100a).
+// See gemm_f64.cuh for the contract.
+//
+// Tile: 64x64 per CTA, 4 warps of 32x32, K staged 16 at a time through
+// double-buffered shared memory (k-major, padded so the DMMA fragment loads
+// are bank-conflict free).  mma.sync.m8n8k4.f64: A fragment A[g][t],
+// B fragment B[t][g], accumulator C[g][2t..2t+1] with g = lane/4, t = lane%4.
+#include "gemm_f64.cuh"
+
+namespace nrgb {
+
+namespace {
+
+constexpr int BM = GEMM_BM, BN = GEMM_BN, BK = GEMM_BK;
+constexpr int PAD = 4;          // row stride 68 doubles: t*68+g hits 16 distinct bank pairs
+constexpr int LDS = BM + PAD;   // BM == BN
+constexpr int NT = 128;
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+struct TileLoader {
+  // 8 A values and 8 B values per thread per K-tile.
+  double ra[8], rb[8];
+
+  __device__ __forceinline__ void load(const GemmSeg& s, int k0, int row0, int col0, int m, int n,
+                                       int tid) {
+    const double alpha = s.alpha;
+    if (!s.transA) {  // A[i + p*lda], contiguous in i
+      const int i = tid & 63, pb = tid >> 6;
+      const int gi = row0 + i;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int p = pb + 2 * r, gp = k0 + p;
+        ra[r] = (gi < m && gp < s.k) ? alpha * __ldg(s.A + (size_t)gp * s.lda + gi) : 0.0;
+      }
+    } else {  // op(A)[i,p] = A[p + i*lda], contiguous in p
+      const int p = tid & 15, ib = tid >> 4;
+      const int gp = k0 + p;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int gi = row0 + ib + 8 * r;
+        ra[r] = (gi < m && gp < s.k) ? alpha * __ldg(s.A + (size_t)gi * s.lda + gp) : 0.0;
+      }
+    }
+    if (!s.transB) {  // op(B)[p,j] = B[p + j*ldb], contiguous in p
+      const int p = tid & 15, jb = tid >> 4;
+      const int gp = k0 + p;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int gj = col0 + jb + 8 * r;
+        rb[r] = (gj < n && gp < s.k) ? __ldg(s.B + (size_t)gj * s.ldb + gp) : 0.0;
+      }
+    } else {  // op(B)[p,j] = B[j + p*ldb], contiguous in j
+      const int j = tid & 63, pb = tid >> 6;
+      const int gj = col0 + j;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int p = pb + 2 * r, gp = k0 + p;
+        rb[r] = (gj < n && gp < s.k) ? __ldg(s.B + (size_t)gp * s.ldb + gj) : 0.0;
+      }
+    }
+  }
+
+  __device__ __forceinline__ void store(const GemmSeg& s, double (*As)[LDS], double (*Bs)[LDS],
+                                        int tid) {
+    if (!s.transA) {
+      const int i = tid & 63, pb = tid >> 6;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) As[pb + 2 * r][i] = ra[r];
+    } else {
+      const int p = tid & 15, ib = tid >> 4;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) As[p][ib + 8 * r] = ra[r];
+    }
+    if (!s.transB) {
+      const int p = tid & 15, jb = tid >> 4;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) Bs[p][jb + 8 * r] = rb[r];
+    } else {
+      const int j = tid & 63, pb = tid >> 6;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) Bs[pb + 2 * r][j] = rb[r];
+    }
+  }
+};
+
+__global__ void __launch_bounds__(NT) gemm_grouped_kernel(const GemmProb* __restrict__ probs,
+                                                          int nprob,
+                                                          const GemmSeg* __restrict__ segs) {
+  __shared__ __align__(16) double As[2][BK][LDS];
+  __shared__ __align__(16) double Bs[2][BK][LDS];
+
+  // Locate the problem owning this tile (probs sorted by tile0).
+  const int tile = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (probs[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+  }
+  const GemmProb P = probs[lo];
+  const int t = tile - P.tile0;
+  const int row0 = (t / P.tiles_n) * BM;
+  const int col0 = (t % P.tiles_n) * BN;
+  const int m = P.m, n = P.n;
+  if (row0 >= m || col0 >= n) return;  // shapes may be set on the device below the planned bound
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  // Flattened (segment, k-tile) iteration.
+  int s = P.seg0, send = P.seg0 + P.nseg;
+  // skip empty segments
+  while (s < send && segs[s].k <= 0) ++s;
+  if (s < send) {
+    TileLoader L;
+    GemmSeg cur = segs[s];
+    int k0 = 0;
+    L.load(cur, k0, row0, col0, m, n, tid);
+    L.store(cur, As[0], Bs[0], tid);
+    __syncthreads();
+    int buf = 0;
+    while (true) {
+      // advance to next (segment, k0)
+      GemmSeg nxt = cur;
+      int nk0 = k0 + BK;
+      int ns = s;
+      bool more = true;
+      if (nk0 >= cur.k) {
+        ns = s + 1;
+        while (ns < send && segs[ns].k <= 0) ++ns;
+        if (ns < send) {
+          nxt = segs[ns];
+          nk0 = 0;
+        } else {
+          more = false;
+        }
+      }
+      if (more) L.load(nxt, nk0, row0, col0, m, n, tid);
+
+#pragma unroll
+      for (int kk = 0; kk < BK; kk += 4) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[buf][kk + tq][wm + i * 8 + g];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk + tq][wn + j * 8 + g];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+      }
+      if (!more) break;
+      L.store(nxt, As[buf ^ 1], Bs[buf ^ 1], tid);
+      __syncthreads();
+      buf ^= 1;
+      cur = nxt;
+      s = ns;
+      k0 = nk0;
+    }
+  }
+
+  // Epilogue: C = acc + beta*C.
+  const double beta = P.beta;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = row0 + wm + i * 8 + g;
+    if (r >= m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = col0 + wn + j * 8 + 2 * tq + h;
+        if (c < n) {
+          double* dst = P.C + (size_t)c * P.ldc + r;
+          const double v = acc[i][j][h];
+          *dst = (beta == 0.0) ? v : v + beta * (*dst);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
+                                int total_tiles, cudaStream_t stream) {
+  if (total_tiles <= 0 || nprob <= 0) return cudaSuccess;
+  gemm_grouped_kernel<<<total_tiles, NT, 0, stream>>>(d_probs, nprob, d_segs);
+  return cudaGetLastError();
+}
+
+}  // namespace nrgb

@@ -1,0 +1,49 @@
+// Grouped, segmented-K FP64 GEMM on the FP64 tensor cores (DMMA) of sm_100a.
+//
+//   C_p[m_p x n_p] = beta_p * C_p + sum_{s in segments(p)} alpha_s * op(A_s) op(B_s)
+//
+// All matrices are column-major.  One launch covers every problem of a
+// batch; a CTA computes one BM x BN tile of one problem and runs the K loop
+// over all segments of that problem, so several products that accumulate
+// into the same output (the rows j of a recalculation table, the
+// combinations i of a density-matrix update) need no atomics and no
+// ordering between launches.
+//
+// This is the contraction that replaces the BLAS gemm calls of
+// src/recalc.cc:90-91, 268-272 and src/dmnrg.h:382-387.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nrgb {
+
+struct GemmSeg {
+  const double* A;   // op(A) is m x k
+  const double* B;   // op(B) is k x n
+  int lda, ldb;
+  int k;
+  int transA, transB;  // 0: as stored (col-major), 1: transposed
+  double alpha;
+};
+
+struct GemmProb {
+  double* C;
+  int ldc;
+  int m, n;
+  double beta;         // 0 -> C is overwritten (not read)
+  int seg0, nseg;      // segment range in the segment array
+  int tile0;           // first global tile index of this problem
+  int tiles_n;         // number of tiles along n
+};
+
+// Launch: problems/segments already in device memory.  total_tiles is the
+// sum over problems of ceil(m/BM)*ceil(n/BN).  Returns cudaError_t.
+cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
+                                int total_tiles, cudaStream_t stream);
+
+// Tile sizes (exported so hosts can compute tile counts).
+constexpr int GEMM_BM = 64;
+constexpr int GEMM_BN = 64;
+constexpr int GEMM_BK = 16;
+
+}  // namespace nrgb

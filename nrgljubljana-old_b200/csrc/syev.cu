@@ -1,0 +1,1342 @@
+// Batched FP64 symmetric eigensolver (see syev.cuh).
+//
+// Numerical methods (written from the published algorithms):
+//  * Householder reflector H = I - tau v v^T, v(0) = 1, chosen so that
+//    H x = beta e_1, beta = -sign(x_0) ||x||, tau = (beta - x_0)/beta.
+//  * Blocked tridiagonalisation with the panel formulation A22 <- A22 - V W^T
+//    - W V^T (Dongarra, Sorensen, Hammarling 1989).
+//  * Implicit symmetric QR step with Wilkinson shift (Golub & Van Loan,
+//    Matrix Computations, Alg. 8.3.2) for the leaves and the small path.
+//  * Divide and conquer: Cuppen's rank-one tearing, deflation of small z_i
+//    and of close d_i by Givens rotations, secular-equation roots by a
+//    safeguarded two-pole rational iteration (Bunch-Nielsen-Sorensen / Li
+//    "middle way" model) in coordinates relative to the nearer pole, and
+//    eigenvectors from the Loewner-formula z-hat (Gu & Eisenstat 1995), which
+//    keeps them orthogonal without extra precision.
+#include <math.h>
+
+#include <algorithm>
+#include <numeric>
+
+#include "gemm_f64.cuh"
+#include "syev.cuh"
+
+namespace nrgb {
+
+namespace {
+
+constexpr int SMALL_N = 32;     // warp-per-problem path
+constexpr int LEAF = 32;        // D&C leaf size
+constexpr int NB = 32;          // tridiagonalisation panel width
+constexpr int NBB = 64;         // back-transformation block of reflectors
+constexpr int TRD_NT = 256;     // threads of the panel kernel
+constexpr double EPS = 2.220446049250313e-16;
+
+// --------------------------------------------------------------------------
+// Small path: one warp per problem (n <= 32), everything in shared memory.
+// --------------------------------------------------------------------------
+struct SmallProb {
+  const double* A;
+  double* w;
+  double* Z;
+  int n;
+};
+
+constexpr int SMALL_WARPS = 2;
+
+__device__ void givens_qr_sweep_warp(double* d, double* e, double (*Z)[33], int n, int lane,
+                                     double* cs, int* fail) {
+  // Implicit symmetric QR with Wilkinson shift on tridiagonal (d, e),
+  // rotations accumulated into the columns of Z (Z <- Z G^T).
+  int iter = 0;
+  const int maxiter = 40 * n + 40;
+  int hi = n - 1;
+  while (hi > 0) {
+    // lane 0 drives the sequential part; all lanes follow the same control flow
+    int lo;
+    if (lane == 0) {
+      // deflate from the bottom
+      while (hi > 0 && fabs(e[hi - 1]) <= EPS * (fabs(d[hi - 1]) + fabs(d[hi]))) {
+        e[hi - 1] = 0.0;
+        --hi;
+      }
+      lo = hi;
+      while (lo > 0 && fabs(e[lo - 1]) > EPS * (fabs(d[lo - 1]) + fabs(d[lo]))) --lo;
+      cs[2] = (double)hi;
+      cs[3] = (double)lo;
+    }
+    __syncwarp();
+    hi = (int)cs[2];
+    lo = (int)cs[3];
+    __syncwarp();
+    if (hi <= 0) break;
+    if (++iter > maxiter) {
+      if (lane == 0) atomicExch(fail, 1);
+      break;
+    }
+    // one implicit QR step on [lo, hi]
+    double x = 0.0, z = 0.0, bulge = 0.0;
+    for (int k = lo; k < hi; ++k) {
+      if (lane == 0) {
+        if (k == lo) {
+          const double dl = (d[hi - 1] - d[hi]) * 0.5;
+          const double eh = e[hi - 1];
+          const double den = dl + copysign(hypot(dl, eh), dl == 0.0 ? 1.0 : dl);
+          const double mu = d[hi] - eh * eh / den;
+          x = d[lo] - mu;
+          z = e[lo];
+        } else {
+          x = e[k - 1];
+          z = bulge;
+        }
+        const double r = hypot(x, z);
+        double c = 1.0, s = 0.0;
+        if (r != 0.0) {
+          c = x / r;
+          s = z / r;
+        }
+        if (k > lo) e[k - 1] = r;
+        // rotate the 2x2 block [[d_k, e_k],[e_k, d_k1]] by R = [[c, s],[-s, c]]
+        const double a = d[k], b = e[k], dd = d[k + 1];
+        d[k] = c * c * a + 2.0 * c * s * b + s * s * dd;
+        d[k + 1] = s * s * a - 2.0 * c * s * b + c * c * dd;
+        e[k] = c * s * (dd - a) + (c * c - s * s) * b;
+        if (k + 1 < hi) {
+          bulge = s * e[k + 1];
+          e[k + 1] = c * e[k + 1];
+        }
+        cs[0] = c;
+        cs[1] = s;
+      }
+      __syncwarp();
+      const double c = cs[0], s = cs[1];
+      if (lane < n) {
+        const double zk = Z[lane][k], zk1 = Z[lane][k + 1];
+        Z[lane][k] = c * zk + s * zk1;
+        Z[lane][k + 1] = -s * zk + c * zk1;
+      }
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(32 * SMALL_WARPS) syev_small_kernel(const SmallProb* probs,
+                                                                       int nprob, int* fail) {
+  __shared__ double As[SMALL_WARPS][32][33];
+  __shared__ double Zs[SMALL_WARPS][32][33];
+  __shared__ double dv[SMALL_WARPS][32], ev[SMALL_WARPS][32], vv[SMALL_WARPS][32],
+      wv[SMALL_WARPS][32], tv[SMALL_WARPS][32];
+  __shared__ double csv[SMALL_WARPS][4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = blockIdx.x * SMALL_WARPS + warp;
+  if (p >= nprob) return;
+  const SmallProb P = probs[p];
+  const int n = P.n;
+  double(*A)[33] = As[warp];
+  double(*Z)[33] = Zs[warp];
+  double *d = dv[warp], *e = ev[warp], *v = vv[warp], *w = wv[warp], *tau = tv[warp];
+  for (int j = 0; j < n; ++j) A[lane][j] = (lane < n) ? P.A[lane + (size_t)j * n] : 0.0;
+  __syncwarp();
+  // Householder tridiagonalisation: columns c = 0 .. n-3
+  for (int c = 0; c + 2 < n; ++c) {
+    const double xi = (lane >= c + 2 && lane < n) ? A[lane][c] : 0.0;
+    const double xn2 = warp_sum(xi * xi);
+    const double alpha = A[c + 1][c];
+    double tc = 0.0, beta = alpha, scal = 0.0;
+    if (xn2 != 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+      tc = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    const double vi = (lane == c + 1) ? 1.0 : ((lane >= c + 2 && lane < n) ? A[lane][c] * scal : 0.0);
+    v[lane] = vi;
+    __syncwarp();
+    // p = tau A22 v
+    double pi = 0.0;
+    if (lane >= c + 1 && lane < n)
+      for (int j = c + 1; j < n; ++j) pi += A[lane][j] * v[j];
+    pi *= tc;
+    const double pv = warp_sum(pi * vi);
+    const double wi = pi - 0.5 * tc * pv * vi;
+    w[lane] = wi;
+    __syncwarp();
+    if (lane >= c + 1 && lane < n)
+      for (int j = c + 1; j < n; ++j) A[lane][j] -= vi * w[j] + wi * v[j];
+    __syncwarp();
+    if (lane >= c + 2 && lane < n) A[lane][c] = vi;  // store reflector
+    if (lane == 0) {
+      e[c] = beta;
+      tau[c] = tc;
+    }
+    __syncwarp();
+  }
+  if (lane < n) d[lane] = A[lane][lane];
+  if (lane == 0 && n >= 2) e[n - 2] = A[n - 1][n - 2];
+  // Form Q = H_0 H_1 ... H_{n-3} explicitly (Z <- I, then Z <- H_c Z for c descending)
+  for (int j = 0; j < n; ++j) Z[lane][j] = (lane == j) ? 1.0 : 0.0;
+  __syncwarp();
+  for (int c = n - 3; c >= 0; --c) {
+    const double tc = tau[c];
+    if (tc == 0.0) continue;
+    // lane j handles column j of Z
+    if (lane < n) {
+      double s = Z[c + 1][lane];
+      for (int i = c + 2; i < n; ++i) s += A[i][c] * Z[i][lane];
+      s *= tc;
+      Z[c + 1][lane] -= s;
+      for (int i = c + 2; i < n; ++i) Z[i][lane] -= A[i][c] * s;
+    }
+    __syncwarp();
+  }
+  givens_qr_sweep_warp(d, e, Z, n, lane, csv[warp], fail);
+  // sort ascending (selection sort by lane 0, swap columns by all lanes)
+  for (int i = 0; i < n - 1; ++i) {
+    if (lane == 0) {
+      int kmin = i;
+      for (int k = i + 1; k < n; ++k)
+        if (d[k] < d[kmin]) kmin = k;
+      csv[warp][0] = (double)kmin;
+      if (kmin != i) {
+        const double t = d[i];
+        d[i] = d[kmin];
+        d[kmin] = t;
+      }
+    }
+    __syncwarp();
+    const int kmin = (int)csv[warp][0];
+    if (kmin != i && lane < n) {
+      const double t = Z[lane][i];
+      Z[lane][i] = Z[lane][kmin];
+      Z[lane][kmin] = t;
+    }
+    __syncwarp();
+  }
+  if (lane < n) P.w[lane] = d[lane];
+  for (int j = 0; j < n; ++j)
+    if (lane < n) P.Z[lane + (size_t)j * n] = Z[lane][j];
+}
+
+// --------------------------------------------------------------------------
+// Tridiagonalisation panel (cooperative persistent kernel).
+// --------------------------------------------------------------------------
+struct TrdProb {
+  double* A;    // n x n, ld n
+  double* d;    // n
+  double* e;    // n-1
+  double* tau;  // n-1
+  double* Vp;   // n x NB panel reflectors (explicit)
+  double* W;    // n x NB
+  double* v;    // n
+  double* y;    // n
+  double* red;  // 2 slots x (2 + 2*NB)
+  int n;
+  int cta0, ncta;
+};
+
+constexpr int RED = 2 + 2 * NB;
+
+__device__ __forceinline__ double ld_volatile(const double* p) {
+  return *reinterpret_cast<const volatile double*>(p);
+}
+
+__global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __restrict__ probs,
+                                                           int nprob, int j0, GridBarrier* bar) {
+  extern __shared__ double sm[];
+  double* scratch = sm;          // 32
+  double* VWc = sm + 32;         // 2*NB
+  double* pq = VWc + 2 * NB;     // 2*NB
+  double* vs = pq + 2 * NB;      // n_max
+  const unsigned nblocks = gridDim.x;
+  const int b = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (probs[mid].cta0 <= b) lo = mid; else hi = mid - 1;
+  }
+  const TrdProb P = probs[lo];
+  const int rank = b - P.cta0;
+  const int n = P.n;
+  const size_t ld = (size_t)n;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = TRD_NT / 32;
+
+  for (int jj = 0; jj < NB; ++jj) {
+    const int c = j0 + jj;
+    const bool act = c < n;
+    double* R = P.red + (c & 1) * RED;
+    double* Ro = P.red + ((c + 1) & 1) * RED;
+    // ---------------- phase 1: update column c (+ finish W[:, jj-1]) ----------------
+    double tprev = 0.0, a2 = 0.0;
+    if (act) {
+      if (jj > 0) {
+        tprev = __ldcg(&P.tau[c - 1]);
+        a2 = -0.5 * tprev * tprev * ld_volatile(&Ro[1]);
+      }
+      if (tid < jj) {
+        const int k = tid;
+        VWc[k] = __ldcg(&P.Vp[c + k * ld]);
+        VWc[NB + k] = (k == jj - 1) ? tprev * __ldcg(&P.y[c]) + a2 : __ldcg(&P.W[c + k * ld]);
+      }
+      __syncthreads();
+      const int m = n - c;
+      const int chunk = (m + P.ncta - 1) / P.ncta;
+      const int r0 = c + rank * chunk, r1 = min(n, r0 + chunk);
+      double ss = 0.0;
+      for (int i = r0 + tid; i < r1; i += TRD_NT) {
+        double a = __ldcg(&P.A[i + c * ld]);
+        if (jj > 0) {
+          const double wl = tprev * __ldcg(&P.y[i]) + a2 * __ldcg(&P.v[i]);
+          P.W[i + (jj - 1) * ld] = wl;
+          for (int k = 0; k < jj - 1; ++k)
+            a -= __ldcg(&P.Vp[i + k * ld]) * VWc[NB + k] + __ldcg(&P.W[i + k * ld]) * VWc[k];
+          a -= __ldcg(&P.Vp[i + (jj - 1) * ld]) * VWc[NB + jj - 1] + wl * VWc[jj - 1];
+        }
+        P.A[i + c * ld] = a;
+        if (i == c) P.d[c] = a;
+        if (i >= c + 2) ss += a * a;
+      }
+      ss = block_sum(ss, scratch);
+      if (tid == 0 && ss != 0.0) atomicAdd(&R[0], ss);
+    }
+    grid_barrier(bar, nblocks);
+    // ---------------- phase 2: Householder vector, p = W^T v, q = V^T v ----------------
+    if (act && c < n - 1) {
+      const double alpha = ld_volatile(&P.A[c + 1 + c * ld]);
+      const double xn2 = ld_volatile(&R[0]);
+      double beta = alpha, tc = 0.0, scal = 0.0;
+      if (xn2 != 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+        tc = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      if (rank == 0 && tid == 0) {
+        P.e[c] = beta;
+        P.tau[c] = tc;
+      }
+      if (rank == 0 && tid < RED) Ro[tid] = 0.0;
+      const int m = n - c - 1;
+      const int chunk = (m + P.ncta - 1) / P.ncta;
+      const int r0 = c + 1 + rank * chunk, r1 = min(n, r0 + chunk);
+      for (int i = r0 + tid; i < r1; i += TRD_NT) {
+        const double vi = (i == c + 1) ? 1.0 : __ldcg(&P.A[i + c * ld]) * scal;
+        P.v[i] = vi;
+        P.Vp[i + jj * ld] = vi;
+        if (i >= c + 2) P.A[i + c * ld] = vi;
+      }
+      __syncthreads();
+      for (int k = warp; k < jj; k += nwarps) {
+        double sp = 0.0, sq = 0.0;
+        for (int i = r0 + lane; i < r1; i += 32) {
+          const double vi = __ldcg(&P.v[i]);
+          sp += __ldcg(&P.W[i + k * ld]) * vi;
+          sq += __ldcg(&P.Vp[i + k * ld]) * vi;
+        }
+        sp = warp_sum(sp);
+        sq = warp_sum(sq);
+        if (lane == 0) {
+          if (sp != 0.0) atomicAdd(&R[2 + k], sp);
+          if (sq != 0.0) atomicAdd(&R[2 + NB + k], sq);
+        }
+      }
+    }
+    grid_barrier(bar, nblocks);
+    // ---------------- phase 3: y = A22 v - V p - W q (column dots) ----------------
+    if (act && c < n - 1) {
+      const int m = n - c - 1;
+      for (int i = tid; i < m; i += TRD_NT) vs[i] = __ldcg(&P.v[c + 1 + i]);
+      if (tid < jj) {
+        pq[tid] = ld_volatile(&R[2 + tid]);
+        pq[NB + tid] = ld_volatile(&R[2 + NB + tid]);
+      }
+      __syncthreads();
+      const int gw = rank * nwarps + warp, tw = P.ncta * nwarps;
+      double yvp = 0.0;
+      for (int j = c + 1 + gw; j < n; j += tw) {
+        const double* col = P.A + (size_t)j * ld + (c + 1);
+        double s0 = 0.0, s1 = 0.0;
+        int i = lane;
+        for (; i + 32 < m; i += 64) {
+          s0 += __ldcg(&col[i]) * vs[i];
+          s1 += __ldcg(&col[i + 32]) * vs[i + 32];
+        }
+        if (i < m) s0 += __ldcg(&col[i]) * vs[i];
+        double corr = 0.0;
+        if (lane < jj) corr = __ldcg(&P.Vp[j + lane * ld]) * pq[lane] + __ldcg(&P.W[j + lane * ld]) * pq[NB + lane];
+        const double yj = warp_sum(s0 + s1 - corr);
+        if (lane == 0) {
+          P.y[j] = yj;
+          yvp += yj * vs[j - c - 1];
+        }
+      }
+      yvp = block_sum(yvp, scratch);
+      if (tid == 0 && yvp != 0.0) atomicAdd(&R[1], yvp);
+    }
+    grid_barrier(bar, nblocks);
+  }
+  // finish W[:, NB-1] for the trailing update
+  const int c = j0 + NB - 1;
+  if (c < n - 1) {
+    const double tc = __ldcg(&P.tau[c]);
+    const double a2 = -0.5 * tc * tc * ld_volatile(&P.red[(c & 1) * RED + 1]);
+    const int m = n - c - 1;
+    const int chunk = (m + P.ncta - 1) / P.ncta;
+    const int r0 = c + 1 + rank * chunk, r1 = min(n, r0 + chunk);
+    for (int i = r0 + tid; i < r1; i += TRD_NT) P.W[i + (NB - 1) * ld] = tc * __ldcg(&P.y[i]) + a2 * __ldcg(&P.v[i]);
+  }
+}
+
+// --------------------------------------------------------------------------
+// Divide and conquer
+// --------------------------------------------------------------------------
+struct DcProb {
+  int n;
+  double* D;      // eigenvalues in progress (n)
+  const double* dT;  // tridiagonal diagonal (n)
+  const double* e;   // off-diagonal (n-1)
+  double* Q;      // n x n (ld n): eigenvectors of T
+  double* W1;     // n x n workspace
+  double* U;      // n x n workspace
+  double* ds;     // n sorted d (then compacted dK in [lo, lo+k))
+  double* zs;     // n sorted z (then zK)
+  double* dD;     // n deflated values (at [lo+k, hi))
+  int* src;       // n source column of sorted position
+  int* flag;      // n per sorted position: 1 = nondeflated, 0 = deflated
+  double* tau;    // n
+  int* orig;      // n
+  double* zhat;   // n
+  int* kcnt;      // n (value at index lo of a node)
+  double* rho;    // n (value at index lo)
+  int* rank;      // n final position
+  int* rotp;      // n rotation pairs (p index)
+  int* rotj;      // n
+  double* rotc;   // n
+  double* rots;   // n
+  int* nrot;      // n (value at index lo)
+};
+
+struct DcNode {
+  int prob, lo, mid, hi;
+};
+
+// Leaf: tridiagonal QR on [lo, hi) of one problem, one warp per leaf.
+__global__ void __launch_bounds__(64) dc_leaf_kernel(const DcProb* __restrict__ probs,
+                                                     const DcNode* __restrict__ leaves, int nleaf,
+                                                     int* fail) {
+  __shared__ double Zs[2][32][33];
+  __shared__ double dv[2][32], ev[2][32], csv[2][4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int li = blockIdx.x * 2 + warp;
+  if (li >= nleaf) return;
+  const DcNode L = leaves[li];
+  const DcProb P = probs[L.prob];
+  const int n = P.n, lo = L.lo, s = L.hi - L.lo;
+  double* d = dv[warp];
+  double* e = ev[warp];
+  double(*Z)[33] = Zs[warp];
+  if (lane < s) {
+    double dd = P.dT[lo + lane];
+    if (lane == 0 && lo > 0) dd -= fabs(P.e[lo - 1]);
+    if (lane == s - 1 && L.hi < n) dd -= fabs(P.e[L.hi - 1]);
+    d[lane] = dd;
+    if (lane < s - 1) e[lane] = P.e[lo + lane];
+  }
+  for (int j = 0; j < s; ++j) Z[lane][j] = (lane == j) ? 1.0 : 0.0;
+  __syncwarp();
+  givens_qr_sweep_warp(d, e, Z, s, lane, csv[warp], fail);
+  for (int i = 0; i < s - 1; ++i) {
+    if (lane == 0) {
+      int kmin = i;
+      for (int k = i + 1; k < s; ++k)
+        if (d[k] < d[kmin]) kmin = k;
+      csv[warp][0] = (double)kmin;
+      if (kmin != i) {
+        const double t = d[i];
+        d[i] = d[kmin];
+        d[kmin] = t;
+      }
+    }
+    __syncwarp();
+    const int kmin = (int)csv[warp][0];
+    if (kmin != i && lane < s) {
+      const double t = Z[lane][i];
+      Z[lane][i] = Z[lane][kmin];
+      Z[lane][kmin] = t;
+    }
+    __syncwarp();
+  }
+  if (lane < s) P.D[lo + lane] = d[lane];
+  for (int j = 0; j < s; ++j)
+    if (lane < s) P.Q[(size_t)(lo + lane) + (size_t)(lo + j) * n] = Z[lane][j];
+}
+
+// Merge, step 1: z, sort, deflation, rotations, compaction.  One CTA per node.
+constexpr int DC_NT = 256;
+
+__global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict__ probs,
+                                                        const DcNode* __restrict__ nodes,
+                                                        GemmProb* gprob, GemmSeg* gseg) {
+  __shared__ double scratch[32];
+  __shared__ int sk[2];
+  const DcNode N = nodes[blockIdx.x];
+  const DcProb P = probs[N.prob];
+  const int n = P.n, lo = N.lo, mid = N.mid, hi = N.hi;
+  const int n1 = mid - lo, np = hi - lo;
+  const size_t ld = (size_t)n;
+  const int tid = threadIdx.x;
+  const double beta = P.e[mid - 1];
+  const double rho = 2.0 * fabs(beta);
+  const double sgn = beta >= 0.0 ? 1.0 : -1.0;
+  const double isq2 = 0.70710678118654752440;
+  // sorted positions by merging the two ascending halves
+  double dmax = 0.0, zmax = 0.0;
+  for (int i = tid; i < np; i += DC_NT) {
+    const double di = P.D[lo + i];
+    double zi;
+    int pos;
+    if (i < n1) {
+      zi = P.Q[(size_t)(mid - 1) + (size_t)(lo + i) * ld] * isq2;
+      // count of second-half values strictly less than di
+      int a = 0, b = np - n1;
+      while (a < b) {
+        const int m = (a + b) >> 1;
+        if (P.D[mid + m] < di) a = m + 1; else b = m;
+      }
+      pos = i + a;
+    } else {
+      zi = sgn * P.Q[(size_t)mid + (size_t)(lo + i) * ld] * isq2;
+      int a = 0, b = n1;
+      while (a < b) {
+        const int m = (a + b) >> 1;
+        if (P.D[lo + m] <= di) a = m + 1; else b = m;
+      }
+      pos = (i - n1) + a;
+    }
+    P.ds[lo + pos] = di;
+    P.zs[lo + pos] = zi;
+    P.src[lo + pos] = i;
+    dmax = fmax(dmax, fabs(di));
+    zmax = fmax(zmax, fabs(zi));
+  }
+  __syncthreads();
+  // copy Q columns in sorted order into W1 (sub-block [lo,hi) x [lo,hi))
+  for (int idx = tid; idx < np * np; idx += DC_NT) {
+    const int r = idx % np, pcol = idx / np;
+    const int s = P.src[lo + pcol];
+    P.W1[(size_t)(lo + r) + (size_t)(lo + pcol) * ld] = P.Q[(size_t)(lo + r) + (size_t)(lo + s) * ld];
+  }
+  // block max of |d| and |z|
+  {
+    // reuse block_sum machinery for max via two passes
+    __shared__ double mx[2][32];
+    double a = dmax, b = zmax;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    if ((tid & 31) == 0) {
+      mx[0][tid >> 5] = a;
+      mx[1][tid >> 5] = b;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int w = 1; w < DC_NT / 32; ++w) {
+        a = fmax(a, mx[0][w]);
+        b = fmax(b, mx[1][w]);
+      }
+      scratch[0] = a;
+      scratch[1] = b;
+    }
+    __syncthreads();
+    dmax = scratch[0];
+    zmax = scratch[1];
+  }
+  __syncthreads();
+  // deflation scan (sequential)
+  if (tid == 0) {
+    const double tol = 8.0 * EPS * fmax(dmax, rho * zmax);
+    int nr = 0, k = 0, prev = -1;
+    for (int j = 0; j < np; ++j) {
+      P.flag[lo + j] = 0;
+      if (rho * fabs(P.zs[lo + j]) <= tol) continue;  // deflated by small z
+      if (prev < 0) {
+        prev = j;
+        continue;
+      }
+      double s = P.zs[lo + prev], c = P.zs[lo + j];
+      const double t = hypot(c, s);
+      const double dt = P.ds[lo + j] - P.ds[lo + prev];
+      c /= t;
+      s = -s / t;
+      if (fabs(dt * c * s) <= tol) {
+        P.zs[lo + j] = t;
+        P.zs[lo + prev] = 0.0;
+        const double dp = P.ds[lo + prev], dj = P.ds[lo + j];
+        P.ds[lo + prev] = dp * c * c + dj * s * s;
+        P.ds[lo + j] = dp * s * s + dj * c * c;
+        P.rotp[lo + nr] = prev;
+        P.rotj[lo + nr] = j;
+        P.rotc[lo + nr] = c;
+        P.rots[lo + nr] = s;
+        ++nr;
+        prev = j;  // prev deflated (flag stays 0)
+      } else {
+        P.flag[lo + prev] = 1;
+        ++k;
+        prev = j;
+      }
+    }
+    if (prev >= 0) {
+      P.flag[lo + prev] = 1;
+      ++k;
+    }
+    sk[0] = k;
+    sk[1] = nr;
+    P.kcnt[lo] = k;
+    P.rho[lo] = rho;
+    P.nrot[lo] = nr;
+  }
+  __syncthreads();
+  const int k = sk[0], nr = sk[1];
+  // apply rotations in order to W1 columns
+  for (int r = 0; r < nr; ++r) {
+    const int pc = P.rotp[lo + r], jc = P.rotj[lo + r];
+    const double c = P.rotc[lo + r], s = P.rots[lo + r];
+    double* cp = P.W1 + (size_t)(lo + pc) * ld + lo;
+    double* cj = P.W1 + (size_t)(lo + jc) * ld + lo;
+    for (int i = tid; i < np; i += DC_NT) {
+      const double x = cp[i], y = cj[i];
+      cp[i] = c * x + s * y;
+      cj[i] = c * y - s * x;
+    }
+    __syncthreads();
+  }
+  // compaction targets: nondeflated first (in order), then deflated (in order)
+  if (tid == 0) {
+    int kk = 0, dd = 0;
+    for (int j = 0; j < np; ++j) {
+      if (P.flag[lo + j]) {
+        P.rank[lo + kk] = j;  // temporarily: source sorted position of K-th
+        ++kk;
+      } else {
+        P.rank[lo + k + dd] = j;
+        ++dd;
+      }
+    }
+  }
+  __syncthreads();
+  // compact values (dK into tau scratch first to avoid overlap, then copy back)
+  for (int a = tid; a < np; a += DC_NT) {
+    const int j = P.rank[lo + a];
+    P.zhat[lo + a] = P.ds[lo + j];
+    P.tau[lo + a] = P.zs[lo + j];
+  }
+  __syncthreads();
+  for (int a = tid; a < np; a += DC_NT) {
+    if (a < k) {
+      P.ds[lo + a] = P.zhat[lo + a];
+      P.zs[lo + a] = P.tau[lo + a];
+    } else {
+      P.dD[lo + a] = P.zhat[lo + a];
+    }
+  }
+  // compact columns into Q[lo:hi, lo + a]
+  for (int idx = tid; idx < np * np; idx += DC_NT) {
+    const int r = idx % np, a = idx / np;
+    const int j = P.rank[lo + a];
+    P.Q[(size_t)(lo + r) + (size_t)(lo + a) * ld] = P.W1[(size_t)(lo + r) + (size_t)(lo + j) * ld];
+  }
+  // GEMM descriptor: W1[lo:hi, lo:lo+k] = Q[lo:hi, lo:lo+k] * U[lo:lo+k, lo:lo+k]
+  if (tid == 0) {
+    GemmProb g = gprob[blockIdx.x];  // tile0/tiles_n preset by the host
+    g.C = P.W1 + lo + (size_t)lo * ld;
+    g.ldc = n;
+    g.m = np;
+    g.n = k;
+    g.beta = 0.0;
+    gprob[blockIdx.x] = g;
+    GemmSeg s;
+    s.A = P.Q + lo + (size_t)lo * ld;
+    s.lda = n;
+    s.B = P.U + lo + (size_t)lo * ld;
+    s.ldb = n;
+    s.k = k;
+    s.transA = 0;
+    s.transB = 0;
+    s.alpha = 1.0;
+    gseg[g.seg0] = s;
+  }
+}
+
+// Secular equation roots.  One thread per root (grid: nodes x rows).
+__global__ void dc_secular_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes,
+                                  int maxnp, int* fail) {
+  const int node = blockIdx.y;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const DcNode N = nodes[node];
+  const DcProb P = probs[N.prob];
+  const int lo = N.lo;
+  const int k = P.kcnt[lo];
+  if (j >= k) return;
+  const double* d = P.ds + lo;
+  const double* z = P.zs + lo;
+  const double rho = P.rho[lo];
+  double zz = 0.0;
+  // origin choice
+  int o;
+  double tlo, thi;
+  if (j < k - 1) {
+    const double gap = d[j + 1] - d[j];
+    const double mid = 0.5 * gap;  // relative to d[j]
+    double f = 1.0;
+    for (int i = 0; i < k; ++i) f += rho * z[i] * z[i] / ((d[i] - d[j]) - mid);
+    if (f >= 0.0) {
+      o = j;
+      tlo = 0.0;
+      thi = mid;
+    } else {
+      o = j + 1;
+      tlo = -mid;
+      thi = 0.0;
+    }
+  } else {
+    for (int i = 0; i < k; ++i) zz += z[i] * z[i];
+    o = j;
+    tlo = 0.0;
+    thi = rho * zz;
+  }
+  const double dorig = d[o];
+  // poles relative to origin: delta_i = d[i] - d[o]; interval poles at j and j+1
+  const double dL = d[j] - dorig;
+  const double dR = (j < k - 1) ? d[j + 1] - dorig : 0.0;
+  double t = 0.5 * (tlo + thi);
+  bool done = false;
+  for (int it = 0; it < 200 && !done; ++it) {
+    double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0;
+    for (int i = 0; i < k; ++i) {
+      const double del = (d[i] - dorig) - t;
+      const double q = z[i] / del;
+      if (i <= j) {
+        psi += z[i] * q;
+        dpsi += q * q;
+      } else {
+        phi += z[i] * q;
+        dphi += q * q;
+      }
+    }
+    const double f = 1.0 + rho * (psi + phi);
+    if (f == 0.0) break;
+    if (f < 0.0) tlo = t; else thi = t;
+    // two-pole (one-pole for the last root) rational model step
+    double tn;
+    const double DL = dL - t;
+    if (j < k - 1) {
+      const double DR = dR - t;
+      const double s = rho * dpsi * DL * DL, S = rho * dphi * DR * DR;
+      const double cc = f - s / DL - S / DR;
+      const double bb = cc * (DL + DR) + s + S;
+      const double c0 = DL * DR * f;
+      double eta;
+      if (cc == 0.0) {
+        eta = c0 / bb;
+      } else {
+        const double disc = fmax(bb * bb - 4.0 * cc * c0, 0.0);
+        const double sq = sqrt(disc);
+        const double q = (bb >= 0.0) ? bb + sq : bb - sq;
+        const double e1 = q / (2.0 * cc), e2 = 2.0 * c0 / q;
+        eta = (e1 > DL && e1 < DR) ? e1 : e2;
+      }
+      tn = t + eta;
+    } else {
+      const double s = rho * dpsi * DL * DL;
+      const double cc = f - s / DL;
+      tn = (cc > 0.0) ? t + DL + s / cc : 0.5 * (tlo + thi);
+    }
+    if (!(tn > tlo && tn < thi)) tn = 0.5 * (tlo + thi);
+    const double step = fabs(tn - t);
+    if (step <= 2.0 * EPS * fabs(tn) || thi - tlo <= 4.0 * EPS * fmax(fabs(tlo), fabs(thi))) done = true;
+    t = tn;
+    if (it == 199 && !done) atomicExch(fail, 2);
+  }
+  P.tau[lo + j] = t;
+  P.orig[lo + j] = o;
+}
+
+// Loewner z-hat.  One thread per i.
+__global__ void dc_lowner_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes) {
+  const int node = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const DcNode N = nodes[node];
+  const DcProb P = probs[N.prob];
+  const int lo = N.lo;
+  const int k = P.kcnt[lo];
+  if (i >= k) return;
+  const double* d = P.ds + lo;
+  const double rho = P.rho[lo];
+  const double di = d[i];
+  auto lam_minus = [&](int j) { return (d[P.orig[lo + j]] - di) + P.tau[lo + j]; };
+  double prod = lam_minus(k - 1) / rho;
+  for (int j = 0; j < i; ++j) prod *= lam_minus(j) / (d[j] - di);
+  for (int j = i; j < k - 1; ++j) prod *= lam_minus(j) / (d[j + 1] - di);
+  P.zhat[lo + i] = copysign(sqrt(fmax(prod, 0.0)), P.zs[lo + i]);
+}
+
+// Eigenvectors of the rank-one problem.  One warp per column j.
+__global__ void dc_vectors_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes) {
+  const int node = blockIdx.y;
+  const int j = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const DcNode N = nodes[node];
+  const DcProb P = probs[N.prob];
+  const int lo = N.lo;
+  const int k = P.kcnt[lo];
+  if (j >= k) return;
+  const double* d = P.ds + lo;
+  const double dor = d[P.orig[lo + j]];
+  const double tj = P.tau[lo + j];
+  double* col = P.U + lo + (size_t)(lo + j) * P.n;
+  double ss = 0.0;
+  for (int i = lane; i < k; i += 32) {
+    const double u = -P.zhat[lo + i] / ((dor - d[i]) + tj);
+    col[i] = u;
+    ss += u * u;
+  }
+  ss = warp_sum(ss);
+  const double inv = 1.0 / sqrt(ss);
+  for (int i = lane; i < k; i += 32) col[i] *= inv;
+}
+
+// Final order: rank of every eigenvalue of the node; writes D and the source.
+__global__ void dc_rank_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes) {
+  const int node = blockIdx.y;
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const DcNode N = nodes[node];
+  const DcProb P = probs[N.prob];
+  const int lo = N.lo, np = N.hi - N.lo;
+  if (a >= np) return;
+  const int k = P.kcnt[lo];
+  const double* d = P.ds + lo;
+  auto val = [&](int b) {
+    return b < k ? d[P.orig[lo + b]] + P.tau[lo + b] : P.dD[lo + b];
+  };
+  const double x = val(a);
+  int r = 0;
+  for (int b = 0; b < np; ++b) {
+    const double y = val(b);
+    r += (y < x) || (y == x && b < a);
+  }
+  P.rank[lo + a] = r;
+  P.D[lo + r] = x;
+}
+
+// Deflated columns Q[:, lo+a] (a >= k) -> W1[:, lo+a]; then all columns of
+// W1 -> Q[:, lo + rank[a]].  Two launches of the same kernel (mode 0/1).
+__global__ void dc_copy_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes,
+                               int mode) {
+  const int node = blockIdx.y;
+  const int a = blockIdx.x;
+  const DcNode N = nodes[node];
+  const DcProb P = probs[N.prob];
+  const int lo = N.lo, np = N.hi - N.lo;
+  if (a >= np) return;
+  const int k = P.kcnt[lo];
+  const size_t ld = (size_t)P.n;
+  if (mode == 0) {
+    if (a < k) return;
+    const double* s = P.Q + lo + (size_t)(lo + a) * ld;
+    double* t = P.W1 + lo + (size_t)(lo + a) * ld;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) t[i] = s[i];
+  } else {
+    const double* s = P.W1 + lo + (size_t)(lo + a) * ld;
+    double* t = P.Q + lo + (size_t)(lo + P.rank[lo + a]) * ld;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) t[i] = s[i];
+  }
+}
+
+// --------------------------------------------------------------------------
+// Back-transformation helpers
+// --------------------------------------------------------------------------
+struct BtProb {
+  int n;
+  const double* A;    // reflectors below the subdiagonal
+  const double* tau;  // n-1
+  double* Vb;         // n x NBB
+  double* G;          // NBB x NBB
+  double* T;          // NBB x NBB
+  double* X;          // NBB x n
+  double* Y;          // NBB x n
+};
+
+__global__ void bt_buildV_kernel(const BtProb* __restrict__ probs, int j0) {
+  const BtProb P = probs[blockIdx.y];
+  const int kcol = blockIdx.x;  // reflector index within block
+  const int c = j0 + kcol;
+  const int n = P.n;
+  double* col = P.Vb + (size_t)kcol * n;
+  const bool valid = c <= n - 2;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double v = 0.0;
+    if (valid) {
+      if (i == c + 1) v = 1.0;
+      else if (i > c + 1) v = P.A[i + (size_t)c * n];
+    }
+    col[i] = v;
+  }
+}
+
+__global__ void bt_T_kernel(const BtProb* __restrict__ probs, int j0) {
+  const BtProb P = probs[blockIdx.x];
+  const int n = P.n;
+  const int nb = min(NBB, max(0, n - 1 - j0));
+  __shared__ double Ts[NBB][NBB + 1];
+  for (int idx = threadIdx.x; idx < NBB * NBB; idx += blockDim.x) Ts[idx % NBB][idx / NBB] = 0.0;
+  __syncthreads();
+  const int i = threadIdx.x;
+  for (int j = 0; j < nb; ++j) {
+    const double tj = P.tau[j0 + j];
+    // T[0:j, j] = -tau_j T[0:j,0:j] G[0:j, j]   (G = V^T V, column-major NBB x NBB)
+    double acc = 0.0;
+    if (i < j)
+      for (int l = i; l < j; ++l) acc += Ts[i][l] * P.G[l + j * NBB];
+    __syncthreads();
+    if (i < j) Ts[i][j] = -tj * acc;
+    if (i == j) Ts[j][j] = tj;
+    __syncthreads();
+  }
+  for (int idx = threadIdx.x; idx < NBB * NBB; idx += blockDim.x) {
+    const int r = idx % NBB, c = idx / NBB;
+    P.T[r + c * NBB] = Ts[r][c];
+  }
+}
+
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+// Host helper that batches GEMM problems and launches them.
+struct GemmBatch {
+  std::vector<GemmProb> probs;
+  std::vector<GemmSeg> segs;
+  int tiles = 0;
+  void add(double* C, int ldc, int m, int n, double beta, const std::vector<GemmSeg>& ss) {
+    if (m <= 0 || n <= 0) return;
+    GemmProb p{};
+    p.C = C;
+    p.ldc = ldc;
+    p.m = m;
+    p.n = n;
+    p.beta = beta;
+    p.seg0 = (int)segs.size();
+    p.nseg = (int)ss.size();
+    p.tile0 = tiles;
+    p.tiles_n = ceil_div(n, GEMM_BN);
+    tiles += ceil_div(m, GEMM_BM) * p.tiles_n;
+    segs.insert(segs.end(), ss.begin(), ss.end());
+    probs.push_back(p);
+  }
+  bool empty() const { return probs.empty(); }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------------
+// host orchestration
+// ------------------------------------------------------------------------
+
+SyevBatched::SyevBatched() {
+  NRGB_CUDA(cudaMalloc(&d_err_, 4 * sizeof(int)));
+  NRGB_CUDA(cudaMalloc(&d_bar_, sizeof(GridBarrier)));
+  int dev = 0;
+  NRGB_CUDA(cudaGetDevice(&dev));
+  NRGB_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
+}
+
+SyevBatched::~SyevBatched() {
+  if (d_err_) cudaFree(d_err_);
+  if (d_bar_) cudaFree(d_bar_);
+}
+
+namespace {
+struct Plan {
+  std::vector<int> small, big;
+};
+
+void plan_tree(int prob, int lo, int hi, std::vector<DcNode>& leaves,
+               std::vector<std::pair<int, DcNode>>& merges, int& height) {
+  if (hi - lo <= LEAF) {
+    leaves.push_back(DcNode{prob, lo, lo, hi});
+    height = 0;
+    return;
+  }
+  const int mid = lo + (hi - lo) / 2;
+  int h1, h2;
+  plan_tree(prob, lo, mid, leaves, merges, h1);
+  plan_tree(prob, mid, hi, leaves, merges, h2);
+  height = std::max(h1, h2) + 1;
+  merges.push_back({height, DcNode{prob, lo, mid, hi}});
+}
+}  // namespace
+
+size_t SyevBatched::workspace_bytes(const std::vector<int>& ns) {
+  ArenaPlan pl;
+  for (int n : ns) {
+    if (n <= SMALL_N) continue;
+    const size_t nn = (size_t)n * n;
+    pl.add<double>(nn);   // W1
+    pl.add<double>(nn);   // U
+    pl.add<double>((size_t)n * NB * 2);
+    pl.add<double>((size_t)n * 16);
+    pl.add<int>((size_t)n * 10);
+    pl.add<double>(2 * RED);
+    pl.add<double>((size_t)n * NBB);
+    pl.add<double>((size_t)NBB * NBB * 2);
+    pl.add<double>((size_t)NBB * n * 2);
+  }
+  pl.add<double>(64 * 1024);
+  return pl.bytes + (size_t)ns.size() * 4096 + (1 << 20);
+}
+
+void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
+  launches_ = 0;
+  NRGB_CUDA(cudaMemsetAsync(d_err_, 0, 4 * sizeof(int), st));
+  NRGB_CUDA(cudaMemsetAsync(d_bar_, 0, sizeof(GridBarrier), st));
+  std::vector<int> small, big;
+  for (int i = 0; i < (int)probs.size(); ++i) {
+    if (probs[i].n <= 0) continue;
+    (probs[i].n <= SMALL_N ? small : big).push_back(i);
+  }
+  std::vector<int> ns;
+  for (int i : big) ns.push_back(probs[i].n);
+  // plus descriptor storage
+  const size_t need = workspace_bytes(ns) + probs.size() * 512 + (1 << 20);
+  if (arena_.capacity() < need) {
+    NRGB_CUDA(cudaStreamSynchronize(st));
+    arena_.reserve(need + need / 4);
+  }
+  arena_.reset();
+
+  // ---------------- small problems ----------------
+  if (!small.empty()) {
+    std::vector<SmallProb> sp;
+    for (int i : small) sp.push_back(SmallProb{probs[i].A, probs[i].w, probs[i].Z, probs[i].n});
+    SmallProb* d_sp = arena_.alloc_n<SmallProb>(sp.size());
+    NRGB_CUDA(cudaMemcpyAsync(d_sp, sp.data(), sp.size() * sizeof(SmallProb), cudaMemcpyHostToDevice, st));
+    syev_small_kernel<<<ceil_div((int)sp.size(), SMALL_WARPS), 32 * SMALL_WARPS, 0, st>>>(
+        d_sp, (int)sp.size(), d_err_);
+    NRGB_CUDA(cudaGetLastError());
+    ++launches_;
+  }
+
+  if (!big.empty()) {
+    const int nbig = (int)big.size();
+    int nmax = 0;
+    for (int i : big) nmax = std::max(nmax, probs[i].n);
+    // per-problem workspaces
+    std::vector<TrdProb> tp(nbig);
+    std::vector<DcProb> dp(nbig);
+    std::vector<BtProb> bp(nbig);
+    std::vector<double*> dT(nbig), eT(nbig), tauT(nbig);
+    for (int b = 0; b < nbig; ++b) {
+      const SyevDesc& S = probs[big[b]];
+      const int n = S.n;
+      const size_t nn = (size_t)n * n;
+      double* W1 = arena_.alloc_n<double>(nn);
+      double* U = arena_.alloc_n<double>(nn);
+      double* Vp = arena_.alloc_n<double>((size_t)n * NB);
+      double* Wp = arena_.alloc_n<double>((size_t)n * NB);
+      double* vec = arena_.alloc_n<double>((size_t)n * 16);
+      int* ivec = arena_.alloc_n<int>((size_t)n * 10);
+      double* red = arena_.alloc_n<double>(2 * RED);
+      double* Vb = arena_.alloc_n<double>((size_t)n * NBB);
+      double* G = arena_.alloc_n<double>((size_t)NBB * NBB);
+      double* T = arena_.alloc_n<double>((size_t)NBB * NBB);
+      double* X = arena_.alloc_n<double>((size_t)NBB * n);
+      double* Y = arena_.alloc_n<double>((size_t)NBB * n);
+      dT[b] = vec;
+      eT[b] = vec + n;
+      tauT[b] = vec + 2 * n;
+      TrdProb& t = tp[b];
+      t.A = S.A;
+      t.d = dT[b];
+      t.e = eT[b];
+      t.tau = tauT[b];
+      t.Vp = Vp;
+      t.W = Wp;
+      t.v = vec + 3 * n;
+      t.y = vec + 4 * n;
+      t.red = red;
+      t.n = n;
+      DcProb& q = dp[b];
+      q.n = n;
+      q.D = S.w;
+      q.dT = dT[b];
+      q.e = eT[b];
+      q.Q = S.Z;
+      q.W1 = W1;
+      q.U = U;
+      q.ds = vec + 5 * n;
+      q.zs = vec + 6 * n;
+      q.dD = vec + 7 * n;
+      q.tau = vec + 8 * n;
+      q.zhat = vec + 9 * n;
+      q.rho = vec + 10 * n;
+      q.rotc = vec + 11 * n;
+      q.rots = vec + 12 * n;
+      q.src = ivec;
+      q.flag = ivec + n;
+      q.orig = ivec + 2 * n;
+      q.kcnt = ivec + 3 * n;
+      q.rank = ivec + 4 * n;
+      q.rotp = ivec + 5 * n;
+      q.rotj = ivec + 6 * n;
+      q.nrot = ivec + 7 * n;
+      BtProb& bt = bp[b];
+      bt.n = n;
+      bt.A = S.A;
+      bt.tau = tauT[b];
+      bt.Vb = Vb;
+      bt.G = G;
+      bt.T = T;
+      bt.X = X;
+      bt.Y = Y;
+      NRGB_CUDA(cudaMemsetAsync(red, 0, 2 * RED * sizeof(double), st));
+      NRGB_CUDA(cudaMemsetAsync(tauT[b], 0, n * sizeof(double), st));
+      NRGB_CUDA(cudaMemsetAsync(S.Z, 0, nn * sizeof(double), st));
+    }
+    // ---------------- 1) tridiagonalisation ----------------
+    {
+      const size_t smem = (size_t)(32 + 4 * NB + nmax) * sizeof(double);
+      NRGB_CUDA(cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+      int per_sm = 0;
+      NRGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_NT, smem));
+      per_sm = std::max(1, std::min(per_sm, 4));
+      const int cap = per_sm * sms_;
+      // sub-batches of at most `cap` problems
+      for (int s0 = 0; s0 < nbig; s0 += cap) {
+        const int s1 = std::min(nbig, s0 + cap);
+        const int cnt = s1 - s0;
+        // CTA allocation proportional to n^2
+        double wsum = 0.0;
+        int nm = 0;
+        for (int b = s0; b < s1; ++b) {
+          wsum += (double)tp[b].n * tp[b].n;
+          nm = std::max(nm, tp[b].n);
+        }
+        int extra = cap - cnt;
+        int tot = 0;
+        std::vector<TrdProb> sub(tp.begin() + s0, tp.begin() + s1);
+        for (int b = 0; b < cnt; ++b) {
+          const double w = (double)sub[b].n * sub[b].n / wsum;
+          int nc = 1 + (int)floor(w * extra);
+          nc = std::min(nc, std::max(1, sub[b].n / 16));
+          sub[b].cta0 = tot;
+          sub[b].ncta = nc;
+          tot += nc;
+        }
+        TrdProb* d_tp = arena_.alloc_n<TrdProb>(sub.size());
+        NRGB_CUDA(cudaMemcpyAsync(d_tp, sub.data(), sub.size() * sizeof(TrdProb), cudaMemcpyHostToDevice, st));
+        for (int j0 = 0; j0 < nm; j0 += NB) {
+          NRGB_CUDA(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned int), st));
+          int np_ = cnt;
+          void* args[] = {(void*)&d_tp, (void*)&np_, (void*)&j0, (void*)&d_bar_};
+          NRGB_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, dim3(tot), dim3(TRD_NT), args,
+                                                smem, st));
+          ++launches_;
+          // trailing update A22 -= V W^T + W V^T for rows/cols >= j0+NB
+          GemmBatch gb;
+          for (int b = 0; b < cnt; ++b) {
+            const int n = sub[b].n;
+            const int r0 = j0 + NB;
+            if (r0 >= n) continue;
+            const int m2 = n - r0;
+            GemmSeg s1{}, s2{};
+            s1.A = sub[b].Vp + r0;
+            s1.lda = n;
+            s1.B = sub[b].W + r0;
+            s1.ldb = n;
+            s1.k = NB;
+            s1.transA = 0;
+            s1.transB = 1;
+            s1.alpha = -1.0;
+            s2 = s1;
+            s2.A = sub[b].W + r0;
+            s2.B = sub[b].Vp + r0;
+            gb.add(sub[b].A + r0 + (size_t)r0 * n, n, m2, m2, 1.0, {s1, s2});
+          }
+          if (!gb.empty()) {
+            GemmProb* d_gp = arena_.alloc_n<GemmProb>(gb.probs.size());
+            GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(gb.segs.size());
+            NRGB_CUDA(cudaMemcpyAsync(d_gp, gb.probs.data(), gb.probs.size() * sizeof(GemmProb),
+                                      cudaMemcpyHostToDevice, st));
+            NRGB_CUDA(cudaMemcpyAsync(d_gs, gb.segs.data(), gb.segs.size() * sizeof(GemmSeg),
+                                      cudaMemcpyHostToDevice, st));
+            NRGB_CUDA(gemm_grouped_launch(d_gp, (int)gb.probs.size(), d_gs, gb.tiles, st));
+            ++launches_;
+          }
+        }
+      }
+    }
+    // ---------------- 2) divide and conquer ----------------
+    {
+      std::vector<DcNode> leaves;
+      std::vector<std::pair<int, DcNode>> merges;
+      int hmax = 0;
+      for (int b = 0; b < nbig; ++b) {
+        int h;
+        plan_tree(b, 0, dp[b].n, leaves, merges, h);
+        hmax = std::max(hmax, h);
+      }
+      DcProb* d_dp = arena_.alloc_n<DcProb>(nbig);
+      NRGB_CUDA(cudaMemcpyAsync(d_dp, dp.data(), nbig * sizeof(DcProb), cudaMemcpyHostToDevice, st));
+      DcNode* d_leaves = arena_.alloc_n<DcNode>(leaves.size());
+      NRGB_CUDA(cudaMemcpyAsync(d_leaves, leaves.data(), leaves.size() * sizeof(DcNode),
+                                cudaMemcpyHostToDevice, st));
+      dc_leaf_kernel<<<ceil_div((int)leaves.size(), 2), 64, 0, st>>>(d_dp, d_leaves, (int)leaves.size(),
+                                                                     d_err_ + 1);
+      NRGB_CUDA(cudaGetLastError());
+      ++launches_;
+      for (int h = 1; h <= hmax; ++h) {
+        std::vector<DcNode> lv;
+        for (auto& m : merges)
+          if (m.first == h) lv.push_back(m.second);
+        if (lv.empty()) continue;
+        const int nn = (int)lv.size();
+        int maxnp = 0;
+        GemmBatch gb;
+        for (auto& nd : lv) {
+          const int np = nd.hi - nd.lo;
+          maxnp = std::max(maxnp, np);
+          GemmSeg s{};
+          gb.add(nullptr, 0, np, np, 0.0, {s});  // shapes fixed on device (n = k <= np)
+        }
+        DcNode* d_nodes = arena_.alloc_n<DcNode>(nn);
+        GemmProb* d_gp = arena_.alloc_n<GemmProb>(nn);
+        GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(nn);
+        NRGB_CUDA(cudaMemcpyAsync(d_nodes, lv.data(), nn * sizeof(DcNode), cudaMemcpyHostToDevice, st));
+        NRGB_CUDA(cudaMemcpyAsync(d_gp, gb.probs.data(), nn * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
+        dc_prep_kernel<<<nn, DC_NT, 0, st>>>(d_dp, d_nodes, d_gp, d_gs);
+        NRGB_CUDA(cudaGetLastError());
+        dim3 g1(ceil_div(maxnp, 128), nn);
+        dc_secular_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes, maxnp, d_err_ + 2);
+        NRGB_CUDA(cudaGetLastError());
+        dc_lowner_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes);
+        NRGB_CUDA(cudaGetLastError());
+        dim3 g2(ceil_div(maxnp, 8), nn);
+        dc_vectors_kernel<<<g2, 256, 0, st>>>(d_dp, d_nodes);
+        NRGB_CUDA(cudaGetLastError());
+        NRGB_CUDA(gemm_grouped_launch(d_gp, nn, d_gs, gb.tiles, st));
+        dc_rank_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes);
+        NRGB_CUDA(cudaGetLastError());
+        dim3 g3(maxnp, nn);
+        dc_copy_kernel<<<g3, 128, 0, st>>>(d_dp, d_nodes, 0);
+        NRGB_CUDA(cudaGetLastError());
+        dc_copy_kernel<<<g3, 128, 0, st>>>(d_dp, d_nodes, 1);
+        NRGB_CUDA(cudaGetLastError());
+        launches_ += 8;
+      }
+      // problems that are a single leaf already have D, Q in place
+    }
+    // ---------------- 3) back-transformation ----------------
+    {
+      BtProb* d_bp = arena_.alloc_n<BtProb>(nbig);
+      NRGB_CUDA(cudaMemcpyAsync(d_bp, bp.data(), nbig * sizeof(BtProb), cudaMemcpyHostToDevice, st));
+      const int last = ((std::max(0, nmax - 2)) / NBB) * NBB;
+      for (int j0 = last; j0 >= 0; j0 -= NBB) {
+        // problems with reflectors in this block: n - 2 >= j0
+        std::vector<int> act;
+        for (int b = 0; b < nbig; ++b)
+          if (bp[b].n - 2 >= j0) act.push_back(b);
+        if (act.empty()) continue;
+        // V blocks (for all problems; inactive ones write zeros harmlessly)
+        bt_buildV_kernel<<<dim3(NBB, nbig), 128, 0, st>>>(d_bp, j0);
+        NRGB_CUDA(cudaGetLastError());
+        GemmBatch g1, g3, g4;
+        for (int b : act) {
+          const BtProb& P = bp[b];
+          const int n = P.n;
+          const int r0 = j0 + 1;
+          const int mrows = n - r0;
+          GemmSeg s{};
+          // G = Vb^T Vb  (rows r0..n)
+          s.A = P.Vb + r0;
+          s.lda = n;
+          s.transA = 1;
+          s.B = P.Vb + r0;
+          s.ldb = n;
+          s.transB = 0;
+          s.k = mrows;
+          s.alpha = 1.0;
+          g1.add(P.G, NBB, NBB, NBB, 0.0, {s});
+        }
+        {
+          GemmProb* d_gp = arena_.alloc_n<GemmProb>(g1.probs.size());
+          GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(g1.segs.size());
+          NRGB_CUDA(cudaMemcpyAsync(d_gp, g1.probs.data(), g1.probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
+          NRGB_CUDA(cudaMemcpyAsync(d_gs, g1.segs.data(), g1.segs.size() * sizeof(GemmSeg), cudaMemcpyHostToDevice, st));
+          NRGB_CUDA(gemm_grouped_launch(d_gp, (int)g1.probs.size(), d_gs, g1.tiles, st));
+        }
+        bt_T_kernel<<<nbig, NBB, 0, st>>>(d_bp, j0);
+        NRGB_CUDA(cudaGetLastError());
+        // X = Vb^T Z ; Y = T X ; Z -= Vb Y   (rows r0..n of Z)
+        GemmBatch gx, gy, gz;
+        for (int b : act) {
+          const BtProb& P = bp[b];
+          const int n = P.n;
+          const int r0 = j0 + 1;
+          const int mrows = n - r0;
+          double* Z = probs[big[b]].Z;
+          GemmSeg s{};
+          s.A = P.Vb + r0;
+          s.lda = n;
+          s.transA = 1;
+          s.B = Z + r0;
+          s.ldb = n;
+          s.transB = 0;
+          s.k = mrows;
+          s.alpha = 1.0;
+          gx.add(P.X, NBB, NBB, n, 0.0, {s});
+          GemmSeg t{};
+          t.A = P.T;
+          t.lda = NBB;
+          t.transA = 0;
+          t.B = P.X;
+          t.ldb = NBB;
+          t.transB = 0;
+          t.k = NBB;
+          t.alpha = 1.0;
+          gy.add(P.Y, NBB, NBB, n, 0.0, {t});
+          GemmSeg u{};
+          u.A = P.Vb + r0;
+          u.lda = n;
+          u.transA = 0;
+          u.B = P.Y;
+          u.ldb = NBB;
+          u.transB = 0;
+          u.k = NBB;
+          u.alpha = -1.0;
+          gz.add(Z + r0, n, mrows, n, 1.0, {u});
+        }
+        for (GemmBatch* gbp : {&gx, &gy, &gz}) {
+          GemmBatch& gb = *gbp;
+          GemmProb* d_gp = arena_.alloc_n<GemmProb>(gb.probs.size());
+          GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(gb.segs.size());
+          NRGB_CUDA(cudaMemcpyAsync(d_gp, gb.probs.data(), gb.probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
+          NRGB_CUDA(cudaMemcpyAsync(d_gs, gb.segs.data(), gb.segs.size() * sizeof(GemmSeg), cudaMemcpyHostToDevice, st));
+          NRGB_CUDA(gemm_grouped_launch(d_gp, (int)gb.probs.size(), d_gs, gb.tiles, st));
+        }
+        launches_ += 6;
+      }
+    }
+  }
+  // error flags
+  int herr[4] = {0, 0, 0, 0};
+  GridBarrier hb{};
+  NRGB_CUDA(cudaMemcpyAsync(herr, d_err_, sizeof(herr), cudaMemcpyDeviceToHost, st));
+  NRGB_CUDA(cudaMemcpyAsync(&hb, d_bar_, sizeof(hb), cudaMemcpyDeviceToHost, st));
+  NRGB_CUDA(cudaStreamSynchronize(st));
+  if (herr[0] || herr[1]) throw CudaError("syev: QR iteration did not converge");
+  if (herr[2]) throw CudaError("syev: secular equation iteration did not converge");
+  if (hb.error) throw CudaError("syev: grid barrier timed out");
+}
+
+}  // namespace nrgb

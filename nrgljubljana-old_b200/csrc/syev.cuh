@@ -1,0 +1,54 @@
+// Batched FP64 symmetric eigensolver for the invariant-subspace blocks of one
+// NRG step (replaces the per-block LAPACK dsyev of src/diag.h:54-89).
+//
+// Each problem: A (n x n, column-major, both triangles filled) -> eigenvalues
+// w (ascending) and orthonormal eigenvectors Z (n x n, column-major, column r
+// is the eigenvector of w[r]; ldz == n).  A is destroyed.
+//
+// Pipeline (all problems of a batch advance together):
+//   n <= 32 : one warp per problem, Householder + implicit QR in shared memory.
+//   n  > 32 : 1) blocked Householder tridiagonalisation (panel of 32 columns
+//                in a cooperative persistent kernel, trailing rank-64 update on
+//                the DMMA GEMM),
+//             2) divide and conquer on the tridiagonal (Cuppen splitting,
+//                Gu-Eisenstat eigenvectors), merges of equal tree height of all
+//                problems in the same launches,
+//             3) back-transformation with blocked (WY) reflectors on the GEMM.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace nrgb {
+
+struct SyevDesc {
+  int n;
+  double* A;   // n x n input (lda = n), destroyed
+  double* w;   // n eigenvalues (ascending)
+  double* Z;   // n x n eigenvectors (ld = n); must not alias A
+};
+
+class SyevBatched {
+ public:
+  SyevBatched();
+  ~SyevBatched();
+  // Solve all problems on `stream`.  Throws CudaError on failure (including
+  // a convergence failure or a barrier timeout reported by the kernels).
+  void run(const std::vector<SyevDesc>& probs, cudaStream_t stream);
+  // Device bytes of workspace that run() will reserve for these sizes.
+  static size_t workspace_bytes(const std::vector<int>& n);
+  // Launch statistics of the last run().
+  int last_launches() const { return launches_; }
+
+ private:
+  DeviceArena arena_;
+  int* d_err_ = nullptr;
+  GridBarrier* d_bar_ = nullptr;
+  int launches_ = 0;
+  int coop_ctas_ = 0;
+  int sms_ = 0;
+};
+
+}  // namespace nrgb

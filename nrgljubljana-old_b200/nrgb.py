@@ -1,0 +1,108 @@
+"""ctypes binding of libnrgb.so (include/nrgb.h).
+
+The library is the product: there is no Python or CPU fallback.  Loading
+fails loudly when the shared object is missing or no CUDA device is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libnrgb.so")
+
+EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
+           "nrgb_syev_batched", "nrgb_syev_batched_dev", "nrgb_gemm_grouped_dev", "nrgb_run"]
+
+
+class GemmTerm(C.Structure):
+    _fields_ = [("a", C.c_void_p), ("b", C.c_void_p), ("lda", C.c_int), ("ldb", C.c_int),
+                ("k", C.c_int), ("trans_a", C.c_int), ("trans_b", C.c_int), ("alpha", C.c_double)]
+
+
+class GemmOut(C.Structure):
+    _fields_ = [("c", C.c_void_p), ("ldc", C.c_int), ("m", C.c_int), ("n", C.c_int),
+                ("beta", C.c_double), ("term0", C.c_int), ("nterms", C.c_int)]
+
+
+_lib = None
+
+
+def load(path: str = LIBPATH):
+    """Load libnrgb.so and declare its signatures (no device needed)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("libnrgb.so not built: run nrgljubljana-old_b200/build.py")
+    lib = C.CDLL(path)
+    vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+    lib.nrgb_create.argtypes = [C.c_int, C.POINTER(vp)]
+    lib.nrgb_destroy.argtypes = [vp]
+    lib.nrgb_last_error.argtypes = [vp]
+    lib.nrgb_last_error.restype = C.c_char_p
+    lib.nrgb_version.restype = C.c_char_p
+    lib.nrgb_syev_batched.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp)]
+    lib.nrgb_syev_batched_dev.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp]
+    lib.nrgb_gemm_grouped_dev.argtypes = [vp, C.c_int, C.POINTER(GemmOut), C.c_int, C.POINTER(GemmTerm), vp]
+    lib.nrgb_run.argtypes = [vp, C.c_char_p, C.c_char_p, dp]
+    _lib = lib
+    return lib
+
+
+class Context:
+    """One nrgb context on a CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.nrgb_create(device, C.byref(h))
+        if rc != 0:
+            raise RuntimeError("nrgb_create failed (status %d): no usable CUDA device" % rc)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nrgb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError("%s failed: %s" % (what, self.lib.nrgb_last_error(self.h).decode()))
+
+    # -- eigensolver --
+    def syev_batched(self, mats):
+        """Host-memory batch: list of symmetric float64 numpy arrays ->
+        (eigenvalues list, eigenvector list).  Inputs are not modified."""
+        import numpy as np
+        n = (C.c_int * len(mats))(*[m.shape[0] for m in mats])
+        bufs = [np.asfortranarray(m, dtype=np.float64).copy(order="F") for m in mats]
+        ws = [np.empty(m.shape[0]) for m in mats]
+        a = (C.c_void_p * len(mats))(*[b.ctypes.data for b in bufs])
+        w = (C.c_void_p * len(mats))(*[x.ctypes.data for x in ws])
+        self._check(self.lib.nrgb_syev_batched(self.h, len(mats), n, a, w), "nrgb_syev_batched")
+        return ws, bufs
+
+    def syev_batched_dev(self, ns, a_ptrs, w_ptrs, z_ptrs, stream=0):
+        k = len(ns)
+        self._check(self.lib.nrgb_syev_batched_dev(
+            self.h, k, (C.c_int * k)(*ns), (C.c_void_p * k)(*a_ptrs), (C.c_void_p * k)(*w_ptrs),
+            (C.c_void_p * k)(*z_ptrs), C.c_void_p(stream)), "nrgb_syev_batched_dev")
+
+    def gemm_grouped_dev(self, outs, terms, stream=0):
+        o = (GemmOut * len(outs))(*outs)
+        t = (GemmTerm * len(terms))(*terms)
+        self._check(self.lib.nrgb_gemm_grouped_dev(self.h, len(outs), o, len(terms), t, C.c_void_p(stream)),
+                    "nrgb_gemm_grouped_dev")
+
+    def run(self, workdir: str, outdir: str):
+        stats = (C.c_double * 8)()
+        self._check(self.lib.nrgb_run(self.h, workdir.encode(), outdir.encode(), stats), "nrgb_run")
+        keys = ["wall_s", "diag_s", "recalc_s", "dm_s", "spec_s", "launches", "h2d_bytes", "d2h_bytes"]
+        return dict(zip(keys, list(stats)))
