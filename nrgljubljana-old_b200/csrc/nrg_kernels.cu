@@ -1,0 +1,247 @@
+// Device kernels of one NRG step besides the eigensolver and the GEMM.
+#include <math.h>
+
+#include "common.cuh"
+#include "nrg_kernels.cuh"
+
+namespace nrgb {
+
+namespace {
+
+__global__ void asm_diag_kernel(const AsmDiag* __restrict__ t) {
+  const AsmDiag D = t[blockIdx.y];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < D.len; r += gridDim.x * blockDim.x) {
+    const size_t p = (size_t)(D.off + r) * (D.n + 1);
+    const double e = D.E ? D.scale * D.E[r] : 0.0;
+    D.H[p] += e + D.shift;
+  }
+}
+
+// One 32x32 tile of an off-diagonal sub-block per CTA (32x8 threads).
+__global__ void asm_off_kernel(const AsmOff* __restrict__ t) {
+  __shared__ double tile[32][33];
+  const AsmOff O = t[blockIdx.y];
+  const int tiles_r = (O.rows + 31) / 32;
+  const int ntiles = tiles_r * ((O.cols + 31) / 32);
+  for (int tt = blockIdx.x; tt < ntiles; tt += gridDim.x) {
+    const int r0 = (tt % tiles_r) * 32, c0 = (tt / tiles_r) * 32;
+    // load M tile (coalesced in r), scale, write the direct block
+    for (int cc = threadIdx.y; cc < 32; cc += blockDim.y) {
+      const int r = r0 + threadIdx.x, c = c0 + cc;
+      double v = 0.0;
+      if (r < O.rows && c < O.cols) {
+        v = O.f * O.M[r + (size_t)c * O.ldm];
+        O.H[(size_t)(O.offi + r) + (size_t)(O.offj + c) * O.n] = v;
+      }
+      tile[threadIdx.x][cc] = v;
+    }
+    __syncthreads();
+    // mirror block H[offj + c, offi + r]: coalesced in c
+    for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+      const int c = c0 + threadIdx.x, r = r0 + rr;
+      if (r < O.rows && c < O.cols)
+        O.H[(size_t)(O.offj + c) + (size_t)(O.offi + r) * O.n] = tile[rr][threadIdx.x];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void gather_diag_kernel(const DiagGather* __restrict__ g, double* __restrict__ dst) {
+  const DiagGather G = g[blockIdx.y];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < G.len; r += gridDim.x * blockDim.x)
+    dst[G.dst_off + r] = G.src[(size_t)r * (G.ld + 1)];
+}
+
+__device__ __forceinline__ void bin_add(double* sbins, const BinGrid& g, double E, double w) {
+  // Bins::add / add_std (src/bins.h:102-131) with the positive/negative split
+  // of ChainSpectrumBinning::add.
+  double* b = sbins;
+  if (E < 0.0) {
+    E = -E;
+    b = sbins + g.nbins;
+  }
+  if (fabs(w) < g.discard * E) return;
+  const double pos = (log10(E) - g.l0) * g.bpd;
+  const long idx = (long)pos;  // truncation toward zero, as the reference's long(pos)
+  if (idx < 0) {
+    atomicAdd(&b[0], w);
+  } else if (idx >= g.nbins - 1) {
+    atomicAdd(&b[g.nbins - 1], w);
+  } else {
+    const double rem = pos - (double)idx;
+    atomicAdd(&b[idx], (1.0 - rem) * w);
+    atomicAdd(&b[idx + 1], rem * w);
+  }
+}
+
+__device__ __forceinline__ void flush_bins(const double* sbins, double* bins, int nb2) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb2; i += blockDim.x) {
+    const double v = sbins[i];
+    if (v != 0.0) atomicAdd(&bins[i], v);
+  }
+}
+
+constexpr int SPEC_NT = 256;
+constexpr int SPEC_PER_CTA = 8192;
+
+__global__ void __launch_bounds__(SPEC_NT) spec_dmnrg_kernel(const SpecDmnrgPair* __restrict__ pairs,
+                                                             BinGrid g, double scale, double Emin,
+                                                             double Emax, double msign,
+                                                             double* __restrict__ bins) {
+  extern __shared__ double sbins[];
+  const int nb2 = 2 * g.nbins;
+  for (int i = threadIdx.x; i < nb2; i += blockDim.x) sbins[i] = 0.0;
+  __syncthreads();
+  const SpecDmnrgPair P = pairs[blockIdx.y];
+  const long total = (long)P.dim1 * P.dimp;
+  const long e0 = (long)blockIdx.x * SPEC_PER_CTA;
+  const long e1 = min(total, e0 + SPEC_PER_CTA);
+  for (long e = e0 + threadIdx.x; e < e1; e += SPEC_NT) {
+    const int rj = (int)(e % P.dim1), rm = (int)(e / P.dim1);
+    const double dE = P.E1[rj] - P.Ep[rm];
+    const double a = fabs(dE);
+    if (a < Emin || a > Emax) continue;
+    const size_t io = (size_t)rj + (size_t)rm * P.ldo;
+    const size_t is = (size_t)rj + (size_t)rm * P.dim1;
+    const double w = P.sf * (P.SA[is] * P.op1[io] + msign * P.SB[is] * P.op2[io]);
+    bin_add(sbins, g, scale * dE, w);
+  }
+  flush_bins(sbins, bins, nb2);
+}
+
+__global__ void __launch_bounds__(SPEC_NT) spec_fdm_kernel(const SpecFdmPair* __restrict__ pairs,
+                                                           BinGrid g, double T, double wnf,
+                                                           double msign, double* __restrict__ bins) {
+  extern __shared__ double sbins[];
+  const int nb2 = 2 * g.nbins;
+  for (int i = threadIdx.x; i < nb2; i += blockDim.x) sbins[i] = 0.0;
+  __syncthreads();
+  const SpecFdmPair P = pairs[blockIdx.y];
+  const long total = (long)P.allj * P.alli;
+  const long e0 = (long)blockIdx.x * SPEC_PER_CTA;
+  const long e1 = min(total, e0 + SPEC_PER_CTA);
+  for (long e = e0 + threadIdx.x; e < e1; e += SPEC_NT) {
+    const int j = (int)(e % P.allj), i = (int)(e / P.allj);
+    const size_t io = (size_t)j + (size_t)i * P.ldo;
+    const double o1 = P.op1[io];
+    const double Ej = P.Ej[j], Ei = P.Ei[i];
+    const double dE = Ej - Ei;
+    const bool idisc = i >= P.reti, jdisc = j >= P.retj;
+    // greater correlation function
+    if (idisc) {
+      bin_add(sbins, g, dE, P.sf * o1 * P.op2[io] * wnf * exp(-Ei / T));          // A3, A2
+    } else if (jdisc) {
+      bin_add(sbins, g, dE, P.sf * o1 * P.O2R[(size_t)j + (size_t)i * P.allj]);  // A1
+    }
+    // lesser correlation function
+    if (idisc && jdisc) {
+      bin_add(sbins, g, dE, P.sf * o1 * P.op2[io] * msign * wnf * exp(-Ej / T));  // B3
+    } else if (idisc && !jdisc) {
+      bin_add(sbins, g, dE, P.sf * o1 * P.RO2[(size_t)j + (size_t)i * P.retj] * msign);  // B2
+    } else if (!idisc && jdisc) {
+      bin_add(sbins, g, dE, P.sf * o1 * P.op2[io] * msign * wnf * exp(-Ej / T));  // B1
+    }
+  }
+  flush_bins(sbins, bins, nb2);
+}
+
+__device__ double window_fnc(double x, double nntanh) {
+  if (nntanh > 0.0) {
+    const double f0 = tanh(nntanh * (0.0 - 0.5)), fx = tanh(nntanh * (x - 0.5)),
+                 f1 = tanh(nntanh * (1.0 - 0.5));
+    return (fx - f0) / (f1 - f0);
+  }
+  return x;
+}
+
+__global__ void merge_bins_kernel(const double* __restrict__ chain, double* __restrict__ full,
+                                  const double* __restrict__ ebins, BinGrid g, int mode, double Emin, double Ex, double Emax,
+                                  double nntanh, double factor, int first, int last) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 2 * g.nbins) return;
+  const double w = chain[i];
+  if (mode == 0) {
+    full[i] += w;
+    return;
+  }
+  const double e = ebins[i % g.nbins];  // representative energies computed on the host
+  if (!(Emin < e && e < Emax && w != 0.0)) return;
+  double win;
+  if (e <= Ex && last) win = 1.0;
+  else if (e >= Ex && first) win = 1.0;
+  else if (e <= Emin || e >= Emax) win = 0.0;
+  else if (e <= Ex) win = window_fnc((e - Emin) / (Ex - Emin), nntanh);
+  else win = 1.0 - window_fnc((e - Ex) / (Emax - Ex), nntanh);
+  full[i] += factor * w * win;
+}
+
+__global__ void col_scale_kernel(const ColScale* __restrict__ cs) {
+  const ColScale C = cs[blockIdx.y];
+  const long total = (long)C.rows * C.cols;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(e % C.rows), c = (int)(e / C.rows);
+    C.dst[(size_t)r + (size_t)c * C.ldd] = C.src[(size_t)r + (size_t)c * C.lds] * C.s[c];
+  }
+}
+
+inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace
+
+cudaError_t assemble_launch(const AsmDiag* d_diag, int ndiag, const AsmOff* d_off, int noff,
+                            int max_len, int max_rc, cudaStream_t st) {
+  if (ndiag > 0) {
+    dim3 g(max(1, min(64, cdiv(max_len, 256))), ndiag);
+    asm_diag_kernel<<<g, 256, 0, st>>>(d_diag);
+  }
+  if (noff > 0) {
+    dim3 g(max(1, min(1024, cdiv(max_rc, 1024))), noff);
+    asm_off_kernel<<<g, dim3(32, 8), 0, st>>>(d_off);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t gather_diag_launch(const DiagGather* d_g, int ng, int max_len, double* dst, cudaStream_t st) {
+  if (ng <= 0) return cudaSuccess;
+  dim3 g(max(1, min(64, cdiv(max_len, 256))), ng);
+  gather_diag_kernel<<<g, 256, 0, st>>>(d_g, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t spec_dmnrg_launch(const SpecDmnrgPair* d_pairs, int npairs, int max_elems, BinGrid g,
+                              double scale, double Emin, double Emax, double msign, double* bins,
+                              cudaStream_t st) {
+  if (npairs <= 0 || max_elems <= 0) return cudaSuccess;
+  dim3 grid(cdiv(max_elems, SPEC_PER_CTA), npairs);
+  const size_t smem = 2 * (size_t)g.nbins * sizeof(double);
+  spec_dmnrg_kernel<<<grid, SPEC_NT, smem, st>>>(d_pairs, g, scale, Emin, Emax, msign, bins);
+  return cudaGetLastError();
+}
+
+cudaError_t spec_fdm_launch(const SpecFdmPair* d_pairs, int npairs, int max_elems, BinGrid g,
+                            double T, double wnf, double msign, double* bins, cudaStream_t st) {
+  if (npairs <= 0 || max_elems <= 0) return cudaSuccess;
+  dim3 grid(cdiv(max_elems, SPEC_PER_CTA), npairs);
+  const size_t smem = 2 * (size_t)g.nbins * sizeof(double);
+  spec_fdm_kernel<<<grid, SPEC_NT, smem, st>>>(d_pairs, g, T, wnf, msign, bins);
+  return cudaGetLastError();
+}
+
+cudaError_t merge_bins_launch(const double* chain, double* full, const double* ebins, BinGrid g,
+                              int mode, double Emin,
+                              double Ex, double Emax, double nntanh, double factor, int first,
+                              int last, cudaStream_t st) {
+  merge_bins_kernel<<<cdiv(2 * g.nbins, 256), 256, 0, st>>>(chain, full, ebins, g, mode, Emin, Ex, Emax,
+                                                            nntanh, factor, first, last);
+  return cudaGetLastError();
+}
+
+cudaError_t col_scale_launch(const ColScale* d_cs, int ncs, int max_rows, int max_cols, cudaStream_t st) {
+  if (ncs <= 0) return cudaSuccess;
+  dim3 g(max(1, min(256, cdiv((long)max_rows * max_cols, 256))), ncs);
+  col_scale_kernel<<<g, 256, 0, st>>>(d_cs);
+  return cudaGetLastError();
+}
+
+}  // namespace nrgb

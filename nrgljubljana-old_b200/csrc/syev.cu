@@ -712,7 +712,7 @@ __global__ void dc_secular_kernel(const DcProb* __restrict__ probs, const DcNode
   const double dR = (j < k - 1) ? d[j + 1] - dorig : 0.0;
   double t = 0.5 * (tlo + thi);
   bool done = false;
-  for (int it = 0; it < 200 && !done; ++it) {
+  for (int it = 0; it < 400; ++it) {
     double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0;
     for (int i = 0; i < k; ++i) {
       const double del = (d[i] - dorig) - t;
@@ -726,7 +726,10 @@ __global__ void dc_secular_kernel(const DcProb* __restrict__ probs, const DcNode
       }
     }
     const double f = 1.0 + rho * (psi + phi);
-    if (f == 0.0) break;
+    if (f == 0.0) {
+      done = true;
+      break;
+    }
     if (f < 0.0) tlo = t; else thi = t;
     // two-pole (one-pole for the last root) rational model step
     double tn;
@@ -753,12 +756,22 @@ __global__ void dc_secular_kernel(const DcProb* __restrict__ probs, const DcNode
       const double cc = f - s / DL;
       tn = (cc > 0.0) ? t + DL + s / cc : 0.5 * (tlo + thi);
     }
+    // converged: the model step is below the resolution of t, or f is below
+    // the rounding error of its own evaluation
+    if (fabs(tn - t) <= 2.0 * EPS * fabs(t) || fabs(f) <= EPS * (8.0 + 8.0 * rho * (phi - psi))) {
+      done = true;
+      break;
+    }
     if (!(tn > tlo && tn < thi)) tn = 0.5 * (tlo + thi);
-    const double step = fabs(tn - t);
-    if (step <= 2.0 * EPS * fabs(tn) || thi - tlo <= 4.0 * EPS * fmax(fabs(tlo), fabs(thi))) done = true;
+    if (thi - tlo <= 4.0 * EPS * fmax(fabs(tlo), fabs(thi))) {
+      t = tn;
+      done = true;
+      break;
+    }
     t = tn;
-    if (it == 199 && !done) atomicExch(fail, 2);
   }
+  // a bracket that is still wide after the iteration limit is a real failure
+  if (!done && thi - tlo > 1e-10 * fmax(fabs(tlo), fabs(thi))) atomicExch(fail, 2);
   P.tau[lo + j] = t;
   P.orig[lo + j] = o;
 }

@@ -1,0 +1,154 @@
+// Symmetry plug-in interface of the NRG step (the role of class Symmetry,
+// src/symmetry.cc:64-221) and the QS plug-in: charge U(1) x spin SU(2),
+// invariant subspaces (Q, SS) with SS = 2S+1 (src/sym-QS.cc).
+//
+// The host expands these tables into flat task lists (assembly terms, GEMM
+// segments) that the device executes; the kernels never see quantum numbers.
+//
+// The QS coefficient tables restate coefnew/qs/qs-1ch-*.dat, each
+// Clebsch-Gordan expression simplified to a closed form in SS; they are
+// checked entry by entry against the reference tables by the test suite.
+#pragma once
+#include <math.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "data.h"
+
+namespace nrgb {
+
+struct OffdiagTerm { int i, j, ch; double factor; };   // 1-based combination indices
+struct DiagTerm { int i, ch; double number; };
+struct RecalcRow { int i1, ip; double factor; };
+struct RecalcTable { Invar Ip; int ch; std::vector<RecalcRow> rows; };
+
+class Symmetry {
+ public:
+  virtual ~Symmetry() = default;
+  virtual std::string name() const = 0;
+  virtual int combs() const = 0;
+  virtual const std::vector<Invar>& In() const = 0;   // ancestor = I + In[i]
+  virtual const std::vector<Invar>& QN() const = 0;   // quantum numbers of the added states
+  virtual int mult(const Invar& I) const = 0;
+  virtual bool allowed(const Invar& I) const = 0;
+  virtual bool triangle(const Invar& a, const Invar& b, const Invar& c) const = 0;
+  virtual Invar singlet() const = 0;
+  virtual Invar doublet() const = 0;
+  virtual Invar triplet() const = 0;
+  virtual std::vector<OffdiagTerm> offdiag(const Invar& I) const = 0;
+  virtual std::vector<DiagTerm> diag() const = 0;
+  // <I1||f^dag_ch||Ip> of the new site, for every I1 reachable from Ip
+  virtual std::vector<RecalcTable> recalc_f(const Invar& Ip) const = 0;
+  // doublet / triplet operator recalculation tables for bra subspace I1
+  virtual std::vector<RecalcTable> recalc_doublet(const Invar& I1) const = 0;
+  virtual std::vector<RecalcTable> recalc_triplet(const Invar& I1) const = 0;
+  virtual double specdens_factor(const Invar& Ip, const Invar& I1) const = 0;
+  virtual double dynsusc_factor(const Invar& Ip, const Invar& I1) const = 0;
+  // symmetry-specific td columns (names and values from Boltzmann sums)
+  virtual std::vector<std::string> td_names() const = 0;
+  virtual std::vector<double> td_values(const std::vector<std::pair<Invar, const std::vector<double>*>>& blocks,
+                                        double factor, double Z) const = 0;
+  static Invar combine(const Invar& a, const Invar& b) { return {a.first + b.first, a.second + b.second}; }
+  static Invar inverse(const Invar& a) { return {-a.first, -a.second}; }
+};
+
+class SymmetryQS : public Symmetry {
+ public:
+  explicit SymmetryQS(int channels) : nch_(channels) {
+    if (channels != 1) throw std::runtime_error("QS symmetry: this build provides the 1-channel tables");
+    in_ = {{1, 0}, {0, -1}, {0, 1}, {-1, 0}};
+    qn_ = {{-1, 1}, {0, 2}, {0, 2}, {1, 1}};
+  }
+  std::string name() const override { return "QS"; }
+  int combs() const override { return 4; }
+  const std::vector<Invar>& In() const override { return in_; }
+  const std::vector<Invar>& QN() const override { return qn_; }
+  int mult(const Invar& I) const override { return I.second; }
+  bool allowed(const Invar& I) const override { return I.second > 0; }
+  static bool su2(int a, int b, int c) {
+    return abs(a - b) <= c - 1 && abs(b - c) <= a - 1 && abs(c - a) <= b - 1;
+  }
+  bool triangle(const Invar& a, const Invar& b, const Invar& c) const override {
+    return a.first == b.first + c.first && su2(a.second, b.second, c.second);
+  }
+  Invar singlet() const override { return {0, 1}; }
+  Invar doublet() const override { return {1, 2}; }
+  Invar triplet() const override { return {0, 3}; }
+
+  std::vector<OffdiagTerm> offdiag(const Invar& I) const override {
+    const double ss = I.second;
+    return {{1, 2, 0, 1.0}, {1, 3, 0, 1.0}, {2, 4, 0, -sqrt((ss - 1) / ss)}, {3, 4, 0, sqrt((ss + 1) / ss)}};
+  }
+  std::vector<DiagTerm> diag() const override { return {{1, 0, 0.0}, {2, 0, 1.0}, {3, 0, 1.0}, {4, 0, 2.0}}; }
+
+  std::vector<RecalcTable> recalc_f(const Invar& Ip) const override {
+    const int qp = Ip.first, ssp = Ip.second;
+    std::vector<RecalcTable> t;
+    t.push_back({{qp + 1, ssp + 1}, 0, {{2, 1, 1.0}, {4, 3, -sqrt(double(ssp) / (ssp + 1))}}});
+    if (ssp > 1) t.push_back({{qp + 1, ssp - 1}, 0, {{3, 1, 1.0}, {4, 2, sqrt(double(ssp) / (ssp - 1))}}});
+    return t;
+  }
+  std::vector<RecalcTable> recalc_doublet(const Invar& I1) const override {
+    const int q1 = I1.first, ss1 = I1.second;
+    const double c = sqrt(double(ss1 - 1) * (ss1 + 1)) / ss1;
+    return {{{q1 - 1, ss1 + 1}, 0, {{1, 1, 1.0}, {2, 2, -c}, {3, 2, 1.0 / ss1}, {3, 3, -1.0}, {4, 4, 1.0}}},
+            {{q1 - 1, ss1 - 1}, 0, {{1, 1, 1.0}, {2, 2, -1.0}, {2, 3, -1.0 / ss1}, {3, 3, -c}, {4, 4, 1.0}}}};
+  }
+  std::vector<RecalcTable> recalc_triplet(const Invar& I1) const override {
+    const int q1 = I1.first, ss1 = I1.second;
+    const double S = (ss1 - 1) / 2.0;
+    std::vector<RecalcTable> t;
+    if (S > 0) {
+      const double t22 = sqrt(1 - 1 / S + 2 / (1 + 2 * S));
+      const double t23 = 1 / sqrt((1 + S) * (1 + 2 * S));
+      const double t32 = -1 / sqrt(S * (1 + 2 * S));
+      const double t33 = sqrt(S * (1 + 2 * S) / (pow(1 + S, 3) * (3 + 2 * S))) * (1 + S) +
+                         2 * sqrt(S / (3 + 11 * S + 12 * S * S + 4 * S * S * S));
+      t.push_back({{q1, ss1}, 0, {{1, 1, 1.0}, {2, 2, t22}, {2, 3, t23}, {3, 2, t32}, {3, 3, t33}, {4, 4, 1.0}}});
+    } else {
+      t.push_back({{q1, ss1}, 0, {{1, 1, 1.0}, {4, 4, 1.0}}});
+    }
+    t.push_back({{q1, ss1 + 2}, 0,
+                 {{1, 1, 1.0}, {2, 2, sqrt(1 + 1 / (1 + S) - 2 / (1 + 2 * S))},
+                  {3, 2, -1 / sqrt((1 + S) * (1 + 2 * S))}, {3, 3, 1.0}, {4, 4, 1.0}}});
+    if (S > 0.5) {
+      const double m33 = (sqrt((-1 + 4 * S * S) / (S + S * S)) + sqrt((-1 + 2 * S) / (S + 3 * S * S + 2 * S * S * S))) / 2;
+      t.push_back({{q1, ss1 - 2}, 0, {{1, 1, 1.0}, {2, 2, 1.0}, {2, 3, 1 / sqrt(S * (1 + 2 * S))}, {3, 3, m33}, {4, 4, 1.0}}});
+    }
+    return t;
+  }
+  double specdens_factor(const Invar& Ip, const Invar& I1) const override {
+    const double Sp = (Ip.second - 1) / 2.0;
+    return I1.second == Ip.second + 1 ? Sp + 1.0 : Sp;
+  }
+  double dynsusc_factor(const Invar& Ip, const Invar& I1) const override {
+    const int ssp = Ip.second, ss1 = I1.second;
+    if (ss1 == ssp + 2) return 1.0 + (ssp - 1) / 3.0;
+    if (ss1 == ssp) return ssp / 3.0;
+    if (ss1 == ssp - 2) return (-2.0 + ssp) / 3.0;
+    throw std::runtime_error("dynsusc_factor: not a triplet pair");
+  }
+  std::vector<std::string> td_names() const override { return {"<Sz^2>", "<Q>", "<Q^2>"}; }
+  std::vector<double> td_values(const std::vector<std::pair<Invar, const std::vector<double>*>>& blocks,
+                                double factor, double Z) const override {
+    double trSZ = 0, trQ = 0, trQ2 = 0;
+    for (const auto& b : blocks) {
+      double sumZ = 0;
+      for (double x : *b.second) sumZ += exp(-factor * x);
+      sumZ *= mult(b.first);
+      const double q = b.first.first, ss = b.first.second;
+      trQ += sumZ * q;
+      trQ2 += sumZ * q * q;
+      trSZ += sumZ * (ss * ss - 1) / 12.0;
+    }
+    return {trSZ / Z, trQ / Z, trQ2 / Z};
+  }
+
+ private:
+  int nch_;
+  std::vector<Invar> in_, qn_;
+};
+
+}  // namespace nrgb

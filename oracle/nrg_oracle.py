@@ -1058,6 +1058,14 @@ class Oracle:
             fh.write("#" + "".join("%*s " % (w, n) for n in names) + "\n")
             for row in self.td_rows:
                 fh.write(" " + "".join("%*s " % (w, _g(v, pr)) for v in row) + "\n")
+        if self.expv_rows and self.expv_rows[0][1]:
+            wc, pc = P["width_custom"], P["prec_custom"]
+            names = sorted(self.expv_rows[0][1])
+            with open(os.path.join(outdir, "custom"), "w") as fh:
+                fh.write("#" + "".join("%*s " % (wc, str(i + 1)) for i in range(len(names) + 1)) + "\n")
+                fh.write("#" + "".join("%*s " % (wc, n) for n in ["T"] + names) + "\n")
+                for T, row in self.expv_rows:
+                    fh.write(" " + "".join("%*s " % (wc, _g(v, pc)) for v in [T] + [row[n] for n in names]) + "\n")
         res = {}
         for sp in getattr(self, "spectra", []):
             res[(sp.kind, sp.spectype, sp.name)] = sp.output(outdir)

@@ -1,0 +1,48 @@
+"""Small NRG workloads shared by the parity tests and smoke(): generated
+`param`/`data` pairs (inputgen) with their oracle results."""
+import os
+
+import numpy as np
+
+import inputgen
+
+CASES = {
+    # SIAM at the particle-hole symmetric point, DM-NRG and FDM spectra
+    "siam_ph": dict(model="siam", U=0.1, eps_d=-0.05, Gamma=0.01, Lambda=2.0, Nmax=16,
+                    params={"keep": 120, "keepenergy": 10.0, "dmnrg": True, "fdm": True, "T": 1e-4,
+                            "specd": "A_d-A_d", "bins": 50, "savebins": True, "broaden": True,
+                            "dumpannotated": 20}),
+    # asymmetric SIAM, larger Lambda, fixed-number truncation, FDM only
+    "siam_asym": dict(model="siam", U=0.3, eps_d=-0.05, Gamma=0.03, Lambda=3.0, Nmax=12,
+                      params={"keep": 200, "fdm": True, "T": 1e-3, "specd": "A_d-A_d", "bins": 40,
+                              "savebins": True, "broaden": False}),
+    # single-channel Kondo model: spin (triplet) spectral function, DM-NRG
+    "kondo1": dict(model="kondo", J=[0.3], Lambda=2.0, Nmax=14,
+                   params={"keep": 150, "dmnrg": True, "fdm": True, "T": 1e-4, "spect": "SZd-SZd",
+                           "bins": 30, "savebins": True, "broaden": False}),
+}
+
+
+def make_case(name, path):
+    c = CASES[name]
+    os.makedirs(path, exist_ok=True)
+    if c["model"] == "siam":
+        inputgen.make_siam(path, c["U"], c["eps_d"], c["Gamma"], c["Lambda"], c["Nmax"], params=c["params"])
+    else:
+        inputgen.make_kondo(path, c["J"], c["Lambda"], c["Nmax"], params=c["params"])
+    return path
+
+
+def read_table(path):
+    rows = []
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("#") or not line.strip():
+                continue
+            rows.append([float(x) for x in line.split()])
+    return np.array(rows)
+
+
+def read_bins(path):
+    a = np.fromfile(path, dtype="<f8")
+    return a.reshape(-1, 2)
