@@ -40,13 +40,17 @@ def test_nrg_run_matches_oracle(ctx, tmp_path, name):
     to = cases.read_table(os.path.join(out_o, "td"))
     tg = cases.read_table(os.path.join(out_g, "td"))
     assert to.shape == tg.shape
-    scale = np.maximum(np.abs(to), 1e-12)
-    assert np.max(np.abs(tg - to) / scale) < RTOL * 10  # td is printed with 10 digits
+    # td is printed with 10 significant digits; columns that vanish by symmetry
+    # (<Q> at particle-hole symmetry) are compared against the column scale
+    colmax = np.max(np.abs(to), axis=0)
+    tol = RTOL * 10 * np.abs(to) + 1e-13 * (1.0 + colmax)
+    assert np.all(np.abs(tg - to) <= tol), np.max(np.abs(tg - to) - tol)
     # expectation values of singlet operators
     if os.path.exists(os.path.join(out_o, "custom")):
         co = cases.read_table(os.path.join(out_o, "custom"))
         cg = cases.read_table(os.path.join(out_g, "custom"))
-        assert np.max(np.abs(cg - co) / np.maximum(np.abs(co), 1e-12)) < RTOL * 10
+        colmax = np.max(np.abs(co), axis=0)
+        assert np.all(np.abs(cg - co) <= RTOL * 10 * np.abs(co) + 1e-13 * (1.0 + colmax))
     # spectral functions (raw bins)
     bins_o = sorted(glob.glob(os.path.join(out_o, "*.bin")))
     bins_g = sorted(glob.glob(os.path.join(out_g, "*.bin")))
