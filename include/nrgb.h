@@ -71,6 +71,34 @@ typedef struct {
 int nrgb_gemm_grouped_dev(nrgb_ctx* ctx, int nout, const nrgb_gemm_out* outs, int nterms,
                           const nrgb_gemm_term* terms, void* stream);
 
+/* The two hot operations of one NRG step on a batch of blocks, host memory:
+ * eigen-decomposition of every block h[b] (n[b] x n[b], column-major,
+ * symmetric; not modified) into w[b] (ascending) and eigenvectors Z_b, then
+ * for every operator o the basis change
+ *     out[o] = Z_{bra[o]}^T * op[o] * Z_{ket[o]}     (n[bra] x n[ket]),
+ * which is the per-table-row contraction U1 * O * Up^T of the reference's
+ * recalc_general (src/recalc.cc:268-272) after dsyev (src/diag.h:54-89).
+ * z[b] may be NULL (eigenvectors not returned). */
+int nrgb_eig_recalc_step(nrgb_ctx* ctx, int nblocks, const int* n, const double* const* h,
+                         double* const* w, double* const* z, int nops, const int* bra, const int* ket,
+                         const double* const* op, double* const* out);
+
+/* Same with device pointers; a_dev[b] holds the block on entry and is
+ * destroyed, z_dev[b] receives the eigenvectors.  Runs on `stream`. */
+int nrgb_eig_recalc_step_dev(nrgb_ctx* ctx, int nblocks, const int* n, double* const* a_dev,
+                             double* const* w_dev, double* const* z_dev, int nops, const int* bra,
+                             const int* ket, const double* const* op_dev, double* const* out_dev,
+                             void* stream);
+
+/* Launch accounting: enable != 0 turns on per-kernel timing with CUDA events
+ * (and resets all counters); enable == 0 turns it off. */
+int nrgb_profile(nrgb_ctx* ctx, int enable);
+/* Launches and total device milliseconds of kernel `name` since the last
+ * nrgb_profile call ("*" = all kernels of the library; ms is 0 unless timing
+ * is on).  Names: trd_panel, gemm_f64, syev_small, dc_*, bt_*, assemble_*,
+ * spec_dmnrg, spec_fdm, merge_bins, gather_diag, col_scale. */
+int nrgb_kernel_stats(nrgb_ctx* ctx, const char* name, long* launches, double* ms);
+
 /* Full NRG run of the QS symmetry on the GPU: reads workdir/param and
  * workdir/data, writes td, custom, annotated.dat (if requested) and the
  * spectral-function files into outdir.  stats (may be NULL) receives

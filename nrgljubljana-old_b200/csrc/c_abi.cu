@@ -18,6 +18,7 @@ struct nrgb_ctx {
   cudaStream_t stream = nullptr;
   std::unique_ptr<nrgb::SyevBatched> syev;
   nrgb::DeviceArena scratch;
+  nrgb::DeviceArena io;
   std::unique_ptr<nrgb::NrgDriver> driver;
 };
 
@@ -69,6 +70,7 @@ int nrgb_destroy(nrgb_ctx* ctx) {
   ctx->driver.reset();
   ctx->syev.reset();
   ctx->scratch.release();
+  ctx->io.release();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return 0;
@@ -154,6 +156,130 @@ int nrgb_gemm_grouped_dev(nrgb_ctx* ctx, int nout, const nrgb_gemm_out* outs, in
     NRGB_CUDA(nrgb::gemm_grouped_launch(dP, (int)P.size(), dS, tiles, st));
     NRGB_CUDA(cudaStreamSynchronize(st));
   });
+}
+
+namespace {
+// out[o] = Z_bra^T * op[o] * Z_ket for all o, two grouped GEMM launches.
+void recalc_pairs(nrgb_ctx* ctx, int nops, const int* n, const int* bra, const int* ket, double* const* Z,
+                  const double* const* op, double* const* out, nrgb::DeviceArena& scr, cudaStream_t st) {
+  std::vector<nrgb::GemmProb> p1, p2;
+  std::vector<nrgb::GemmSeg> s1, s2;
+  int t1 = 0, t2 = 0;
+  auto add = [](std::vector<nrgb::GemmProb>& P, std::vector<nrgb::GemmSeg>& S, int& tiles, double* C, int m,
+                int nn, const nrgb::GemmSeg& g) {
+    nrgb::GemmProb q{};
+    q.C = C;
+    q.ldc = m;
+    q.m = m;
+    q.n = nn;
+    q.beta = 0.0;
+    q.seg0 = (int)S.size();
+    q.nseg = 1;
+    q.tile0 = tiles;
+    q.tiles_n = (nn + nrgb::GEMM_BN - 1) / nrgb::GEMM_BN;
+    tiles += ((m + nrgb::GEMM_BM - 1) / nrgb::GEMM_BM) * q.tiles_n;
+    P.push_back(q);
+    S.push_back(g);
+  };
+  for (int o = 0; o < nops; ++o) {
+    const int nb = n[bra[o]], nk = n[ket[o]];
+    if (nb <= 0 || nk <= 0) continue;
+    double* T = scr.alloc_n<double>((size_t)nb * nk);
+    add(p1, s1, t1, T, nb, nk, nrgb::GemmSeg{op[o], Z[ket[o]], nb, nk, nk, 0, 0, 1.0});
+    add(p2, s2, t2, out[o], nb, nk, nrgb::GemmSeg{Z[bra[o]], T, nb, nb, nb, 1, 0, 1.0});
+  }
+  if (p1.empty()) return;
+  auto* d1 = scr.alloc_n<nrgb::GemmProb>(p1.size());
+  auto* e1 = scr.alloc_n<nrgb::GemmSeg>(s1.size());
+  auto* d2 = scr.alloc_n<nrgb::GemmProb>(p2.size());
+  auto* e2 = scr.alloc_n<nrgb::GemmSeg>(s2.size());
+  NRGB_CUDA(cudaMemcpyAsync(d1, p1.data(), p1.size() * sizeof(p1[0]), cudaMemcpyHostToDevice, st));
+  NRGB_CUDA(cudaMemcpyAsync(e1, s1.data(), s1.size() * sizeof(s1[0]), cudaMemcpyHostToDevice, st));
+  NRGB_CUDA(cudaMemcpyAsync(d2, p2.data(), p2.size() * sizeof(p2[0]), cudaMemcpyHostToDevice, st));
+  NRGB_CUDA(cudaMemcpyAsync(e2, s2.data(), s2.size() * sizeof(s2[0]), cudaMemcpyHostToDevice, st));
+  NRGB_CUDA(nrgb::gemm_grouped_launch(d1, (int)p1.size(), e1, t1, st));
+  NRGB_CUDA(nrgb::gemm_grouped_launch(d2, (int)p2.size(), e2, t2, st));
+}
+
+size_t recalc_scratch(int nops, const int* n, const int* bra, const int* ket) {
+  size_t b = 0;
+  for (int o = 0; o < nops; ++o) b += ((size_t)n[bra[o]] * n[ket[o]] + 64) * sizeof(double);
+  return b + (size_t)nops * 4 * 128 + (1 << 16);
+}
+}  // namespace
+
+int nrgb_eig_recalc_step_dev(nrgb_ctx* ctx, int nblocks, const int* n, double* const* a_dev,
+                             double* const* w_dev, double* const* z_dev, int nops, const int* bra,
+                             const int* ket, const double* const* op_dev, double* const* out_dev,
+                             void* stream) {
+  return guarded(ctx, [&] {
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int o = 0; o < nops; ++o)
+      if (bra[o] < 0 || bra[o] >= nblocks || ket[o] < 0 || ket[o] >= nblocks)
+        throw nrgb::CudaError("eig_recalc: operator block index out of range");
+    std::vector<nrgb::SyevDesc> d(nblocks);
+    for (int b = 0; b < nblocks; ++b) d[b] = nrgb::SyevDesc{n[b], a_dev[b], w_dev[b], z_dev[b]};
+    ctx->syev->run(d, st);
+    ctx->scratch.reserve(recalc_scratch(nops, n, bra, ket));
+    ctx->scratch.reset();
+    recalc_pairs(ctx, nops, n, bra, ket, z_dev, op_dev, out_dev, ctx->scratch, st);
+    NRGB_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int nrgb_eig_recalc_step(nrgb_ctx* ctx, int nblocks, const int* n, const double* const* h,
+                         double* const* w, double* const* z, int nops, const int* bra, const int* ket,
+                         const double* const* op, double* const* out) {
+  return guarded(ctx, [&] {
+    cudaStream_t st = ctx->stream;
+    for (int o = 0; o < nops; ++o)
+      if (bra[o] < 0 || bra[o] >= nblocks || ket[o] < 0 || ket[o] >= nblocks)
+        throw nrgb::CudaError("eig_recalc: operator block index out of range");
+    size_t tot = recalc_scratch(nops, n, bra, ket);
+    for (int b = 0; b < nblocks; ++b) tot += (2 * (size_t)n[b] * n[b] + n[b] + 96) * sizeof(double);
+    for (int o = 0; o < nops; ++o) tot += (2 * (size_t)n[bra[o]] * n[ket[o]] + 64) * sizeof(double);
+    ctx->io.reserve(tot);
+    ctx->io.reset();
+    std::vector<double*> A(nblocks), W(nblocks), Z(nblocks), O(nops), R(nops);
+    std::vector<nrgb::SyevDesc> d(nblocks);
+    for (int b = 0; b < nblocks; ++b) {
+      const size_t nn = (size_t)n[b] * n[b];
+      A[b] = ctx->io.alloc_n<double>(nn);
+      Z[b] = ctx->io.alloc_n<double>(nn);
+      W[b] = ctx->io.alloc_n<double>(n[b] + 1);
+      if (nn) NRGB_CUDA(cudaMemcpyAsync(A[b], h[b], nn * sizeof(double), cudaMemcpyHostToDevice, st));
+      d[b] = nrgb::SyevDesc{n[b], A[b], W[b], Z[b]};
+    }
+    for (int o = 0; o < nops; ++o) {
+      const size_t nn = (size_t)n[bra[o]] * n[ket[o]];
+      O[o] = ctx->io.alloc_n<double>(nn);
+      R[o] = ctx->io.alloc_n<double>(nn);
+      if (nn) NRGB_CUDA(cudaMemcpyAsync(O[o], op[o], nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    ctx->syev->run(d, st);
+    ctx->scratch.reserve(recalc_scratch(nops, n, bra, ket));
+    ctx->scratch.reset();
+    recalc_pairs(ctx, nops, n, bra, ket, Z.data(), (const double* const*)O.data(), R.data(), ctx->scratch, st);
+    for (int b = 0; b < nblocks; ++b) {
+      if (!n[b]) continue;
+      NRGB_CUDA(cudaMemcpyAsync(w[b], W[b], n[b] * sizeof(double), cudaMemcpyDeviceToHost, st));
+      if (z && z[b])
+        NRGB_CUDA(cudaMemcpyAsync(z[b], Z[b], (size_t)n[b] * n[b] * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    for (int o = 0; o < nops; ++o) {
+      const size_t nn = (size_t)n[bra[o]] * n[ket[o]];
+      if (nn) NRGB_CUDA(cudaMemcpyAsync(out[o], R[o], nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    NRGB_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int nrgb_profile(nrgb_ctx* ctx, int enable) {
+  return guarded(ctx, [&] { nrgb::KernelStats::get().enable(enable != 0); });
+}
+
+int nrgb_kernel_stats(nrgb_ctx* ctx, const char* name, long* launches, double* ms) {
+  return guarded(ctx, [&] { nrgb::KernelStats::get().query(name ? name : "*", launches, ms); });
 }
 
 int nrgb_run(nrgb_ctx* ctx, const char* workdir, const char* outdir, double* stats) {

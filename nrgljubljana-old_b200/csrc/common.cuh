@@ -70,6 +70,42 @@ struct ArenaPlan {
   void add(size_t n) { bytes = ((bytes + 255) & ~size_t(255)) + n * sizeof(T) + 8; }
 };
 
+// Launch counting and optional per-kernel timing with CUDA events on the
+// launching stream (used by the benchmark to time the dominant kernel
+// inside a larger call).  One instance per process; not thread-safe.
+class KernelStats {
+ public:
+  static KernelStats& get();
+  void enable(bool on);              // resets all counters
+  bool timing() const { return timing_; }
+  // bracket one launch: begin() before, end() after (no-ops without timing)
+  void begin(const char* name, cudaStream_t s);
+  void end(cudaStream_t s);
+  void count(const char* name, long n = 1);
+  // launches and total milliseconds of `name` ("*" = all kernels); syncs events
+  void query(const char* name, long* launches, double* ms);
+
+ private:
+  struct Rec { std::string name; cudaEvent_t a, b; };
+  bool timing_ = false;
+  std::vector<Rec> open_, done_;
+  std::vector<cudaEvent_t> pool_;
+  std::vector<std::pair<std::string, long>> counts_;
+  std::vector<std::pair<std::string, double>> ms_;
+  cudaEvent_t ev();
+  void settle();
+};
+
+// Counts (and, when timing is on, times) one kernel launch statement.
+#define NRGB_LAUNCH(name, stream, ...)                 \
+  do {                                                 \
+    ::nrgb::KernelStats& ks__ = ::nrgb::KernelStats::get(); \
+    ks__.count(name);                                  \
+    ks__.begin(name, stream);                          \
+    __VA_ARGS__;                                       \
+    ks__.end(stream);                                  \
+  } while (0)
+
 // Device-side state of a grid barrier (one per cooperative launch).
 struct GridBarrier {
   unsigned int count;

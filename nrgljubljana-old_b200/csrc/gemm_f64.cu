@@ -5,6 +5,7 @@
 // double-buffered shared memory (k-major, padded so the DMMA fragment loads
 // are bank-conflict free).  mma.sync.m8n8k4.f64: A fragment A[g][t],
 // B fragment B[t][g], accumulator C[g][2t..2t+1] with g = lane/4, t = lane%4.
+#include "common.cuh"
 #include "gemm_f64.cuh"
 
 namespace nrgb {
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(NT) gemm_grouped_kernel(const GemmProb* __rest
 cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
                                 int total_tiles, cudaStream_t stream) {
   if (total_tiles <= 0 || nprob <= 0) return cudaSuccess;
-  gemm_grouped_kernel<<<total_tiles, NT, 0, stream>>>(d_probs, nprob, d_segs);
+  NRGB_LAUNCH("gemm_f64", stream, gemm_grouped_kernel<<<total_tiles, NT, 0, stream>>>(d_probs, nprob, d_segs));
   return cudaGetLastError();
 }
 

@@ -193,11 +193,11 @@ cudaError_t assemble_launch(const AsmDiag* d_diag, int ndiag, const AsmOff* d_of
                             int max_len, int max_rc, cudaStream_t st) {
   if (ndiag > 0) {
     dim3 g(max(1, min(64, cdiv(max_len, 256))), ndiag);
-    asm_diag_kernel<<<g, 256, 0, st>>>(d_diag);
+    NRGB_LAUNCH("assemble_diag", st, asm_diag_kernel<<<g, 256, 0, st>>>(d_diag));
   }
   if (noff > 0) {
     dim3 g(max(1, min(1024, cdiv(max_rc, 1024))), noff);
-    asm_off_kernel<<<g, dim3(32, 8), 0, st>>>(d_off);
+    NRGB_LAUNCH("assemble_off", st, asm_off_kernel<<<g, dim3(32, 8), 0, st>>>(d_off));
   }
   return cudaGetLastError();
 }
@@ -205,7 +205,7 @@ cudaError_t assemble_launch(const AsmDiag* d_diag, int ndiag, const AsmOff* d_of
 cudaError_t gather_diag_launch(const DiagGather* d_g, int ng, int max_len, double* dst, cudaStream_t st) {
   if (ng <= 0) return cudaSuccess;
   dim3 g(max(1, min(64, cdiv(max_len, 256))), ng);
-  gather_diag_kernel<<<g, 256, 0, st>>>(d_g, dst);
+  NRGB_LAUNCH("gather_diag", st, gather_diag_kernel<<<g, 256, 0, st>>>(d_g, dst));
   return cudaGetLastError();
 }
 
@@ -215,7 +215,7 @@ cudaError_t spec_dmnrg_launch(const SpecDmnrgPair* d_pairs, int npairs, int max_
   if (npairs <= 0 || max_elems <= 0) return cudaSuccess;
   dim3 grid(cdiv(max_elems, SPEC_PER_CTA), npairs);
   const size_t smem = 2 * (size_t)g.nbins * sizeof(double);
-  spec_dmnrg_kernel<<<grid, SPEC_NT, smem, st>>>(d_pairs, g, scale, Emin, Emax, msign, bins);
+  NRGB_LAUNCH("spec_dmnrg", st, spec_dmnrg_kernel<<<grid, SPEC_NT, smem, st>>>(d_pairs, g, scale, Emin, Emax, msign, bins));
   return cudaGetLastError();
 }
 
@@ -224,7 +224,7 @@ cudaError_t spec_fdm_launch(const SpecFdmPair* d_pairs, int npairs, int max_elem
   if (npairs <= 0 || max_elems <= 0) return cudaSuccess;
   dim3 grid(cdiv(max_elems, SPEC_PER_CTA), npairs);
   const size_t smem = 2 * (size_t)g.nbins * sizeof(double);
-  spec_fdm_kernel<<<grid, SPEC_NT, smem, st>>>(d_pairs, g, T, wnf, msign, bins);
+  NRGB_LAUNCH("spec_fdm", st, spec_fdm_kernel<<<grid, SPEC_NT, smem, st>>>(d_pairs, g, T, wnf, msign, bins));
   return cudaGetLastError();
 }
 
@@ -232,15 +232,16 @@ cudaError_t merge_bins_launch(const double* chain, double* full, const double* e
                               int mode, double Emin,
                               double Ex, double Emax, double nntanh, double factor, int first,
                               int last, cudaStream_t st) {
-  merge_bins_kernel<<<cdiv(2 * g.nbins, 256), 256, 0, st>>>(chain, full, ebins, g, mode, Emin, Ex, Emax,
-                                                            nntanh, factor, first, last);
+  NRGB_LAUNCH("merge_bins", st,
+              merge_bins_kernel<<<cdiv(2 * g.nbins, 256), 256, 0, st>>>(chain, full, ebins, g, mode, Emin, Ex,
+                                                                        Emax, nntanh, factor, first, last));
   return cudaGetLastError();
 }
 
 cudaError_t col_scale_launch(const ColScale* d_cs, int ncs, int max_rows, int max_cols, cudaStream_t st) {
   if (ncs <= 0) return cudaSuccess;
   dim3 g(max(1, min(256, cdiv((long)max_rows * max_cols, 256))), ncs);
-  col_scale_kernel<<<g, 256, 0, st>>>(d_cs);
+  NRGB_LAUNCH("col_scale", st, col_scale_kernel<<<g, 256, 0, st>>>(d_cs));
   return cudaGetLastError();
 }
 

@@ -1,0 +1,87 @@
+// KernelStats (common.cuh): launch counters and event timing per kernel name.
+#include <string.h>
+
+#include "common.cuh"
+
+namespace nrgb {
+
+KernelStats& KernelStats::get() {
+  static KernelStats s;
+  return s;
+}
+
+cudaEvent_t KernelStats::ev() {
+  if (!pool_.empty()) {
+    cudaEvent_t e = pool_.back();
+    pool_.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  NRGB_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+void KernelStats::enable(bool on) {
+  settle();
+  counts_.clear();
+  ms_.clear();
+  timing_ = on;
+}
+
+void KernelStats::begin(const char* name, cudaStream_t s) {
+  if (!timing_) return;
+  Rec r{name, ev(), ev()};
+  NRGB_CUDA(cudaEventRecord(r.a, s));
+  open_.push_back(r);
+}
+
+void KernelStats::end(cudaStream_t s) {
+  if (!timing_ || open_.empty()) return;
+  Rec r = open_.back();
+  open_.pop_back();
+  NRGB_CUDA(cudaEventRecord(r.b, s));
+  done_.push_back(r);
+  if (done_.size() > 4096) settle();
+}
+
+void KernelStats::count(const char* name, long n) {
+  for (auto& c : counts_)
+    if (c.first == name) {
+      c.second += n;
+      return;
+    }
+  counts_.push_back({name, n});
+}
+
+void KernelStats::settle() {
+  for (auto& r : done_) {
+    float ms = 0.f;
+    NRGB_CUDA(cudaEventSynchronize(r.b));
+    NRGB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+    bool found = false;
+    for (auto& m : ms_)
+      if (m.first == r.name) {
+        m.second += ms;
+        found = true;
+      }
+    if (!found) ms_.push_back({r.name, (double)ms});
+    pool_.push_back(r.a);
+    pool_.push_back(r.b);
+  }
+  done_.clear();
+}
+
+void KernelStats::query(const char* name, long* launches, double* ms) {
+  settle();
+  const bool all = strcmp(name, "*") == 0;
+  long n = 0;
+  double t = 0;
+  for (auto& c : counts_)
+    if (all || c.first == name) n += c.second;
+  for (auto& m : ms_)
+    if (all || m.first == name) t += m.second;
+  if (launches) *launches = n;
+  if (ms) *ms = t;
+}
+
+}  // namespace nrgb

@@ -1033,8 +1033,9 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     for (int i : small) sp.push_back(SmallProb{probs[i].A, probs[i].w, probs[i].Z, probs[i].n});
     SmallProb* d_sp = arena_.alloc_n<SmallProb>(sp.size());
     NRGB_CUDA(cudaMemcpyAsync(d_sp, sp.data(), sp.size() * sizeof(SmallProb), cudaMemcpyHostToDevice, st));
-    syev_small_kernel<<<ceil_div((int)sp.size(), SMALL_WARPS), 32 * SMALL_WARPS, 0, st>>>(
-        d_sp, (int)sp.size(), d_err_);
+    NRGB_LAUNCH("syev_small", st,
+                syev_small_kernel<<<ceil_div((int)sp.size(), SMALL_WARPS), 32 * SMALL_WARPS, 0, st>>>(
+                    d_sp, (int)sp.size(), d_err_));
     NRGB_CUDA(cudaGetLastError());
     ++launches_;
   }
@@ -1152,8 +1153,9 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           NRGB_CUDA(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned int), st));
           int np_ = cnt;
           void* args[] = {(void*)&d_tp, (void*)&np_, (void*)&j0, (void*)&d_bar_};
-          NRGB_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, dim3(tot), dim3(TRD_NT), args,
-                                                smem, st));
+          NRGB_LAUNCH("trd_panel", st,
+                      NRGB_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, dim3(tot), dim3(TRD_NT),
+                                                            args, smem, st)));
           ++launches_;
           // trailing update A22 -= V W^T + W V^T for rows/cols >= j0+NB
           GemmBatch gb;
@@ -1204,8 +1206,9 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       DcNode* d_leaves = arena_.alloc_n<DcNode>(leaves.size());
       NRGB_CUDA(cudaMemcpyAsync(d_leaves, leaves.data(), leaves.size() * sizeof(DcNode),
                                 cudaMemcpyHostToDevice, st));
-      dc_leaf_kernel<<<ceil_div((int)leaves.size(), 2), 64, 0, st>>>(d_dp, d_leaves, (int)leaves.size(),
-                                                                     d_err_ + 1);
+      NRGB_LAUNCH("dc_leaf", st,
+                  dc_leaf_kernel<<<ceil_div((int)leaves.size(), 2), 64, 0, st>>>(d_dp, d_leaves,
+                                                                                 (int)leaves.size(), d_err_ + 1));
       NRGB_CUDA(cudaGetLastError());
       ++launches_;
       for (int h = 1; h <= hmax; ++h) {
@@ -1227,23 +1230,23 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(nn);
         NRGB_CUDA(cudaMemcpyAsync(d_nodes, lv.data(), nn * sizeof(DcNode), cudaMemcpyHostToDevice, st));
         NRGB_CUDA(cudaMemcpyAsync(d_gp, gb.probs.data(), nn * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
-        dc_prep_kernel<<<nn, DC_NT, 0, st>>>(d_dp, d_nodes, d_gp, d_gs);
+        NRGB_LAUNCH("dc_prep", st, dc_prep_kernel<<<nn, DC_NT, 0, st>>>(d_dp, d_nodes, d_gp, d_gs));
         NRGB_CUDA(cudaGetLastError());
         dim3 g1(ceil_div(maxnp, 128), nn);
-        dc_secular_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes, maxnp, d_err_ + 2);
+        NRGB_LAUNCH("dc_secular", st, dc_secular_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes, maxnp, d_err_ + 2));
         NRGB_CUDA(cudaGetLastError());
-        dc_lowner_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes);
+        NRGB_LAUNCH("dc_lowner", st, dc_lowner_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
         dim3 g2(ceil_div(maxnp, 8), nn);
-        dc_vectors_kernel<<<g2, 256, 0, st>>>(d_dp, d_nodes);
+        NRGB_LAUNCH("dc_vectors", st, dc_vectors_kernel<<<g2, 256, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
         NRGB_CUDA(gemm_grouped_launch(d_gp, nn, d_gs, gb.tiles, st));
-        dc_rank_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes);
+        NRGB_LAUNCH("dc_rank", st, dc_rank_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
         dim3 g3(maxnp, nn);
-        dc_copy_kernel<<<g3, 128, 0, st>>>(d_dp, d_nodes, 0);
+        NRGB_LAUNCH("dc_copy", st, dc_copy_kernel<<<g3, 128, 0, st>>>(d_dp, d_nodes, 0));
         NRGB_CUDA(cudaGetLastError());
-        dc_copy_kernel<<<g3, 128, 0, st>>>(d_dp, d_nodes, 1);
+        NRGB_LAUNCH("dc_copy", st, dc_copy_kernel<<<g3, 128, 0, st>>>(d_dp, d_nodes, 1));
         NRGB_CUDA(cudaGetLastError());
         launches_ += 8;
       }
@@ -1261,7 +1264,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           if (bp[b].n - 2 >= j0) act.push_back(b);
         if (act.empty()) continue;
         // V blocks (for all problems; inactive ones write zeros harmlessly)
-        bt_buildV_kernel<<<dim3(NBB, nbig), 128, 0, st>>>(d_bp, j0);
+        NRGB_LAUNCH("bt_buildV", st, bt_buildV_kernel<<<dim3(NBB, nbig), 128, 0, st>>>(d_bp, j0));
         NRGB_CUDA(cudaGetLastError());
         GemmBatch g1, g3, g4;
         for (int b : act) {
@@ -1288,7 +1291,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           NRGB_CUDA(cudaMemcpyAsync(d_gs, g1.segs.data(), g1.segs.size() * sizeof(GemmSeg), cudaMemcpyHostToDevice, st));
           NRGB_CUDA(gemm_grouped_launch(d_gp, (int)g1.probs.size(), d_gs, g1.tiles, st));
         }
-        bt_T_kernel<<<nbig, NBB, 0, st>>>(d_bp, j0);
+        NRGB_LAUNCH("bt_T", st, bt_T_kernel<<<nbig, NBB, 0, st>>>(d_bp, j0));
         NRGB_CUDA(cudaGetLastError());
         // X = Vb^T Z ; Y = T X ; Z -= Vb Y   (rows r0..n of Z)
         GemmBatch gx, gy, gz;

@@ -12,7 +12,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libnrgb.so")
 
 EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
-           "nrgb_syev_batched", "nrgb_syev_batched_dev", "nrgb_gemm_grouped_dev", "nrgb_run"]
+           "nrgb_syev_batched", "nrgb_syev_batched_dev", "nrgb_gemm_grouped_dev",
+           "nrgb_eig_recalc_step", "nrgb_eig_recalc_step_dev", "nrgb_profile", "nrgb_kernel_stats",
+           "nrgb_run"]
 
 
 class GemmTerm(C.Structure):
@@ -46,6 +48,12 @@ def load(path: str = LIBPATH):
     lib.nrgb_syev_batched_dev.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp]
     lib.nrgb_gemm_grouped_dev.argtypes = [vp, C.c_int, C.POINTER(GemmOut), C.c_int, C.POINTER(GemmTerm), vp]
     lib.nrgb_run.argtypes = [vp, C.c_char_p, C.c_char_p, dp]
+    lib.nrgb_eig_recalc_step.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                         C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp)]
+    lib.nrgb_eig_recalc_step_dev.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                             C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp), vp]
+    lib.nrgb_profile.argtypes = [vp, C.c_int]
+    lib.nrgb_kernel_stats.argtypes = [vp, C.c_char_p, C.POINTER(C.c_long), dp]
     _lib = lib
     return lib
 
@@ -100,6 +108,35 @@ class Context:
         t = (GemmTerm * len(terms))(*terms)
         self._check(self.lib.nrgb_gemm_grouped_dev(self.h, len(outs), o, len(terms), t, C.c_void_p(stream)),
                     "nrgb_gemm_grouped_dev")
+
+    @staticmethod
+    def _ptrs(xs):
+        return (C.c_void_p * len(xs))(*[int(x) if x is not None else None for x in xs])
+
+    def eig_recalc_step(self, ns, h, w, z, bra, ket, op, out):
+        """Host-memory step: pointers are addresses of column-major float64 buffers."""
+        nb, no = len(ns), len(bra)
+        self._check(self.lib.nrgb_eig_recalc_step(
+            self.h, nb, (C.c_int * nb)(*ns), self._ptrs(h), self._ptrs(w), self._ptrs(z) if z else None,
+            no, (C.c_int * no)(*bra), (C.c_int * no)(*ket), self._ptrs(op), self._ptrs(out)),
+            "nrgb_eig_recalc_step")
+
+    def eig_recalc_step_dev(self, ns, a, w, z, bra, ket, op, out, stream=0):
+        nb, no = len(ns), len(bra)
+        self._check(self.lib.nrgb_eig_recalc_step_dev(
+            self.h, nb, (C.c_int * nb)(*ns), self._ptrs(a), self._ptrs(w), self._ptrs(z),
+            no, (C.c_int * no)(*bra), (C.c_int * no)(*ket), self._ptrs(op), self._ptrs(out),
+            C.c_void_p(stream)), "nrgb_eig_recalc_step_dev")
+
+    def profile(self, enable=True):
+        self._check(self.lib.nrgb_profile(self.h, 1 if enable else 0), "nrgb_profile")
+
+    def kernel_stats(self, name="*"):
+        n = C.c_long()
+        ms = C.c_double()
+        self._check(self.lib.nrgb_kernel_stats(self.h, name.encode(), C.byref(n), C.byref(ms)),
+                    "nrgb_kernel_stats")
+        return n.value, ms.value
 
     def run(self, workdir: str, outdir: str):
         stats = (C.c_double * 8)()
