@@ -99,6 +99,29 @@ int nrgb_profile(nrgb_ctx* ctx, int enable);
  * spec_dmnrg, spec_fdm, merge_bins, gather_diag, col_scale. */
 int nrgb_kernel_stats(nrgb_ctx* ctx, const char* name, long* launches, double* ms);
 
+/* Allocation-free basis change, device pointers:
+ *     out[o] = Z_bra[o]^T * op[o] * Z_ket[o]
+ * (Z_bra[o]: n_bra[o] x n_bra[o], op[o]: n_bra[o] x n_ket[o],
+ *  Z_ket[o]: n_ket[o] x n_ket[o], out[o]: n_bra[o] x n_ket[o], column-major).
+ * This entry point has no counterpart in the reference.  It is for callers
+ * that must not see the library allocate device memory: a host that owns the
+ * device-memory budget (e.g. a serving loop that admits runs by projected
+ * footprint) or a loop that cannot take the device-wide synchronisation of
+ * cudaMalloc/cudaFree.  It needs no context and calls no allocator: its
+ * intermediates and launch descriptors live in a fixed 32 MiB device array
+ * inside the library, which every GPU that loads the library holds until the
+ * process exits.  Limits: at most 1024 operators, and the descriptors plus all
+ * n_bra*n_ket intermediates (each rounded up to 256 bytes) must fit in 32 MiB.
+ * The first call on a device looks up the array's device address (set-up);
+ * make that first call before any stream capture.  Calls share the array:
+ * calls whose GPU work overlaps race, so order them on one stream; the call
+ * returns after its work on `stream` has finished.
+ * Returns 0 on success, 1 for invalid arguments, 5 when the sizes exceed the
+ * limits above, 6 on a CUDA error. */
+int nrgb_basis_change_noalloc(int nops, const int* n_bra, const int* n_ket, const double* const* z_bra,
+                              const double* const* z_ket, const double* const* op, double* const* out,
+                              void* stream);
+
 /* Full NRG run of the QS symmetry on the GPU: reads workdir/param and
  * workdir/data, writes td, custom, annotated.dat (if requested) and the
  * spectral-function files into outdir.  stats (may be NULL) receives

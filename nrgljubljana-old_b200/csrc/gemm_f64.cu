@@ -202,4 +202,11 @@ cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSe
   return cudaGetLastError();
 }
 
+cudaError_t gemm_grouped_launch_unaccounted(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
+                                            int total_tiles, cudaStream_t stream) {
+  if (total_tiles <= 0 || nprob <= 0) return cudaSuccess;
+  gemm_grouped_kernel<<<total_tiles, NT, 0, stream>>>(d_probs, nprob, d_segs);
+  return cudaGetLastError();
+}
+
 }  // namespace nrgb

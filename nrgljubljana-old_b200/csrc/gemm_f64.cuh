@@ -41,6 +41,11 @@ struct GemmProb {
 cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
                                 int total_tiles, cudaStream_t stream);
 
+// Same launch without the library's launch accounting (no host bookkeeping,
+// no events): used by the allocation-free entry point.
+cudaError_t gemm_grouped_launch_unaccounted(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
+                                            int total_tiles, cudaStream_t stream);
+
 // Tile sizes (exported so hosts can compute tile counts).
 constexpr int GEMM_BM = 64;
 constexpr int GEMM_BN = 64;

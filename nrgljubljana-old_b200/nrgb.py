@@ -14,7 +14,7 @@ LIBPATH = os.path.join(HERE, "libnrgb.so")
 EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
            "nrgb_syev_batched", "nrgb_syev_batched_dev", "nrgb_gemm_grouped_dev",
            "nrgb_eig_recalc_step", "nrgb_eig_recalc_step_dev", "nrgb_profile", "nrgb_kernel_stats",
-           "nrgb_run"]
+           "nrgb_basis_change_noalloc", "nrgb_run"]
 
 
 class GemmTerm(C.Structure):
@@ -54,6 +54,8 @@ def load(path: str = LIBPATH):
                                              C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp), vp]
     lib.nrgb_profile.argtypes = [vp, C.c_int]
     lib.nrgb_kernel_stats.argtypes = [vp, C.c_char_p, C.POINTER(C.c_long), dp]
+    lib.nrgb_basis_change_noalloc.argtypes = [C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                              C.POINTER(vp), vp]
     _lib = lib
     return lib
 
