@@ -46,9 +46,14 @@ NOPS_PER_PAIR = 6
 SEED = 20261204  # 20261203 + config index 1
 
 
+NMAX = 4096
+
+
 def step_sizes(step):
+    """Block sizes of a step: log-uniform on [16, 4096] (NMAX caps them for
+    small profiling cases)."""
     rng = np.random.default_rng(SEED + step)
-    return [int(round(math.exp(x))) for x in rng.uniform(math.log(16), math.log(4096), NBLOCKS)]
+    return [min(NMAX, int(round(math.exp(x)))) for x in rng.uniform(math.log(16), math.log(4096), NBLOCKS)]
 
 
 def pairs():
@@ -348,15 +353,19 @@ def run_ours(args, rank, world):
     value = world * 3600.0 / (STEPS_PER_RUN * elapsed / args.steps)
     # ---- e2e through the host-buffer C ABI ----
     hb = []
-    for s in range(min(nbatch, 2)):
+    if args.no_e2e:
+        nbatch_e2e = 0
+    else:
+        nbatch_e2e = min(nbatch, 2)
+    for s in range(nbatch_e2e):
         ns, H, O = batches[s]
         hH = [h.cpu().pin_memory() for h in H]
         hO = [o.cpu().pin_memory() for o in O]
         hw = [torch.empty(n, dtype=torch.float64).pin_memory() for n in ns]
         hout = [torch.empty(ns[k], ns[b], dtype=torch.float64).pin_memory() for b, k in zip(bra, ket)]
         hb.append((ns, hH, hO, hw, hout))
-    e2e_steps = max(3, min(args.steps, 8))
-    for s in range(1):
+    e2e_steps = max(3, min(args.steps, 8)) if hb else 0
+    for s in range(1 if hb else 0):
         ns, hH, hO, hw, hout = hb[0]
         ctx.eig_recalc_step(ns, [x.data_ptr() for x in hH], [x.data_ptr() for x in hw], None, bra, ket,
                             [x.data_ptr() for x in hO], [x.data_ptr() for x in hout])
@@ -369,13 +378,13 @@ def run_ours(args, rank, world):
         ctx.eig_recalc_step(ns, [x.data_ptr() for x in hH], [x.data_ptr() for x in hw], None, bra, ket,
                             [x.data_ptr() for x in hO], [x.data_ptr() for x in hout])
     torch.cuda.synchronize()
-    e2e_elapsed = time.perf_counter() - t0
+    e2e_elapsed = max(time.perf_counter() - t0, 1e-9)
     if dist:
         t = torch.tensor([e2e_elapsed], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_elapsed = float(t.item())
-    e2e_value = world * 3600.0 / (STEPS_PER_RUN * e2e_elapsed / e2e_steps)
-    ns0 = hb[0][0]
+    e2e_value = world * 3600.0 / (STEPS_PER_RUN * e2e_elapsed / e2e_steps) if hb else None
+    ns0 = batches[0][0]
     h2d = sum(8 * n * n for n in ns0) + sum(8 * ns0[b] * ns0[k] for b, k in zip(bra, ket))
     d2h = sum(8 * n for n in ns0) + sum(8 * ns0[b] * ns0[k] for b, k in zip(bra, ket))
     # ---- roofline of the dominant kernel ----
@@ -452,9 +461,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    ap.add_argument("--nmax", type=int, default=4096, help="cap on block sizes (small profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    global NMAX
+    NMAX = args.nmax
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
