@@ -452,6 +452,32 @@ def run_ours(args, rank, world):
     return 0
 
 
+def run_ncu_small(nmax):
+    """Small profiling case (no torch on the GPU): 12 blocks with sizes up to
+    `nmax` and their 72 operators through the host-buffer C ABI, twice."""
+    import nrgb
+    rng = np.random.default_rng(SEED)
+    ns = [int(x) for x in np.linspace(48, nmax, 12)]
+    bra = [k for k in range(len(ns)) for _ in range(NOPS_PER_PAIR)]
+    ket = [(k + 1) % len(ns) for k in range(len(ns)) for _ in range(NOPS_PER_PAIR)]
+    H = []
+    for n in ns:
+        X = rng.standard_normal((n, n))
+        H.append(np.asfortranarray((X + X.T) / 2))
+    O = [np.asfortranarray(rng.standard_normal((ns[b], ns[k]))) for b, k in zip(bra, ket)]
+    W = [np.empty(n) for n in ns]
+    R = [np.empty((ns[b], ns[k]), order="F") for b, k in zip(bra, ket)]
+    ctx = nrgb.Context(0)
+    for _ in range(2):
+        ctx.eig_recalc_step(ns, [h.ctypes.data for h in H], [w.ctypes.data for w in W], None, bra, ket,
+                            [o.ctypes.data for o in O], [r.ctypes.data for r in R])
+    for h, w in zip(H, W):
+        assert abs(np.sum(w) - np.trace(h)) <= 1e-9 * (1 + np.abs(h).sum())
+    ctx.close()
+    print(json.dumps({"ncu_small": nmax, "blocks": ns}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -463,11 +489,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--nmax", type=int, default=4096, help="cap on block sizes (small profiling cases)")
+    ap.add_argument("--ncu-small", type=int, default=0,
+                    help="run only the small profiling case with blocks up to this size (no torch GPU work)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     global NMAX
     NMAX = args.nmax
+    if args.ncu_small:
+        return run_ncu_small(args.ncu_small)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":

@@ -103,7 +103,9 @@ __global__ void __launch_bounds__(NT) gemm_grouped_kernel(const GemmProb* __rest
     if (probs[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
   }
   const GemmProb P = probs[lo];
-  const int t = tile - P.tile0;
+  const int ks = P.ksplit > 1 ? P.ksplit : 1;
+  const int t = (tile - P.tile0) / ks;
+  const int kc = (tile - P.tile0) % ks;
   const int row0 = (t / P.tiles_n) * BM;
   const int col0 = (t % P.tiles_n) * BN;
   const int m = P.m, n = P.n;
@@ -120,25 +122,39 @@ __global__ void __launch_bounds__(NT) gemm_grouped_kernel(const GemmProb* __rest
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-  // Flattened (segment, k-tile) iteration.
-  int s = P.seg0, send = P.seg0 + P.nseg;
-  // skip empty segments
-  while (s < send && segs[s].k <= 0) ++s;
-  if (s < send) {
+  // Flattened (segment, k-tile) iteration over this CTA's share of the K tiles.
+  const int send = P.seg0 + P.nseg;
+  int ktot = 0;
+  for (int q = P.seg0; q < send; ++q) ktot += segs[q].k > 0 ? (segs[q].k + BK - 1) / BK : 0;
+  const int per = (ktot + ks - 1) / ks;
+  const int kt0 = kc * per;
+  int remaining = min(ktot, kt0 + per) - kt0;
+  int s = P.seg0, k0 = 0;
+  {
+    int kt = 0;
+    while (s < send) {
+      const int nt = segs[s].k > 0 ? (segs[s].k + BK - 1) / BK : 0;
+      if (kt + nt > kt0) break;
+      kt += nt;
+      ++s;
+    }
+    k0 = (kt0 - kt) * BK;
+  }
+  if (remaining > 0 && s < send) {
     TileLoader L;
     GemmSeg cur = segs[s];
-    int k0 = 0;
     L.load(cur, k0, row0, col0, m, n, tid);
     L.store(cur, As[0], Bs[0], tid);
     __syncthreads();
     int buf = 0;
     while (true) {
+      --remaining;
       // advance to next (segment, k0)
       GemmSeg nxt = cur;
       int nk0 = k0 + BK;
       int ns = s;
-      bool more = true;
-      if (nk0 >= cur.k) {
+      bool more = remaining > 0;
+      if (more && nk0 >= cur.k) {
         ns = s + 1;
         while (ns < send && segs[ns].k <= 0) ++ns;
         if (ns < send) {
@@ -186,7 +202,8 @@ __global__ void __launch_bounds__(NT) gemm_grouped_kernel(const GemmProb* __rest
         if (c < n) {
           double* dst = P.C + (size_t)c * P.ldc + r;
           const double v = acc[i][j][h];
-          *dst = (beta == 0.0) ? v : v + beta * (*dst);
+          if (ks > 1) atomicAdd(dst, v);
+          else *dst = (beta == 0.0) ? v : v + beta * (*dst);
         }
       }
     }

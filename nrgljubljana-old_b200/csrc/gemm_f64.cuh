@@ -34,10 +34,13 @@ struct GemmProb {
   int seg0, nseg;      // segment range in the segment array
   int tile0;           // first global tile index of this problem
   int tiles_n;         // number of tiles along n
+  int ksplit;          // >1: the K loop is split over this many CTAs per output
+                       // tile, which accumulate with atomics (C must be zero
+                       // on entry and beta is ignored); 0 or 1: no split
 };
 
 // Launch: problems/segments already in device memory.  total_tiles is the
-// sum over problems of ceil(m/BM)*ceil(n/BN).  Returns cudaError_t.
+// sum over problems of ceil(m/BM)*ceil(n/BN)*max(1,ksplit).  Returns cudaError_t.
 cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
                                 int total_tiles, cudaStream_t stream);
 

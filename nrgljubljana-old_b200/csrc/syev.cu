@@ -225,8 +225,8 @@ struct TrdProb {
   double* d;    // n
   double* e;    // n-1
   double* tau;  // n-1
-  double* Vp;   // n x NB panel reflectors (explicit)
-  double* W;    // n x NB
+  double* Vp;   // n x NB panel reflectors, row-major (row i at Vp + i*NB)
+  double* W;    // n x NB, row-major
   double* v;    // n
   double* y;    // n
   double* red;  // 2 slots x (2 + 2*NB)
@@ -240,13 +240,20 @@ __device__ __forceinline__ double ld_volatile(const double* p) {
   return *reinterpret_cast<const volatile double*>(p);
 }
 
+// One panel of NB columns for every problem (cooperative launch).  Per column
+// c three phases separated by grid barriers; every load of data written by
+// other CTAs during the launch bypasses L1 (__ldcg).
+//   1: a = A[c:, c] - V W[c,:]^T - W V[c,:]^T   (also finishes W[:, jj-1])
+//   2: Householder vector v, p = W^T v, q = V^T v
+//   3: y = A22 v - V p - W q  (one warp per column of A22)
 __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __restrict__ probs,
                                                            int nprob, int j0, GridBarrier* bar) {
   extern __shared__ double sm[];
   double* scratch = sm;          // 32
-  double* VWc = sm + 32;         // 2*NB
+  double* VWc = sm + 32;         // 2*NB: row c of V and W
   double* pq = VWc + 2 * NB;     // 2*NB
-  double* vs = pq + 2 * NB;      // n_max
+  double* pqw = pq + 2 * NB;     // (TRD_NT/32) x 2*NB partial p,q
+  double* vs = pqw + (TRD_NT / 32) * 2 * NB;  // n_max
   const unsigned nblocks = gridDim.x;
   const int b = blockIdx.x;
   int lo = 0, hi = nprob - 1;
@@ -259,48 +266,50 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
   const int n = P.n;
   const size_t ld = (size_t)n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nwarps = TRD_NT / 32;
+  constexpr int nwarps = TRD_NT / 32;
+  const int gw = rank * nwarps + warp, tw = P.ncta * nwarps;  // warp index within the problem
 
   for (int jj = 0; jj < NB; ++jj) {
     const int c = j0 + jj;
     const bool act = c < n;
     double* R = P.red + (c & 1) * RED;
     double* Ro = P.red + ((c + 1) & 1) * RED;
-    // ---------------- phase 1: update column c (+ finish W[:, jj-1]) ----------------
-    double tprev = 0.0, a2 = 0.0;
+    // ---------------- phase 1 ----------------
     if (act) {
+      double tprev = 0.0, a2 = 0.0;
       if (jj > 0) {
         tprev = __ldcg(&P.tau[c - 1]);
         a2 = -0.5 * tprev * tprev * ld_volatile(&Ro[1]);
       }
       if (tid < jj) {
         const int k = tid;
-        VWc[k] = __ldcg(&P.Vp[c + k * ld]);
-        VWc[NB + k] = (k == jj - 1) ? tprev * __ldcg(&P.y[c]) + a2 : __ldcg(&P.W[c + k * ld]);
+        VWc[k] = __ldcg(&P.Vp[(size_t)c * NB + k]);
+        VWc[NB + k] = (k == jj - 1) ? tprev * __ldcg(&P.y[c]) + a2 : __ldcg(&P.W[(size_t)c * NB + k]);
       }
       __syncthreads();
-      const int m = n - c;
-      const int chunk = (m + P.ncta - 1) / P.ncta;
-      const int r0 = c + rank * chunk, r1 = min(n, r0 + chunk);
       double ss = 0.0;
-      for (int i = r0 + tid; i < r1; i += TRD_NT) {
-        double a = __ldcg(&P.A[i + c * ld]);
-        if (jj > 0) {
-          const double wl = tprev * __ldcg(&P.y[i]) + a2 * __ldcg(&P.v[i]);
-          P.W[i + (jj - 1) * ld] = wl;
-          for (int k = 0; k < jj - 1; ++k)
-            a -= __ldcg(&P.Vp[i + k * ld]) * VWc[NB + k] + __ldcg(&P.W[i + k * ld]) * VWc[k];
-          a -= __ldcg(&P.Vp[i + (jj - 1) * ld]) * VWc[NB + jj - 1] + wl * VWc[jj - 1];
+      for (int i = c + gw; i < n; i += tw) {
+        double wl = 0.0;
+        if (jj > 0) wl = tprev * __ldcg(&P.y[i]) + a2 * __ldcg(&P.v[i]);
+        double t = 0.0;
+        if (lane < jj) {
+          const double wik = (lane == jj - 1) ? wl : __ldcg(&P.W[(size_t)i * NB + lane]);
+          t = __ldcg(&P.Vp[(size_t)i * NB + lane]) * VWc[NB + lane] + wik * VWc[lane];
         }
-        P.A[i + c * ld] = a;
-        if (i == c) P.d[c] = a;
-        if (i >= c + 2) ss += a * a;
+        t = warp_sum(t);
+        if (lane == 0) {
+          if (jj > 0) P.W[(size_t)i * NB + jj - 1] = wl;
+          const double a = __ldcg(&P.A[i + c * ld]) - t;
+          P.A[i + c * ld] = a;
+          if (i == c) P.d[c] = a;
+          if (i >= c + 2) ss += a * a;
+        }
       }
       ss = block_sum(ss, scratch);
       if (tid == 0 && ss != 0.0) atomicAdd(&R[0], ss);
     }
     grid_barrier(bar, nblocks);
-    // ---------------- phase 2: Householder vector, p = W^T v, q = V^T v ----------------
+    // ---------------- phase 2 ----------------
     if (act && c < n - 1) {
       const double alpha = ld_volatile(&P.A[c + 1 + c * ld]);
       const double xn2 = ld_volatile(&R[0]);
@@ -321,27 +330,35 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
       for (int i = r0 + tid; i < r1; i += TRD_NT) {
         const double vi = (i == c + 1) ? 1.0 : __ldcg(&P.A[i + c * ld]) * scal;
         P.v[i] = vi;
-        P.Vp[i + jj * ld] = vi;
+        P.Vp[(size_t)i * NB + jj] = vi;
         if (i >= c + 2) P.A[i + c * ld] = vi;
       }
       __syncthreads();
-      for (int k = warp; k < jj; k += nwarps) {
+      if (jj > 0) {
         double sp = 0.0, sq = 0.0;
-        for (int i = r0 + lane; i < r1; i += 32) {
+        for (int i = r0 + warp; i < r1; i += nwarps) {
           const double vi = __ldcg(&P.v[i]);
-          sp += __ldcg(&P.W[i + k * ld]) * vi;
-          sq += __ldcg(&P.Vp[i + k * ld]) * vi;
+          if (lane < jj) {
+            sp += __ldcg(&P.W[(size_t)i * NB + lane]) * vi;
+            sq += __ldcg(&P.Vp[(size_t)i * NB + lane]) * vi;
+          }
         }
-        sp = warp_sum(sp);
-        sq = warp_sum(sq);
-        if (lane == 0) {
-          if (sp != 0.0) atomicAdd(&R[2 + k], sp);
-          if (sq != 0.0) atomicAdd(&R[2 + NB + k], sq);
+        pqw[warp * 2 * NB + lane] = sp;
+        pqw[warp * 2 * NB + NB + lane] = sq;
+        __syncthreads();
+        if (tid < jj) {
+          double a = 0.0, bq = 0.0;
+          for (int w = 0; w < nwarps; ++w) {
+            a += pqw[w * 2 * NB + tid];
+            bq += pqw[w * 2 * NB + NB + tid];
+          }
+          if (a != 0.0) atomicAdd(&R[2 + tid], a);
+          if (bq != 0.0) atomicAdd(&R[2 + NB + tid], bq);
         }
       }
     }
     grid_barrier(bar, nblocks);
-    // ---------------- phase 3: y = A22 v - V p - W q (column dots) ----------------
+    // ---------------- phase 3 ----------------
     if (act && c < n - 1) {
       const int m = n - c - 1;
       for (int i = tid; i < m; i += TRD_NT) vs[i] = __ldcg(&P.v[c + 1 + i]);
@@ -350,20 +367,27 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
         pq[NB + tid] = ld_volatile(&R[2 + NB + tid]);
       }
       __syncthreads();
-      const int gw = rank * nwarps + warp, tw = P.ncta * nwarps;
       double yvp = 0.0;
       for (int j = c + 1 + gw; j < n; j += tw) {
         const double* col = P.A + (size_t)j * ld + (c + 1);
-        double s0 = 0.0, s1 = 0.0;
+        double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         int i = lane;
-        for (; i + 32 < m; i += 64) {
-          s0 += __ldcg(&col[i]) * vs[i];
-          s1 += __ldcg(&col[i + 32]) * vs[i + 32];
+        for (; i + 480 < m; i += 512) {
+          double x[16];
+#pragma unroll
+          for (int u = 0; u < 16; ++u) x[u] = __ldcg(&col[i + 32 * u]);
+#pragma unroll
+          for (int u = 0; u < 16; ++u) s[u & 7] += x[u] * vs[i + 32 * u];
         }
-        if (i < m) s0 += __ldcg(&col[i]) * vs[i];
+        for (; i + 224 < m; i += 256) {
+#pragma unroll
+          for (int u = 0; u < 8; ++u) s[u] += __ldcg(&col[i + 32 * u]) * vs[i + 32 * u];
+        }
+        for (; i < m; i += 32) s[0] += __ldcg(&col[i]) * vs[i];
         double corr = 0.0;
-        if (lane < jj) corr = __ldcg(&P.Vp[j + lane * ld]) * pq[lane] + __ldcg(&P.W[j + lane * ld]) * pq[NB + lane];
-        const double yj = warp_sum(s0 + s1 - corr);
+        if (lane < jj)
+          corr = __ldcg(&P.Vp[(size_t)j * NB + lane]) * pq[lane] + __ldcg(&P.W[(size_t)j * NB + lane]) * pq[NB + lane];
+        const double yj = warp_sum(((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7])) - corr);
         if (lane == 0) {
           P.y[j] = yj;
           yvp += yj * vs[j - c - 1];
@@ -382,7 +406,8 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
     const int m = n - c - 1;
     const int chunk = (m + P.ncta - 1) / P.ncta;
     const int r0 = c + 1 + rank * chunk, r1 = min(n, r0 + chunk);
-    for (int i = r0 + tid; i < r1; i += TRD_NT) P.W[i + (NB - 1) * ld] = tc * __ldcg(&P.y[i]) + a2 * __ldcg(&P.v[i]);
+    for (int i = r0 + tid; i < r1; i += TRD_NT)
+      P.W[(size_t)i * NB + NB - 1] = tc * __ldcg(&P.y[i]) + a2 * __ldcg(&P.v[i]);
   }
 }
 
@@ -483,6 +508,7 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
   const int n = P.n, lo = N.lo, mid = N.mid, hi = N.hi;
   const int n1 = mid - lo, np = hi - lo;
   const size_t ld = (size_t)n;
+  (void)ld;
   const int tid = threadIdx.x;
   const double beta = P.e[mid - 1];
   const double rho = 2.0 * fabs(beta);
@@ -519,12 +545,6 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
     zmax = fmax(zmax, fabs(zi));
   }
   __syncthreads();
-  // copy Q columns in sorted order into W1 (sub-block [lo,hi) x [lo,hi))
-  for (int idx = tid; idx < np * np; idx += DC_NT) {
-    const int r = idx % np, pcol = idx / np;
-    const int s = P.src[lo + pcol];
-    P.W1[(size_t)(lo + r) + (size_t)(lo + pcol) * ld] = P.Q[(size_t)(lo + r) + (size_t)(lo + s) * ld];
-  }
   // block max of |d| and |z|
   {
     // reuse block_sum machinery for max via two passes
@@ -598,20 +618,7 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
     P.nrot[lo] = nr;
   }
   __syncthreads();
-  const int k = sk[0], nr = sk[1];
-  // apply rotations in order to W1 columns
-  for (int r = 0; r < nr; ++r) {
-    const int pc = P.rotp[lo + r], jc = P.rotj[lo + r];
-    const double c = P.rotc[lo + r], s = P.rots[lo + r];
-    double* cp = P.W1 + (size_t)(lo + pc) * ld + lo;
-    double* cj = P.W1 + (size_t)(lo + jc) * ld + lo;
-    for (int i = tid; i < np; i += DC_NT) {
-      const double x = cp[i], y = cj[i];
-      cp[i] = c * x + s * y;
-      cj[i] = c * y - s * x;
-    }
-    __syncthreads();
-  }
+  const int k = sk[0];
   // compaction targets: nondeflated first (in order), then deflated (in order)
   if (tid == 0) {
     int kk = 0, dd = 0;
@@ -641,12 +648,6 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
       P.dD[lo + a] = P.zhat[lo + a];
     }
   }
-  // compact columns into Q[lo:hi, lo + a]
-  for (int idx = tid; idx < np * np; idx += DC_NT) {
-    const int r = idx % np, a = idx / np;
-    const int j = P.rank[lo + a];
-    P.Q[(size_t)(lo + r) + (size_t)(lo + a) * ld] = P.W1[(size_t)(lo + r) + (size_t)(lo + j) * ld];
-  }
   // GEMM descriptor: W1[lo:hi, lo:lo+k] = Q[lo:hi, lo:lo+k] * U[lo:lo+k, lo:lo+k]
   if (tid == 0) {
     GemmProb g = gprob[blockIdx.x];  // tile0/tiles_n preset by the host
@@ -669,11 +670,39 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
   }
 }
 
-// Secular equation roots.  One thread per root (grid: nodes x rows).
-__global__ void dc_secular_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes,
-                                  int maxnp, int* fail) {
+// Merge, step 2 (one thread per row of the node's block): gather the child
+// eigenvector columns in sorted order, apply the deflation rotations in
+// order, and compact (nondeflated first) into Q[lo:hi, lo:hi].  Rows are
+// independent, so the sequential rotation list costs O(nrot) per row.
+__global__ void dc_permute_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes) {
   const int node = blockIdx.y;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const DcNode N = nodes[node];
+  const DcProb P = probs[N.prob];
+  const int lo = N.lo, np = N.hi - N.lo;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= np) return;
+  const size_t ld = (size_t)P.n;
+  double* w1 = P.W1 + (size_t)(lo + r) + (size_t)lo * ld;   // row r, columns lo..hi
+  const double* q = P.Q + (size_t)(lo + r) + (size_t)lo * ld;
+  for (int pos = 0; pos < np; ++pos) w1[(size_t)pos * ld] = q[(size_t)P.src[lo + pos] * ld];
+  const int nr = P.nrot[lo];
+  for (int t = 0; t < nr; ++t) {
+    const size_t pc = (size_t)P.rotp[lo + t] * ld, jc = (size_t)P.rotj[lo + t] * ld;
+    const double c = P.rotc[lo + t], s = P.rots[lo + t];
+    const double x = w1[pc], y = w1[jc];
+    w1[pc] = c * x + s * y;
+    w1[jc] = c * y - s * x;
+  }
+  double* qo = P.Q + (size_t)(lo + r) + (size_t)lo * ld;
+  for (int a = 0; a < np; ++a) qo[(size_t)a * ld] = w1[(size_t)P.rank[lo + a] * ld];
+}
+
+// Secular equation roots, one warp per root: lanes share the pole sums.
+__global__ void dc_secular_warp_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes,
+                                       int* fail) {
+  const int node = blockIdx.y;
+  const int j = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   const DcNode N = nodes[node];
   const DcProb P = probs[N.prob];
   const int lo = N.lo;
@@ -682,15 +711,13 @@ __global__ void dc_secular_kernel(const DcProb* __restrict__ probs, const DcNode
   const double* d = P.ds + lo;
   const double* z = P.zs + lo;
   const double rho = P.rho[lo];
-  double zz = 0.0;
-  // origin choice
   int o;
   double tlo, thi;
   if (j < k - 1) {
-    const double gap = d[j + 1] - d[j];
-    const double mid = 0.5 * gap;  // relative to d[j]
-    double f = 1.0;
-    for (int i = 0; i < k; ++i) f += rho * z[i] * z[i] / ((d[i] - d[j]) - mid);
+    const double mid = 0.5 * (d[j + 1] - d[j]);
+    double f = 0.0;
+    for (int i = lane; i < k; i += 32) f += z[i] * z[i] / ((d[i] - d[j]) - mid);
+    f = 1.0 + rho * warp_sum(f);
     if (f >= 0.0) {
       o = j;
       tlo = 0.0;
@@ -701,20 +728,21 @@ __global__ void dc_secular_kernel(const DcProb* __restrict__ probs, const DcNode
       thi = 0.0;
     }
   } else {
-    for (int i = 0; i < k; ++i) zz += z[i] * z[i];
+    double zz = 0.0;
+    for (int i = lane; i < k; i += 32) zz += z[i] * z[i];
+    zz = warp_sum(zz);
     o = j;
     tlo = 0.0;
     thi = rho * zz;
   }
   const double dorig = d[o];
-  // poles relative to origin: delta_i = d[i] - d[o]; interval poles at j and j+1
   const double dL = d[j] - dorig;
   const double dR = (j < k - 1) ? d[j + 1] - dorig : 0.0;
   double t = 0.5 * (tlo + thi);
   bool done = false;
   for (int it = 0; it < 400; ++it) {
     double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0;
-    for (int i = 0; i < k; ++i) {
+    for (int i = lane; i < k; i += 32) {
       const double del = (d[i] - dorig) - t;
       const double q = z[i] / del;
       if (i <= j) {
@@ -725,39 +753,40 @@ __global__ void dc_secular_kernel(const DcProb* __restrict__ probs, const DcNode
         dphi += q * q;
       }
     }
+    psi = warp_sum(psi);
+    dpsi = warp_sum(dpsi);
+    phi = warp_sum(phi);
+    dphi = warp_sum(dphi);
+    // all lanes hold identical sums and run the same scalar update
     const double f = 1.0 + rho * (psi + phi);
     if (f == 0.0) {
       done = true;
       break;
     }
     if (f < 0.0) tlo = t; else thi = t;
-    // two-pole (one-pole for the last root) rational model step
     double tn;
     const double DL = dL - t;
     if (j < k - 1) {
       const double DR = dR - t;
-      const double s = rho * dpsi * DL * DL, S = rho * dphi * DR * DR;
-      const double cc = f - s / DL - S / DR;
-      const double bb = cc * (DL + DR) + s + S;
+      const double sL = rho * dpsi * DL * DL, sR = rho * dphi * DR * DR;
+      const double cc = f - sL / DL - sR / DR;
+      const double bb = cc * (DL + DR) + sL + sR;
       const double c0 = DL * DR * f;
       double eta;
       if (cc == 0.0) {
         eta = c0 / bb;
       } else {
-        const double disc = fmax(bb * bb - 4.0 * cc * c0, 0.0);
-        const double sq = sqrt(disc);
-        const double q = (bb >= 0.0) ? bb + sq : bb - sq;
-        const double e1 = q / (2.0 * cc), e2 = 2.0 * c0 / q;
+        const double sq = sqrt(fmax(bb * bb - 4.0 * cc * c0, 0.0));
+        const double qq = (bb >= 0.0) ? bb + sq : bb - sq;
+        const double e1 = qq / (2.0 * cc), e2 = 2.0 * c0 / qq;
         eta = (e1 > DL && e1 < DR) ? e1 : e2;
       }
       tn = t + eta;
     } else {
-      const double s = rho * dpsi * DL * DL;
-      const double cc = f - s / DL;
-      tn = (cc > 0.0) ? t + DL + s / cc : 0.5 * (tlo + thi);
+      const double sL = rho * dpsi * DL * DL;
+      const double cc = f - sL / DL;
+      tn = (cc > 0.0) ? t + DL + sL / cc : 0.5 * (tlo + thi);
     }
-    // converged: the model step is below the resolution of t, or f is below
-    // the rounding error of its own evaluation
     if (fabs(tn - t) <= 2.0 * EPS * fabs(t) || fabs(f) <= EPS * (8.0 + 8.0 * rho * (phi - psi))) {
       done = true;
       break;
@@ -770,10 +799,11 @@ __global__ void dc_secular_kernel(const DcProb* __restrict__ probs, const DcNode
     }
     t = tn;
   }
-  // a bracket that is still wide after the iteration limit is a real failure
-  if (!done && thi - tlo > 1e-10 * fmax(fabs(tlo), fabs(thi))) atomicExch(fail, 2);
-  P.tau[lo + j] = t;
-  P.orig[lo + j] = o;
+  if (lane == 0) {
+    if (!done && thi - tlo > 1e-10 * fmax(fabs(tlo), fabs(thi))) atomicExch(fail, 2);
+    P.tau[lo + j] = t;
+    P.orig[lo + j] = o;
+  }
 }
 
 // Loewner z-hat.  One thread per i.
@@ -930,9 +960,10 @@ struct GemmBatch {
   std::vector<GemmProb> probs;
   std::vector<GemmSeg> segs;
   int tiles = 0;
-  void add(double* C, int ldc, int m, int n, double beta, const std::vector<GemmSeg>& ss) {
+  void add(double* C, int ldc, int m, int n, double beta, const std::vector<GemmSeg>& ss, int ksplit = 1) {
     if (m <= 0 || n <= 0) return;
     GemmProb p{};
+    p.ksplit = ksplit;
     p.C = C;
     p.ldc = ldc;
     p.m = m;
@@ -942,7 +973,7 @@ struct GemmBatch {
     p.nseg = (int)ss.size();
     p.tile0 = tiles;
     p.tiles_n = ceil_div(n, GEMM_BN);
-    tiles += ceil_div(m, GEMM_BM) * p.tiles_n;
+    tiles += ceil_div(m, GEMM_BM) * p.tiles_n * std::max(1, ksplit);
     segs.insert(segs.end(), ss.begin(), ss.end());
     probs.push_back(p);
   }
@@ -1005,6 +1036,10 @@ size_t SyevBatched::workspace_bytes(const std::vector<int>& ns) {
     pl.add<double>((size_t)NBB * n * 2);
   }
   pl.add<double>(64 * 1024);
+  int nmx = 0;
+  for (int n : ns) nmx = std::max(nmx, n);
+  // per-panel launch descriptors
+  pl.add<char>((size_t)(nmx / NB + 2) * (ns.size() * (sizeof(TrdProb) + 2 * sizeof(GemmSeg) + sizeof(GemmProb)) + 2048));
   return pl.bytes + (size_t)ns.size() * 4096 + (1 << 20);
 }
 
@@ -1118,65 +1153,74 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     }
     // ---------------- 1) tridiagonalisation ----------------
     {
-      const size_t smem = (size_t)(32 + 4 * NB + nmax) * sizeof(double);
+      const size_t smem = (size_t)(32 + 4 * NB + (TRD_NT / 32) * 2 * NB + nmax) * sizeof(double);
       NRGB_CUDA(cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
       int per_sm = 0;
       NRGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_NT, smem));
       per_sm = std::max(1, std::min(per_sm, 4));
       const int cap = per_sm * sms_;
-      // sub-batches of at most `cap` problems
-      for (int s0 = 0; s0 < nbig; s0 += cap) {
-        const int s1 = std::min(nbig, s0 + cap);
-        const int cnt = s1 - s0;
-        // CTA allocation proportional to n^2
-        double wsum = 0.0;
-        int nm = 0;
-        for (int b = s0; b < s1; ++b) {
-          wsum += (double)tp[b].n * tp[b].n;
-          nm = std::max(nm, tp[b].n);
-        }
-        int extra = cap - cnt;
-        int tot = 0;
-        std::vector<TrdProb> sub(tp.begin() + s0, tp.begin() + s1);
-        for (int b = 0; b < cnt; ++b) {
-          const double w = (double)sub[b].n * sub[b].n / wsum;
-          int nc = 1 + (int)floor(w * extra);
-          nc = std::min(nc, std::max(1, sub[b].n / 16));
-          sub[b].cta0 = tot;
-          sub[b].ncta = nc;
-          tot += nc;
-        }
-        TrdProb* d_tp = arena_.alloc_n<TrdProb>(sub.size());
-        NRGB_CUDA(cudaMemcpyAsync(d_tp, sub.data(), sub.size() * sizeof(TrdProb), cudaMemcpyHostToDevice, st));
-        for (int j0 = 0; j0 < nm; j0 += NB) {
+      // One cooperative launch per panel of NB columns.  All problems advance
+      // column by column in lockstep, so a column costs the maximum over
+      // problems of (trailing size)^2 / CTAs: the CTAs of each launch are
+      // shared among the problems that still have columns left in
+      // proportion to (n - j0)^2, and finished problems get none.
+      std::vector<int> order(nbig);
+      std::iota(order.begin(), order.end(), 0);
+      for (int j0 = 0; j0 < nmax; j0 += NB) {
+        std::vector<int> act;
+        for (int b : order)
+          if (tp[b].n > j0) act.push_back(b);
+        for (size_t s0 = 0; s0 < act.size(); s0 += cap) {
+          const size_t s1 = std::min(act.size(), s0 + cap);
+          const int cnt = (int)(s1 - s0);
+          double wsum = 0.0;
+          for (size_t q = s0; q < s1; ++q) wsum += pow((double)(tp[act[q]].n - j0), 2.0);
+          const int extra = cap - cnt;
+          std::vector<TrdProb> sub;
+          int tot = 0;
+          for (size_t q = s0; q < s1; ++q) {
+            TrdProb t = tp[act[q]];
+            const double w = pow((double)(t.n - j0), 2.0) / wsum;
+            int nc = 1 + (int)floor(w * extra);
+            nc = std::min(nc, std::max(1, (t.n - j0) / 8));
+            t.cta0 = tot;
+            t.ncta = nc;
+            tot += nc;
+            sub.push_back(t);
+          }
+          TrdProb* d_tp = arena_.alloc_n<TrdProb>(sub.size());
+          NRGB_CUDA(cudaMemcpyAsync(d_tp, sub.data(), sub.size() * sizeof(TrdProb), cudaMemcpyHostToDevice, st));
           NRGB_CUDA(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned int), st));
           int np_ = cnt;
-          void* args[] = {(void*)&d_tp, (void*)&np_, (void*)&j0, (void*)&d_bar_};
+          int j0_ = j0;
+          void* args[] = {(void*)&d_tp, (void*)&np_, (void*)&j0_, (void*)&d_bar_};
           NRGB_LAUNCH("trd_panel", st,
                       NRGB_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, dim3(tot), dim3(TRD_NT),
                                                             args, smem, st)));
           ++launches_;
           // trailing update A22 -= V W^T + W V^T for rows/cols >= j0+NB
           GemmBatch gb;
-          for (int b = 0; b < cnt; ++b) {
-            const int n = sub[b].n;
+          for (const TrdProb& t : sub) {
+            const int n = t.n;
             const int r0 = j0 + NB;
             if (r0 >= n) continue;
             const int m2 = n - r0;
+            // Vp, W are row-major n x NB: as column-major matrices they are
+            // NB x n with ld NB, so op(A) = stored^T and op(B) = stored.
             GemmSeg s1{}, s2{};
-            s1.A = sub[b].Vp + r0;
-            s1.lda = n;
-            s1.B = sub[b].W + r0;
-            s1.ldb = n;
+            s1.A = t.Vp + (size_t)r0 * NB;
+            s1.lda = NB;
+            s1.B = t.W + (size_t)r0 * NB;
+            s1.ldb = NB;
             s1.k = NB;
-            s1.transA = 0;
-            s1.transB = 1;
+            s1.transA = 1;
+            s1.transB = 0;
             s1.alpha = -1.0;
             s2 = s1;
-            s2.A = sub[b].W + r0;
-            s2.B = sub[b].Vp + r0;
-            gb.add(sub[b].A + r0 + (size_t)r0 * n, n, m2, m2, 1.0, {s1, s2});
+            s2.A = t.W + (size_t)r0 * NB;
+            s2.B = t.Vp + (size_t)r0 * NB;
+            gb.add(t.A + r0 + (size_t)r0 * n, n, m2, m2, 1.0, {s1, s2});
           }
           if (!gb.empty()) {
             GemmProb* d_gp = arena_.alloc_n<GemmProb>(gb.probs.size());
@@ -1233,7 +1277,10 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         NRGB_LAUNCH("dc_prep", st, dc_prep_kernel<<<nn, DC_NT, 0, st>>>(d_dp, d_nodes, d_gp, d_gs));
         NRGB_CUDA(cudaGetLastError());
         dim3 g1(ceil_div(maxnp, 128), nn);
-        NRGB_LAUNCH("dc_secular", st, dc_secular_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes, maxnp, d_err_ + 2));
+        NRGB_LAUNCH("dc_permute", st, dc_permute_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
+        NRGB_CUDA(cudaGetLastError());
+        dim3 gw(ceil_div(maxnp, 8), nn);
+        NRGB_LAUNCH("dc_secular", st, dc_secular_warp_kernel<<<gw, 256, 0, st>>>(d_dp, d_nodes, d_err_ + 2));
         NRGB_CUDA(cudaGetLastError());
         NRGB_LAUNCH("dc_lowner", st, dc_lowner_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
@@ -1248,7 +1295,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         NRGB_CUDA(cudaGetLastError());
         NRGB_LAUNCH("dc_copy", st, dc_copy_kernel<<<g3, 128, 0, st>>>(d_dp, d_nodes, 1));
         NRGB_CUDA(cudaGetLastError());
-        launches_ += 8;
+        launches_ += 9;
       }
       // problems that are a single leaf already have D, Q in place
     }
@@ -1282,7 +1329,9 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           s.transB = 0;
           s.k = mrows;
           s.alpha = 1.0;
-          g1.add(P.G, NBB, NBB, NBB, 0.0, {s});
+          // one output tile, K = mrows: split the K loop so that many CTAs work
+          NRGB_CUDA(cudaMemsetAsync(P.G, 0, sizeof(double) * NBB * NBB, st));
+          g1.add(P.G, NBB, NBB, NBB, 0.0, {s}, std::max(1, std::min(64, mrows / 256)));
         }
         {
           GemmProb* d_gp = arena_.alloc_n<GemmProb>(g1.probs.size());
@@ -1310,7 +1359,8 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           s.transB = 0;
           s.k = mrows;
           s.alpha = 1.0;
-          gx.add(P.X, NBB, NBB, n, 0.0, {s});
+          NRGB_CUDA(cudaMemsetAsync(P.X, 0, sizeof(double) * NBB * n, st));
+          gx.add(P.X, NBB, NBB, n, 0.0, {s}, std::max(1, std::min(16, mrows / 512)));
           GemmSeg t{};
           t.A = P.T;
           t.lda = NBB;
