@@ -340,9 +340,11 @@ def run_ours(args, rank, world):
     step_ms = [a.elapsed_time(b) for a, b in evs]
     launches, _ = ctx.kernel_stats("*")
     kstats = {}
-    for name in ("trd_panel", "gemm_f64", "dc_prep", "dc_secular", "dc_lowner", "dc_vectors", "dc_rank",
-                 "dc_copy", "dc_leaf", "bt_T", "bt_buildV", "syev_small"):
-        kstats[name] = ctx.kernel_stats(name)
+    for name in ("trd_panel", "gemm_f64*", "dc_prep", "dc_permute", "dc_secular", "dc_lowner", "dc_vectors",
+                 "dc_rank", "dc_copy", "dc_leaf", "bt_T", "bt_buildV", "syev_small"):
+        kstats[name.rstrip("*")] = ctx.kernel_stats(name)
+    gemm_sites = {k: ctx.kernel_stats(k) for k in ("gemm_f64_trailing", "gemm_f64_dc", "gemm_f64_bt",
+                                                   "gemm_f64_recalc")}
     ctx.profile(False)
     clk = clocks.stop()
     if dist:
@@ -399,6 +401,8 @@ def run_ours(args, rank, world):
     name, (nl, ms) = top
     steps_ns = [batches[(args.warmup + i) % nbatch][0] for i in range(args.steps)]
     roof = None
+    if name == "gemm_f64":
+        name = "gemm_f64"
     if name == "trd_panel" and nl:
         bytes_total = sum(trd_panel_step_bytes(ns) for ns in steps_ns)
         per_launch_bytes = bytes_total / nl
@@ -432,7 +436,8 @@ def run_ours(args, rank, world):
             "e2e": {"value": e2e_value, "unit": "runs/hour", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "roofline": roof,
-            "kernel_time_share": {k: round(v, 4) for k, v in share.items() if v > 0.001}}
+            "kernel_time_share": {k: round(v, 4) for k, v in share.items() if v > 0.001},
+            "gemm_ms_per_step_by_site": {k: round(v[1] / args.steps, 3) for k, v in gemm_sites.items()}}
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         t, frac = cpu_step(0, threads, budget_s=args.cpu_budget)

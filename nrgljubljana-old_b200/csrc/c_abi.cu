@@ -126,7 +126,7 @@ int nrgb_gemm_grouped_dev(nrgb_ctx* ctx, int nout, const nrgb_gemm_out* outs, in
       const nrgb_gemm_term& x = terms[t];
       S[t] = nrgb::GemmSeg{x.a, x.b, x.lda, x.ldb, x.k, x.trans_a, x.trans_b, x.alpha};
     }
-    int tiles = 0;
+    int tiles = 0, stiles = 0;
     for (int o = 0; o < nout; ++o) {
       const nrgb_gemm_out& y = outs[o];
       if (y.m <= 0 || y.n <= 0) continue;
@@ -139,9 +139,7 @@ int nrgb_gemm_grouped_dev(nrgb_ctx* ctx, int nout, const nrgb_gemm_out* outs, in
       p.beta = y.beta;
       p.seg0 = y.term0;
       p.nseg = y.nterms;
-      p.tile0 = tiles;
-      p.tiles_n = (y.n + nrgb::GEMM_BN - 1) / nrgb::GEMM_BN;
-      tiles += ((y.m + nrgb::GEMM_BM - 1) / nrgb::GEMM_BM) * p.tiles_n;
+      nrgb::gemm_assign_tiles(p, tiles, stiles);
       P.push_back(p);
     }
     if (P.empty()) return;
@@ -153,7 +151,7 @@ int nrgb_gemm_grouped_dev(nrgb_ctx* ctx, int nout, const nrgb_gemm_out* outs, in
     auto* dS = ctx->scratch.alloc_n<nrgb::GemmSeg>(S.size());
     NRGB_CUDA(cudaMemcpyAsync(dP, P.data(), P.size() * sizeof(nrgb::GemmProb), cudaMemcpyHostToDevice, st));
     NRGB_CUDA(cudaMemcpyAsync(dS, S.data(), S.size() * sizeof(nrgb::GemmSeg), cudaMemcpyHostToDevice, st));
-    NRGB_CUDA(nrgb::gemm_grouped_launch(dP, (int)P.size(), dS, tiles, st));
+    NRGB_CUDA(nrgb::gemm_grouped_launch(dP, (int)P.size(), dS, tiles, st, "gemm_f64", stiles));
     NRGB_CUDA(cudaStreamSynchronize(st));
   });
 }
@@ -164,9 +162,9 @@ void recalc_pairs(nrgb_ctx* ctx, int nops, const int* n, const int* bra, const i
                   const double* const* op, double* const* out, nrgb::DeviceArena& scr, cudaStream_t st) {
   std::vector<nrgb::GemmProb> p1, p2;
   std::vector<nrgb::GemmSeg> s1, s2;
-  int t1 = 0, t2 = 0;
-  auto add = [](std::vector<nrgb::GemmProb>& P, std::vector<nrgb::GemmSeg>& S, int& tiles, double* C, int m,
-                int nn, const nrgb::GemmSeg& g) {
+  int t1 = 0, t2 = 0, u1 = 0, u2 = 0;
+  auto add = [](std::vector<nrgb::GemmProb>& P, std::vector<nrgb::GemmSeg>& S, int& tiles, int& stiles,
+                double* C, int m, int nn, const nrgb::GemmSeg& g) {
     nrgb::GemmProb q{};
     q.C = C;
     q.ldc = m;
@@ -175,9 +173,7 @@ void recalc_pairs(nrgb_ctx* ctx, int nops, const int* n, const int* bra, const i
     q.beta = 0.0;
     q.seg0 = (int)S.size();
     q.nseg = 1;
-    q.tile0 = tiles;
-    q.tiles_n = (nn + nrgb::GEMM_BN - 1) / nrgb::GEMM_BN;
-    tiles += ((m + nrgb::GEMM_BM - 1) / nrgb::GEMM_BM) * q.tiles_n;
+    nrgb::gemm_assign_tiles(q, tiles, stiles);
     P.push_back(q);
     S.push_back(g);
   };
@@ -185,8 +181,8 @@ void recalc_pairs(nrgb_ctx* ctx, int nops, const int* n, const int* bra, const i
     const int nb = n[bra[o]], nk = n[ket[o]];
     if (nb <= 0 || nk <= 0) continue;
     double* T = scr.alloc_n<double>((size_t)nb * nk);
-    add(p1, s1, t1, T, nb, nk, nrgb::GemmSeg{op[o], Z[ket[o]], nb, nk, nk, 0, 0, 1.0});
-    add(p2, s2, t2, out[o], nb, nk, nrgb::GemmSeg{Z[bra[o]], T, nb, nb, nb, 1, 0, 1.0});
+    add(p1, s1, t1, u1, T, nb, nk, nrgb::GemmSeg{op[o], Z[ket[o]], nb, nk, nk, 0, 0, 1.0});
+    add(p2, s2, t2, u2, out[o], nb, nk, nrgb::GemmSeg{Z[bra[o]], T, nb, nb, nb, 1, 0, 1.0});
   }
   if (p1.empty()) return;
   auto* d1 = scr.alloc_n<nrgb::GemmProb>(p1.size());
@@ -197,8 +193,8 @@ void recalc_pairs(nrgb_ctx* ctx, int nops, const int* n, const int* bra, const i
   NRGB_CUDA(cudaMemcpyAsync(e1, s1.data(), s1.size() * sizeof(s1[0]), cudaMemcpyHostToDevice, st));
   NRGB_CUDA(cudaMemcpyAsync(d2, p2.data(), p2.size() * sizeof(p2[0]), cudaMemcpyHostToDevice, st));
   NRGB_CUDA(cudaMemcpyAsync(e2, s2.data(), s2.size() * sizeof(s2[0]), cudaMemcpyHostToDevice, st));
-  NRGB_CUDA(nrgb::gemm_grouped_launch(d1, (int)p1.size(), e1, t1, st));
-  NRGB_CUDA(nrgb::gemm_grouped_launch(d2, (int)p2.size(), e2, t2, st));
+  NRGB_CUDA(nrgb::gemm_grouped_launch(d1, (int)p1.size(), e1, t1, st, "gemm_f64_recalc", u1));
+  NRGB_CUDA(nrgb::gemm_grouped_launch(d2, (int)p2.size(), e2, t2, st, "gemm_f64_recalc", u2));
 }
 
 size_t recalc_scratch(int nops, const int* n, const int* bra, const int* ket) {

@@ -37,12 +37,22 @@ struct GemmProb {
   int ksplit;          // >1: the K loop is split over this many CTAs per output
                        // tile, which accumulate with atomics (C must be zero
                        // on entry and beta is ignored); 0 or 1: no split
+  int stile0;          // first global 128x128 tile index (large-tile kernel)
+  int stiles_n;        // number of 128x128 tiles along n
 };
+
+// Fill tile0/tiles_n/stile0/stiles_n of `p` (m, n, ksplit set) and advance
+// the running tile counters of a launch.
+void gemm_assign_tiles(GemmProb& p, int& tiles, int& stiles);
 
 // Launch: problems/segments already in device memory.  total_tiles is the
 // sum over problems of ceil(m/BM)*ceil(n/BN)*max(1,ksplit).  Returns cudaError_t.
+// `tag` names the call site in the launch accounting (KernelStats).
+// total_stiles > 0 allows the 128x128-tile kernel, chosen when the launch's
+// problems are large enough that the bigger tiles waste little work.
 cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
-                                int total_tiles, cudaStream_t stream);
+                                int total_tiles, cudaStream_t stream, const char* tag = "gemm_f64",
+                                int total_stiles = 0);
 
 // Same launch without the library's launch accounting (no host bookkeeping,
 // no events): used by the allocation-free entry point.

@@ -74,12 +74,19 @@ void KernelStats::settle() {
 void KernelStats::query(const char* name, long* launches, double* ms) {
   settle();
   const bool all = strcmp(name, "*") == 0;
+  const size_t len = strlen(name);
+  const bool prefix = len > 1 && name[len - 1] == '*';
+  auto match = [&](const std::string& k) {
+    if (all) return true;
+    if (prefix) return k.compare(0, len - 1, name, len - 1) == 0;
+    return k == name;
+  };
   long n = 0;
   double t = 0;
   for (auto& c : counts_)
-    if (all || c.first == name) n += c.second;
+    if (match(c.first)) n += c.second;
   for (auto& m : ms_)
-    if (all || m.first == name) t += m.second;
+    if (match(m.first)) t += m.second;
   if (launches) *launches = n;
   if (ms) *ms = t;
 }

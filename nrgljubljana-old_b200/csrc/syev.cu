@@ -230,6 +230,7 @@ struct TrdProb {
   double* v;    // n
   double* y;    // n
   double* red;  // 2 slots x (2 + 2*NB)
+  GridBarrier* bar;  // this problem's barrier: only its own CTAs synchronise
   int n;
   int cta0, ncta;
 };
@@ -247,14 +248,13 @@ __device__ __forceinline__ double ld_volatile(const double* p) {
 //   2: Householder vector v, p = W^T v, q = V^T v
 //   3: y = A22 v - V p - W q  (one warp per column of A22)
 __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __restrict__ probs,
-                                                           int nprob, int j0, GridBarrier* bar) {
+                                                           int nprob, int j0, int* fail) {
   extern __shared__ double sm[];
   double* scratch = sm;          // 32
   double* VWc = sm + 32;         // 2*NB: row c of V and W
   double* pq = VWc + 2 * NB;     // 2*NB
   double* pqw = pq + 2 * NB;     // (TRD_NT/32) x 2*NB partial p,q
   double* vs = pqw + (TRD_NT / 32) * 2 * NB;  // n_max
-  const unsigned nblocks = gridDim.x;
   const int b = blockIdx.x;
   int lo = 0, hi = nprob - 1;
   while (lo < hi) {
@@ -263,6 +263,10 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
   }
   const TrdProb P = probs[lo];
   const int rank = b - P.cta0;
+  // Problems are independent: each synchronises only its own CTAs, so a
+  // small problem does not wait for a large one inside a panel.
+  GridBarrier* bar = P.bar;
+  const unsigned nblocks = (unsigned)P.ncta;
   const int n = P.n;
   const size_t ld = (size_t)n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -409,6 +413,8 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
     for (int i = r0 + tid; i < r1; i += TRD_NT)
       P.W[(size_t)i * NB + NB - 1] = tc * __ldcg(&P.y[i]) + a2 * __ldcg(&P.v[i]);
   }
+  // a barrier that gave up is reported to the host (the barriers are reset per launch)
+  if (tid == 0 && *reinterpret_cast<volatile int*>(&bar->error)) atomicExch(fail, 1);
 }
 
 // --------------------------------------------------------------------------
@@ -959,7 +965,7 @@ inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 struct GemmBatch {
   std::vector<GemmProb> probs;
   std::vector<GemmSeg> segs;
-  int tiles = 0;
+  int tiles = 0, stiles = 0;
   void add(double* C, int ldc, int m, int n, double beta, const std::vector<GemmSeg>& ss, int ksplit = 1) {
     if (m <= 0 || n <= 0) return;
     GemmProb p{};
@@ -971,9 +977,7 @@ struct GemmBatch {
     p.beta = beta;
     p.seg0 = (int)segs.size();
     p.nseg = (int)ss.size();
-    p.tile0 = tiles;
-    p.tiles_n = ceil_div(n, GEMM_BN);
-    tiles += ceil_div(m, GEMM_BM) * p.tiles_n * std::max(1, ksplit);
+    gemm_assign_tiles(p, tiles, stiles);
     segs.insert(segs.end(), ss.begin(), ss.end());
     probs.push_back(p);
   }
@@ -1167,6 +1171,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       // proportion to (n - j0)^2, and finished problems get none.
       std::vector<int> order(nbig);
       std::iota(order.begin(), order.end(), 0);
+      GridBarrier* bars = arena_.alloc_n<GridBarrier>(nbig);
       for (int j0 = 0; j0 < nmax; j0 += NB) {
         std::vector<int> act;
         for (int b : order)
@@ -1179,8 +1184,10 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           const int extra = cap - cnt;
           std::vector<TrdProb> sub;
           int tot = 0;
+          NRGB_CUDA(cudaMemsetAsync(bars, 0, sizeof(GridBarrier) * nbig, st));
           for (size_t q = s0; q < s1; ++q) {
             TrdProb t = tp[act[q]];
+            t.bar = bars + act[q];
             const double w = pow((double)(t.n - j0), 2.0) / wsum;
             int nc = 1 + (int)floor(w * extra);
             nc = std::min(nc, std::max(1, (t.n - j0) / 8));
@@ -1191,10 +1198,10 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           }
           TrdProb* d_tp = arena_.alloc_n<TrdProb>(sub.size());
           NRGB_CUDA(cudaMemcpyAsync(d_tp, sub.data(), sub.size() * sizeof(TrdProb), cudaMemcpyHostToDevice, st));
-          NRGB_CUDA(cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned int), st));
           int np_ = cnt;
           int j0_ = j0;
-          void* args[] = {(void*)&d_tp, (void*)&np_, (void*)&j0_, (void*)&d_bar_};
+          int* fail = d_err_ + 3;
+          void* args[] = {(void*)&d_tp, (void*)&np_, (void*)&j0_, (void*)&fail};
           NRGB_LAUNCH("trd_panel", st,
                       NRGB_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, dim3(tot), dim3(TRD_NT),
                                                             args, smem, st)));
@@ -1229,7 +1236,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
                                       cudaMemcpyHostToDevice, st));
             NRGB_CUDA(cudaMemcpyAsync(d_gs, gb.segs.data(), gb.segs.size() * sizeof(GemmSeg),
                                       cudaMemcpyHostToDevice, st));
-            NRGB_CUDA(gemm_grouped_launch(d_gp, (int)gb.probs.size(), d_gs, gb.tiles, st));
+            NRGB_CUDA(gemm_grouped_launch(d_gp, (int)gb.probs.size(), d_gs, gb.tiles, st, "gemm_f64_trailing", gb.stiles));
             ++launches_;
           }
         }
@@ -1287,7 +1294,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         dim3 g2(ceil_div(maxnp, 8), nn);
         NRGB_LAUNCH("dc_vectors", st, dc_vectors_kernel<<<g2, 256, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
-        NRGB_CUDA(gemm_grouped_launch(d_gp, nn, d_gs, gb.tiles, st));
+        NRGB_CUDA(gemm_grouped_launch(d_gp, nn, d_gs, gb.tiles, st, "gemm_f64_dc", gb.stiles));
         NRGB_LAUNCH("dc_rank", st, dc_rank_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
         dim3 g3(maxnp, nn);
@@ -1338,7 +1345,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(g1.segs.size());
           NRGB_CUDA(cudaMemcpyAsync(d_gp, g1.probs.data(), g1.probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
           NRGB_CUDA(cudaMemcpyAsync(d_gs, g1.segs.data(), g1.segs.size() * sizeof(GemmSeg), cudaMemcpyHostToDevice, st));
-          NRGB_CUDA(gemm_grouped_launch(d_gp, (int)g1.probs.size(), d_gs, g1.tiles, st));
+          NRGB_CUDA(gemm_grouped_launch(d_gp, (int)g1.probs.size(), d_gs, g1.tiles, st, "gemm_f64_bt", g1.stiles));
         }
         NRGB_LAUNCH("bt_T", st, bt_T_kernel<<<nbig, NBB, 0, st>>>(d_bp, j0));
         NRGB_CUDA(cudaGetLastError());
@@ -1388,7 +1395,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(gb.segs.size());
           NRGB_CUDA(cudaMemcpyAsync(d_gp, gb.probs.data(), gb.probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
           NRGB_CUDA(cudaMemcpyAsync(d_gs, gb.segs.data(), gb.segs.size() * sizeof(GemmSeg), cudaMemcpyHostToDevice, st));
-          NRGB_CUDA(gemm_grouped_launch(d_gp, (int)gb.probs.size(), d_gs, gb.tiles, st));
+          NRGB_CUDA(gemm_grouped_launch(d_gp, (int)gb.probs.size(), d_gs, gb.tiles, st, "gemm_f64_bt", gb.stiles));
         }
         launches_ += 6;
       }
@@ -1400,6 +1407,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
   NRGB_CUDA(cudaMemcpyAsync(herr, d_err_, sizeof(herr), cudaMemcpyDeviceToHost, st));
   NRGB_CUDA(cudaMemcpyAsync(&hb, d_bar_, sizeof(hb), cudaMemcpyDeviceToHost, st));
   NRGB_CUDA(cudaStreamSynchronize(st));
+  hb.error |= herr[3];
   if (herr[0] || herr[1]) throw CudaError("syev: QR iteration did not converge");
   if (herr[2]) throw CudaError("syev: secular equation iteration did not converge");
   if (hb.error) throw CudaError("syev: grid barrier timed out");

@@ -106,7 +106,7 @@ struct Prev {
 struct Grouped {
   std::vector<GemmProb> probs;
   std::vector<GemmSeg> segs;
-  int tiles = 0;
+  int tiles = 0, stiles = 0;
   void out(double* C, int ldc, int m, int n, double beta, const std::vector<GemmSeg>& ss) {
     if (m <= 0 || n <= 0) return;
     GemmProb p{};
@@ -117,9 +117,7 @@ struct Grouped {
     p.beta = beta;
     p.seg0 = (int)segs.size();
     p.nseg = (int)ss.size();
-    p.tile0 = tiles;
-    p.tiles_n = (n + GEMM_BN - 1) / GEMM_BN;
-    tiles += ((m + GEMM_BM - 1) / GEMM_BM) * p.tiles_n;
+    gemm_assign_tiles(p, tiles, stiles);
     segs.insert(segs.end(), ss.begin(), ss.end());
     probs.push_back(p);
   }
@@ -187,7 +185,7 @@ struct NrgDriver::Impl {
     if (g.probs.empty()) return;
     GemmProb* dp = upload(g.probs);
     GemmSeg* ds = upload(g.segs);
-    NRGB_CUDA(gemm_grouped_launch(dp, (int)g.probs.size(), ds, g.tiles, st));
+    NRGB_CUDA(gemm_grouped_launch(dp, (int)g.probs.size(), ds, g.tiles, st, "gemm_f64_nrg", g.stiles));
     launches += 1;
   }
   DevMat upload_mat(const HostMat& M, Slab& slab) {

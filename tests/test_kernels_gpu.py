@@ -94,3 +94,36 @@ def test_syev_batched_host_api(ctx, kind):
         assert res <= 1e-13 * nrm * max(10, n)
         orth = np.abs(Zi.T @ Zi - np.eye(n)).max()
         assert orth <= 1e-13 * max(10, n)
+
+
+def test_gemm_grouped_large_tiles(ctx):
+    """Problems large enough that the launch uses the 128x128-tile kernel."""
+    import nrgb
+    rng = np.random.default_rng(5)
+    dev = "cuda:0"
+    outs, terms, refs, keep = [], [], [], []
+    for idx in range(8):
+        m, n, k = 600 + 7 * idx, 590 - 5 * idx, 300 + 11 * idx
+        ta, tb = idx & 1, (idx >> 1) & 1
+        C0 = torch.tensor(rng.standard_normal((m, n)), device=dev)
+        Cc = _col(C0)
+        ref = -1.0 * C0.clone()
+        t0 = len(terms)
+        for s in range(3):
+            kk = k + 17 * s
+            A = torch.tensor(rng.standard_normal((m, kk)), device=dev)
+            B = torch.tensor(rng.standard_normal((kk, n)), device=dev)
+            alpha = 1.5 - 0.75 * s
+            As = _col(A.t()) if ta else _col(A)
+            Bs = _col(B.t()) if tb else _col(B)
+            keep += [As, Bs]
+            terms.append(nrgb.GemmTerm(As.data_ptr(), Bs.data_ptr(), (kk if ta else m), (n if tb else kk), kk,
+                                       ta, tb, alpha))
+            ref += alpha * (A @ B)
+        outs.append(nrgb.GemmOut(Cc.data_ptr(), m, m, n, -1.0, t0, 3))
+        refs.append((Cc, ref))
+    ctx.gemm_grouped_dev(outs, terms)
+    torch.cuda.synchronize()
+    for Cc, ref in refs:
+        err = (Cc.t() - ref).abs().max().item()
+        assert err <= 1e-13 * (ref.abs().max().item() + 1.0) * 50
