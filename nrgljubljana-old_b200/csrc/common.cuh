@@ -6,6 +6,7 @@
 #include <stdio.h>
 
 #include <stdexcept>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -72,73 +73,93 @@ struct ArenaPlan {
 
 // Launch counting and optional per-kernel timing with CUDA events on the
 // launching stream (used by the benchmark to time the dominant kernel
-// inside a larger call).  One instance per process; not thread-safe.
+// inside a larger call).  One instance per process, shared by every context
+// and thread: all members are guarded by one mutex, and each bracketed
+// launch carries its own record slot, so launches from several host threads
+// may interleave.
 class KernelStats {
  public:
   static KernelStats& get();
   void enable(bool on);              // resets all counters
   bool timing() const { return timing_; }
-  // bracket one launch: begin() before, end() after (no-ops without timing)
-  void begin(const char* name, cudaStream_t s);
-  void end(cudaStream_t s);
+  // bracket one launch: begin() before (counts it and, with timing on,
+  // records the start event and returns a slot), end(slot) after
+  int begin(const char* name, cudaStream_t s);
+  void end(int slot, cudaStream_t s);
   void count(const char* name, long n = 1);
   // launches and total milliseconds of `name` ("*" = all kernels); syncs events
   void query(const char* name, long* launches, double* ms);
 
  private:
   struct Rec { std::string name; cudaEvent_t a, b; };
+  std::mutex m_;
   bool timing_ = false;
   std::vector<Rec> open_, done_;
+  std::vector<int> free_;
   std::vector<cudaEvent_t> pool_;
   std::vector<std::pair<std::string, long>> counts_;
   std::vector<std::pair<std::string, double>> ms_;
   cudaEvent_t ev();
+  void count_locked(const char* name, long n);
   void settle();
 };
 
 // Counts (and, when timing is on, times) one kernel launch statement.
-#define NRGB_LAUNCH(name, stream, ...)                 \
-  do {                                                 \
+#define NRGB_LAUNCH(name, stream, ...)                      \
+  do {                                                      \
     ::nrgb::KernelStats& ks__ = ::nrgb::KernelStats::get(); \
-    ks__.count(name);                                  \
-    ks__.begin(name, stream);                          \
-    __VA_ARGS__;                                       \
-    ks__.end(stream);                                  \
+    const int slot__ = ks__.begin(name, stream);            \
+    __VA_ARGS__;                                            \
+    ks__.end(slot__, stream);                               \
   } while (0)
 
-// Device-side state of a grid barrier (one per cooperative launch).
+// Device-side state of a grid barrier.  The arrival counter and the
+// generation word sit on separate 128-byte lines, so CTAs polling the
+// generation do not contend with the atomics on the counter.
 struct GridBarrier {
   unsigned int count;
-  unsigned int gen;
   int error;     // set when a wait gave up
-  int pad;
+  unsigned int pad0[30];
+  unsigned int gen;
+  unsigned int pad1[31];
 };
 
 #ifdef __CUDACC__
-// Sense-free generation barrier for co-resident CTAs (cooperative launch).
-// Every wait is bounded: after ~2^26 polls the CTA records an error and
-// continues; once the error is set all later barriers return immediately,
-// so a broken launch ends instead of hanging the GPU.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Generation barrier for co-resident CTAs (cooperative launch).  Thread 0
+// of each CTA arrives with a release-acquire atomic and polls the
+// generation with acquire loads and exponential back-off.  Every wait is
+// bounded: after 2^23 polls (about a second) the CTA records an error and
+// continues, and a waiting CTA that sees the error leaves too; once
+// the error is set all later barriers return immediately, so a broken
+// launch ends instead of hanging the GPU.
 __device__ __forceinline__ void grid_barrier(GridBarrier* b, unsigned int nblocks) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile GridBarrier* vb = b;
-    if (vb->error == 0) {
-      const unsigned int g = vb->gen;
+    if (*reinterpret_cast<volatile int*>(&b->error) == 0) {
+      const unsigned int g = ld_acquire_u32(&b->gen);
       __threadfence();
-      const unsigned int arrived = atomicAdd(&b->count, 1u) + 1u;
-      if (arrived == nblocks) {
+      unsigned int arrived;
+      asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;\n" : "=r"(arrived) : "l"(&b->count) : "memory");
+      if (arrived + 1u == nblocks) {
         b->count = 0;
         __threadfence();
-        atomicAdd(&b->gen, 1u);
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;\n" ::"l"(&b->gen) : "memory");
       } else {
         long long it = 0;
-        while (vb->gen == g) {
-          if (++it > (1ll << 26)) {
+        unsigned ns = 8;
+        while (ld_acquire_u32(&b->gen) == g) {
+          if (++it > (1ll << 23) || *reinterpret_cast<volatile int*>(&b->error)) {
             atomicExch(&b->error, 1);
             break;
           }
-          __nanosleep(20);
+          __nanosleep(ns);
+          if (ns < 128) ns <<= 1;
         }
       }
       __threadfence();

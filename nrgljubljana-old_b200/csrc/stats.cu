@@ -22,29 +22,47 @@ cudaEvent_t KernelStats::ev() {
 }
 
 void KernelStats::enable(bool on) {
+  std::lock_guard<std::mutex> g(m_);
   settle();
   counts_.clear();
   ms_.clear();
   timing_ = on;
 }
 
-void KernelStats::begin(const char* name, cudaStream_t s) {
-  if (!timing_) return;
-  Rec r{name, ev(), ev()};
-  NRGB_CUDA(cudaEventRecord(r.a, s));
-  open_.push_back(r);
+int KernelStats::begin(const char* name, cudaStream_t s) {
+  std::lock_guard<std::mutex> g(m_);
+  count_locked(name, 1);
+  if (!timing_) return -1;
+  int slot;
+  if (!free_.empty()) {
+    slot = free_.back();
+    free_.pop_back();
+  } else {
+    slot = (int)open_.size();
+    open_.push_back(Rec{});
+  }
+  open_[slot] = Rec{name, ev(), ev()};
+  NRGB_CUDA(cudaEventRecord(open_[slot].a, s));
+  return slot;
 }
 
-void KernelStats::end(cudaStream_t s) {
-  if (!timing_ || open_.empty()) return;
-  Rec r = open_.back();
-  open_.pop_back();
+void KernelStats::end(int slot, cudaStream_t s) {
+  if (slot < 0) return;
+  std::lock_guard<std::mutex> g(m_);
+  if (slot >= (int)open_.size()) return;
+  Rec r = open_[slot];
+  free_.push_back(slot);
   NRGB_CUDA(cudaEventRecord(r.b, s));
   done_.push_back(r);
   if (done_.size() > 4096) settle();
 }
 
 void KernelStats::count(const char* name, long n) {
+  std::lock_guard<std::mutex> g(m_);
+  count_locked(name, n);
+}
+
+void KernelStats::count_locked(const char* name, long n) {
   for (auto& c : counts_)
     if (c.first == name) {
       c.second += n;
@@ -72,6 +90,7 @@ void KernelStats::settle() {
 }
 
 void KernelStats::query(const char* name, long* launches, double* ms) {
+  std::lock_guard<std::mutex> g(m_);
   settle();
   const bool all = strcmp(name, "*") == 0;
   const size_t len = strlen(name);

@@ -242,18 +242,27 @@ __device__ __forceinline__ double ld_volatile(const double* p) {
 }
 
 // One panel of NB columns for every problem (cooperative launch).  Per column
-// c three phases separated by grid barriers; every load of data written by
+// c two phases separated by grid barriers; every load of data written by
 // other CTAs during the launch bypasses L1 (__ldcg).
-//   1: a = A[c:, c] - V W[c,:]^T - W V[c,:]^T   (also finishes W[:, jj-1])
-//   2: Householder vector v, p = W^T v, q = V^T v
-//   3: y = A22 v - V p - W q  (one warp per column of A22)
+//   A: finish the previous column: y = y' - V p - W q (p = W^T v, q = V^T v
+//      of that column), W[:, jj-1] = tau y + a2 v with
+//      a2 = -tau^2/2 * (y'^T v - 2 p^T q);  then
+//      a = A[c:, c] - V W[c,:]^T - W V[c,:]^T and its norm below c+1.
+//   B: Householder vector v of column c (every CTA forms all of it in shared
+//      memory), partial p = W^T v, q = V^T v over this CTA's row chunk, and
+//      y' = A22 v (one warp per column of A22), with y'^T v.
+// Deferring the V p + W q correction of y to the next column's phase A saves
+// the third grid barrier per column that an eager correction needs.  The
+// entries below the subdiagonal of column c are overwritten with v one
+// phase later too, because every CTA reads the updated column in phase B.
 __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __restrict__ probs,
                                                            int nprob, int j0, int* fail) {
   extern __shared__ double sm[];
   double* scratch = sm;          // 32
   double* VWc = sm + 32;         // 2*NB: row c of V and W
-  double* pq = VWc + 2 * NB;     // 2*NB
-  double* pqw = pq + 2 * NB;     // (TRD_NT/32) x 2*NB partial p,q
+  double* pq = VWc + 2 * NB;     // 2*NB: p, q of the previous column
+  double* misc = pq + 2 * NB;    // 8
+  double* pqw = misc + 8;        // (TRD_NT/32) x 2*NB partial p,q
   double* vs = pqw + (TRD_NT / 32) * 2 * NB;  // n_max
   const int b = blockIdx.x;
   int lo = 0, hi = nprob - 1;
@@ -276,33 +285,52 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
   for (int jj = 0; jj < NB; ++jj) {
     const int c = j0 + jj;
     const bool act = c < n;
-    double* R = P.red + (c & 1) * RED;
-    double* Ro = P.red + ((c + 1) & 1) * RED;
-    // ---------------- phase 1 ----------------
+    double* R = P.red + (c & 1) * RED;         // this column's sums
+    double* Ro = P.red + ((c + 1) & 1) * RED;  // previous column's sums (next column's slot)
+    // ---------------- phase A ----------------
     if (act) {
-      double tprev = 0.0, a2 = 0.0;
-      if (jj > 0) {
-        tprev = __ldcg(&P.tau[c - 1]);
-        a2 = -0.5 * tprev * tprev * ld_volatile(&Ro[1]);
-      }
-      if (tid < jj) {
+      const int kp = jj - 1;  // columns of V, W before the previous one
+      double tprev = 0.0;
+      if (jj > 0) tprev = __ldcg(&P.tau[c - 1]);
+      if (tid < NB) {
         const int k = tid;
-        VWc[k] = __ldcg(&P.Vp[(size_t)c * NB + k]);
-        VWc[NB + k] = (k == jj - 1) ? tprev * __ldcg(&P.y[c]) + a2 : __ldcg(&P.W[(size_t)c * NB + k]);
+        pq[k] = (k < kp) ? ld_volatile(&Ro[2 + k]) : 0.0;
+        pq[NB + k] = (k < kp) ? ld_volatile(&Ro[2 + NB + k]) : 0.0;
+        VWc[k] = (k < jj) ? __ldcg(&P.Vp[(size_t)c * NB + k]) : 0.0;
+        VWc[NB + k] = (k < kp) ? __ldcg(&P.W[(size_t)c * NB + k]) : 0.0;
       }
       __syncthreads();
+      if (jj > 0 && warp == 0) {
+        // scalar a2 and row c of the previous column of W (every CTA)
+        const double ptq = warp_sum(pq[lane] * pq[NB + lane]);
+        const double corr = warp_sum(VWc[lane] * pq[lane] + VWc[NB + lane] * pq[NB + lane]);
+        const double a2 = -0.5 * tprev * tprev * (ld_volatile(&Ro[1]) - 2.0 * ptq);
+        if (lane == 0) {
+          misc[0] = a2;
+          VWc[NB + kp] = tprev * (__ldcg(&P.y[c]) - corr) + a2 * __ldcg(&P.v[c]);
+        }
+      }
+      __syncthreads();
+      const double a2 = (jj > 0) ? misc[0] : 0.0;
+      const double pk = pq[lane], qk = pq[NB + lane];
+      const double vck = VWc[lane], wck = VWc[NB + lane];
       double ss = 0.0;
       for (int i = c + gw; i < n; i += tw) {
+        double vik = 0.0, wik = 0.0;
+        if (lane < jj) vik = __ldcg(&P.Vp[(size_t)i * NB + lane]);
+        if (lane < kp) wik = __ldcg(&P.W[(size_t)i * NB + lane]);
         double wl = 0.0;
-        if (jj > 0) wl = tprev * __ldcg(&P.y[i]) + a2 * __ldcg(&P.v[i]);
-        double t = 0.0;
-        if (lane < jj) {
-          const double wik = (lane == jj - 1) ? wl : __ldcg(&P.W[(size_t)i * NB + lane]);
-          t = __ldcg(&P.Vp[(size_t)i * NB + lane]) * VWc[NB + lane] + wik * VWc[lane];
+        if (jj > 0) {
+          const double corr = warp_sum(vik * pk + wik * qk);
+          wl = tprev * (__ldcg(&P.y[i]) - corr) + a2 * __ldcg(&P.v[i]);
+          if (lane == kp) wik = wl;
         }
-        t = warp_sum(t);
+        const double t = warp_sum(vik * wck + wik * vck);
         if (lane == 0) {
-          if (jj > 0) P.W[(size_t)i * NB + jj - 1] = wl;
+          if (jj > 0) {
+            P.W[(size_t)i * NB + kp] = wl;
+            if (i >= c + 1) P.A[i + (size_t)(c - 1) * ld] = __ldcg(&P.v[i]);
+          }
           const double a = __ldcg(&P.A[i + c * ld]) - t;
           P.A[i + c * ld] = a;
           if (i == c) P.d[c] = a;
@@ -313,9 +341,9 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
       if (tid == 0 && ss != 0.0) atomicAdd(&R[0], ss);
     }
     grid_barrier(bar, nblocks);
-    // ---------------- phase 2 ----------------
+    // ---------------- phase B ----------------
     if (act && c < n - 1) {
-      const double alpha = ld_volatile(&P.A[c + 1 + c * ld]);
+      const double alpha = __ldcg(&P.A[c + 1 + c * ld]);
       const double xn2 = ld_volatile(&R[0]);
       double beta = alpha, tc = 0.0, scal = 0.0;
       if (xn2 != 0.0) {
@@ -327,21 +355,21 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
         P.e[c] = beta;
         P.tau[c] = tc;
       }
-      if (rank == 0 && tid < RED) Ro[tid] = 0.0;
+      if (rank == 0 && tid < RED) Ro[tid] = 0.0;  // read in phase A, refilled from the next phase A on
       const int m = n - c - 1;
+      for (int i = tid; i < m; i += TRD_NT) vs[i] = (i == 0) ? 1.0 : __ldcg(&P.A[c + 1 + i + c * ld]) * scal;
+      __syncthreads();
       const int chunk = (m + P.ncta - 1) / P.ncta;
       const int r0 = c + 1 + rank * chunk, r1 = min(n, r0 + chunk);
       for (int i = r0 + tid; i < r1; i += TRD_NT) {
-        const double vi = (i == c + 1) ? 1.0 : __ldcg(&P.A[i + c * ld]) * scal;
+        const double vi = vs[i - c - 1];
         P.v[i] = vi;
         P.Vp[(size_t)i * NB + jj] = vi;
-        if (i >= c + 2) P.A[i + c * ld] = vi;
       }
-      __syncthreads();
       if (jj > 0) {
         double sp = 0.0, sq = 0.0;
         for (int i = r0 + warp; i < r1; i += nwarps) {
-          const double vi = __ldcg(&P.v[i]);
+          const double vi = vs[i - c - 1];
           if (lane < jj) {
             sp += __ldcg(&P.W[(size_t)i * NB + lane]) * vi;
             sq += __ldcg(&P.Vp[(size_t)i * NB + lane]) * vi;
@@ -360,17 +388,6 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
           if (bq != 0.0) atomicAdd(&R[2 + NB + tid], bq);
         }
       }
-    }
-    grid_barrier(bar, nblocks);
-    // ---------------- phase 3 ----------------
-    if (act && c < n - 1) {
-      const int m = n - c - 1;
-      for (int i = tid; i < m; i += TRD_NT) vs[i] = __ldcg(&P.v[c + 1 + i]);
-      if (tid < jj) {
-        pq[tid] = ld_volatile(&R[2 + tid]);
-        pq[NB + tid] = ld_volatile(&R[2 + NB + tid]);
-      }
-      __syncthreads();
       double yvp = 0.0;
       for (int j = c + 1 + gw; j < n; j += tw) {
         const double* col = P.A + (size_t)j * ld + (c + 1);
@@ -388,10 +405,7 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
           for (int u = 0; u < 8; ++u) s[u] += __ldcg(&col[i + 32 * u]) * vs[i + 32 * u];
         }
         for (; i < m; i += 32) s[0] += __ldcg(&col[i]) * vs[i];
-        double corr = 0.0;
-        if (lane < jj)
-          corr = __ldcg(&P.Vp[(size_t)j * NB + lane]) * pq[lane] + __ldcg(&P.W[(size_t)j * NB + lane]) * pq[NB + lane];
-        const double yj = warp_sum(((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7])) - corr);
+        const double yj = warp_sum(((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7])));
         if (lane == 0) {
           P.y[j] = yj;
           yvp += yj * vs[j - c - 1];
@@ -402,16 +416,30 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
     }
     grid_barrier(bar, nblocks);
   }
-  // finish W[:, NB-1] for the trailing update
+  // finish the panel's last column: W[:, NB-1] for the trailing update and v
+  // below its subdiagonal
   const int c = j0 + NB - 1;
   if (c < n - 1) {
+    const double* R = P.red + (c & 1) * RED;
     const double tc = __ldcg(&P.tau[c]);
-    const double a2 = -0.5 * tc * tc * ld_volatile(&P.red[(c & 1) * RED + 1]);
-    const int m = n - c - 1;
-    const int chunk = (m + P.ncta - 1) / P.ncta;
-    const int r0 = c + 1 + rank * chunk, r1 = min(n, r0 + chunk);
-    for (int i = r0 + tid; i < r1; i += TRD_NT)
-      P.W[(size_t)i * NB + NB - 1] = tc * __ldcg(&P.y[i]) + a2 * __ldcg(&P.v[i]);
+    if (tid < NB) {
+      pq[tid] = (tid < NB - 1) ? ld_volatile(&R[2 + tid]) : 0.0;
+      pq[NB + tid] = (tid < NB - 1) ? ld_volatile(&R[2 + NB + tid]) : 0.0;
+    }
+    __syncthreads();
+    const double pk = pq[lane], qk = pq[NB + lane];
+    const double a2 = -0.5 * tc * tc * (ld_volatile(&R[1]) - 2.0 * warp_sum(pk * qk));
+    for (int i = c + 1 + gw; i < n; i += tw) {
+      double corr = 0.0;
+      if (lane < NB - 1)
+        corr = __ldcg(&P.Vp[(size_t)i * NB + lane]) * pk + __ldcg(&P.W[(size_t)i * NB + lane]) * qk;
+      corr = warp_sum(corr);
+      if (lane == 0) {
+        const double vi = __ldcg(&P.v[i]);
+        P.W[(size_t)i * NB + NB - 1] = tc * (__ldcg(&P.y[i]) - corr) + a2 * vi;
+        if (i >= c + 2) P.A[i + c * ld] = vi;
+      }
+    }
   }
   // a barrier that gave up is reported to the host (the barriers are reset per launch)
   if (tid == 0 && *reinterpret_cast<volatile int*>(&bar->error)) atomicExch(fail, 1);
@@ -1157,7 +1185,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     }
     // ---------------- 1) tridiagonalisation ----------------
     {
-      const size_t smem = (size_t)(32 + 4 * NB + (TRD_NT / 32) * 2 * NB + nmax) * sizeof(double);
+      const size_t smem = (size_t)(32 + 4 * NB + 8 + (TRD_NT / 32) * 2 * NB + nmax) * sizeof(double);
       NRGB_CUDA(cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
       int per_sm = 0;

@@ -160,6 +160,16 @@ struct NrgDriver::Impl {
   // statistics
   double t_diag = 0, t_recalc = 0, t_dm = 0, t_spec = 0;
   double launches = 0, h2d = 0, d2h = 0;
+  // wall time per named section, reported on stderr when NRGB_TIMING is set
+  // (the counterpart of the reference's Timing report, src/nrg.h:136-190)
+  std::map<std::string, double> sections;
+  struct Section {
+    Impl* d;
+    const char* name;
+    Clock::time_point t0;
+    Section(Impl* d_, const char* n) : d(d_), name(n), t0(Clock::now()) {}
+    ~Section() { d->sections[name] += secs(t0); }
+  };
   // device scratch for descriptors
   DeviceArena desc;
   size_t desc_off = 0;
@@ -479,6 +489,7 @@ struct NrgDriver::Impl {
     size_t hcap = 0;
     double* H = nullptr;
     for (int N = Ninit; N < Nmax; ++N) {
+      auto ts = Clock::now();
       const double scale1 = scale_of(P, N + 1);
       desc_reset();
       // subspaces of the new step and their ancestors
@@ -553,12 +564,15 @@ struct NrgDriver::Impl {
         }
         sd.push_back(SyevDesc{b.dim, Hb, b.w, b.Z});
       }
+      sections["sweep1 setup"] += secs(ts);
       auto t0 = Clock::now();
       NRGB_CUDA(assemble_launch(upload(ad), (int)ad.size(), upload(ao), (int)ao.size(), maxlen, maxrc, st));
       launches += 2;
       syev->run(sd, st);
       launches += syev->last_launches();
       t_diag += secs(t0);
+      sections["sweep1 diag"] += secs(t0);
+      ts = Clock::now();
       // eigenvalues to the host: ground state, clusters, truncation
       for (auto& kv : S.blocks) {
         kv.second.value = download(kv.second.w, kv.second.dim);
@@ -591,6 +605,7 @@ struct NrgDriver::Impl {
         std::sort(l.begin(), l.end());
         annotated.push_back(std::move(l));
       }
+      sections["sweep1 truncate+td"] += secs(ts);
       // operator recalculation
       t0 = Clock::now();
       auto f_new = std::make_unique<Slab>(st);
@@ -633,6 +648,7 @@ struct NrgDriver::Impl {
       expv_rows.push_back({scale1 / P.betabar, row});
       NRGB_CUDA(cudaStreamSynchronize(st));
       t_recalc += secs(t0);
+      sections["sweep1 recalc"] += secs(t0);
       // the new <f> and singlets replace the old ones; truncated values become prev
       opch = std::move(opch_new);
       f_slab = std::move(f_new);
@@ -922,6 +938,7 @@ struct NrgDriver::Impl {
       for (auto& kv : ops) nops[kv.first] = recalc_op(kv.first.first, S, kv.second, recalc_all, *nslab);
       NRGB_CUDA(cudaStreamSynchronize(st));
       t_recalc += secs(t0);
+      sections["sweep2 recalc"] += secs(t0);
       t0 = Clock::now();
       // absolute energies shifted by the absolute ground state (FDM)
       std::map<Invar, double*> absdev;
@@ -1016,6 +1033,7 @@ struct NrgDriver::Impl {
         NRGB_CUDA(cudaStreamSynchronize(st));
       }
       t_spec += secs(t0);
+      sections["sweep2 spec"] += secs(t0);
       // operators for the next step: the kept states only (nrg_trim_matrices)
       for (auto& kv : nops)
         for (auto& m : kv.second) {
@@ -1188,6 +1206,8 @@ struct NrgDriver::Impl {
     rhofdm.clear();
     rho_slabs.clear();
     spectra.clear();
+    sections.clear();
+    std::unique_ptr<Section> sec(new Section(this, "read input"));
     desc.reserve(64 << 20);
     desc.reset();
     P = Params();
@@ -1204,22 +1224,29 @@ struct NrgDriver::Impl {
     if (Nmax <= Ninit) throw std::runtime_error("zero-bandwidth runs (Nmax == Ninit) are not supported");
     if (P.dm && P.T <= 0) throw std::runtime_error("density-matrix runs need T > 0");
     Slab persist(st);
+    sec.reset();
     sweep1(persist);
     if (P.dm) {
       auto t1 = Clock::now();
-      if (P.dmnrg) calc_densitymatrix();
+      if (P.dmnrg) {
+        Section x(this, "DM");
+        calc_densitymatrix();
+      }
       if (P.fdm) {
+        Section x(this, "FDM");
         calc_ZnD();
         calc_fulldensitymatrix();
       }
       t_dm += secs(t1);
       sweep2(persist);
     }
+    sec.reset(new Section(this, "write output"));
     write_td(od);
     write_custom(od);
     write_annotated(od);
     write_spectra(od);
     NRGB_CUDA(cudaStreamSynchronize(st));
+    sec.reset(new Section(this, "release"));
     // release device memory of the run
     spectra.clear();
     rho.clear();
@@ -1227,6 +1254,17 @@ struct NrgDriver::Impl {
     rho_slabs.clear();
     steps.clear();
     NRGB_CUDA(cudaStreamSynchronize(st));
+    sec.reset();
+    if (getenv("NRGB_TIMING")) {
+      const double all = secs(t0);
+      double sum = 0;
+      fprintf(stderr, "Timing report\n=============\n%20s: %.4f s\n", "All", all);
+      for (const auto& kv : sections) {
+        fprintf(stderr, "%20s: %.4f s\n", kv.first.c_str(), kv.second);
+        sum += kv.second;
+      }
+      fprintf(stderr, "%20s: %.4f s\n", "Other", all - sum);
+    }
     if (stats) {
       stats[0] = secs(t0);
       stats[1] = t_diag;

@@ -20,6 +20,17 @@ CASES = {
     "kondo1": dict(model="kondo", J=[0.3], Lambda=2.0, Nmax=14,
                    params={"keep": 150, "dmnrg": True, "fdm": True, "T": 1e-4, "spect": "SZd-SZd",
                            "bins": 30, "savebins": True, "broaden": False}),
+    # the plain-method SIAM workload at full size: Nmax=30, keep 500 or
+    # 10 omega_N, DM-NRG A(omega) at T=1e-8, 50 bins per decade
+    "siam_nmax30": dict(model="siam", U=0.1, eps_d=-0.05, Gamma=0.01, Lambda=2.0, Nmax=30,
+                        params={"keep": 500, "keepenergy": 10.0, "dmnrg": True, "T": 1e-8,
+                                "specd": "A_d-A_d", "bins": 50, "savebins": True, "broaden": True,
+                                "dumpannotated": 20}),
+    # one run of the served z-averaging workload (z = 5/8, Nmax = 40), at its
+    # smallest Nkeep: FDM A(omega)
+    "siam_zshift": dict(model="siam", U=0.2, eps_d=-0.1, Gamma=0.02, Lambda=2.0, Nmax=40, z=0.625,
+                        params={"keep": 200, "fdm": True, "T": 1e-5, "specd": "A_d-A_d", "bins": 50,
+                                "savebins": True, "broaden": False}),
 }
 
 
@@ -27,7 +38,8 @@ def make_case(name, path):
     c = CASES[name]
     os.makedirs(path, exist_ok=True)
     if c["model"] == "siam":
-        inputgen.make_siam(path, c["U"], c["eps_d"], c["Gamma"], c["Lambda"], c["Nmax"], params=c["params"])
+        inputgen.make_siam(path, c["U"], c["eps_d"], c["Gamma"], c["Lambda"], c["Nmax"], z=c.get("z", 1.0),
+                           params=c["params"])
     else:
         inputgen.make_kondo(path, c["J"], c["Lambda"], c["Nmax"], params=c["params"])
     return path
