@@ -98,6 +98,11 @@ int nrgb_profile(nrgb_ctx* ctx, int enable);
  * is on).  Names: trd_panel, gemm_f64, syev_small, dc_*, bt_*, assemble_*,
  * spec_dmnrg, spec_fdm, merge_bins, gather_diag, col_scale. */
 int nrgb_kernel_stats(nrgb_ctx* ctx, const char* name, long* launches, double* ms);
+/* Algorithmic work stated by the host code for the launches counted under
+ * `name` (same name matching): bytes for trd_panel (each column's trailing
+ * block read once), flops (2 m n k) for the gemm_f64* call sites.  Counted
+ * since the last nrgb_profile(ctx, 1). */
+int nrgb_kernel_work(nrgb_ctx* ctx, const char* name, double* units);
 
 /* Allocation-free basis change, device pointers:
  *     out[o] = Z_bra[o]^T * op[o] * Z_ket[o]
@@ -129,6 +134,58 @@ int nrgb_basis_change_noalloc(int nops, const int* n_bra, const int* n_ket, cons
  * [3] density-matrix seconds, [4] spectral seconds, [5] kernels launched,
  * [6] host->device bytes, [7] device->host bytes. */
 int nrgb_run(nrgb_ctx* ctx, const char* workdir, const char* outdir, double* stats);
+
+/* Eigensolver structure of nrgb_run and nrgb_eig_recalc_step(_dev) on this
+ * context: 0 (default) solves all blocks of a step in one batched call; 1
+ * makes one solver call per block,
+ * the structure of the reference's per-subspace dsyev loop
+ * (src/nrg.cc:2484-2507), for comparisons.  Results agree to rounding. */
+int nrgb_set_eig_mode(nrgb_ctx* ctx, int mode);
+
+/* ---------------------------------------------------------------------------
+ * Run server: many NRG runs in flight on one GPU (continuous batching).
+ * No counterpart in the reference, which runs one calculation per process
+ * (src/nrg.cc:3429-3469); each run is what nrgb_run does for one work
+ * directory, with the same outputs.
+ *
+ * Requests queue in submission order.  A worker slot (max_runs of them)
+ * admits the head of the queue when its projected device bytes
+ * (nrgb_project_bytes) fit in mem_budget_bytes beside the runs already
+ * admitted; a run is always admitted when no other runs.  Admitted runs
+ * execute concurrently, each on its own stream; the block eigensolves of
+ * all runs in their first sweep are merged into shared batched solver
+ * calls, which wait at most batch_window_us for every such run to queue its
+ * blocks.  All calls are thread-safe.
+ * ------------------------------------------------------------------------- */
+typedef struct nrgb_server nrgb_server;
+
+/* mem_budget_bytes <= 0: 85% of the device memory free at creation.
+ * Returns 0, 1 (bad arguments), 2 (CUDA error), 3 (no device), 4 (bad device). */
+int nrgb_server_create(int device, int max_runs, double mem_budget_bytes, double batch_window_us,
+                       nrgb_server** out);
+/* Queue a run; *ticket (>= 1) identifies it.  Returns 0, 1, or 2 when the
+ * input cannot be read (text via nrgb_server_error(srv, 0)). */
+int nrgb_server_submit(nrgb_server* srv, const char* workdir, const char* outdir, long long* ticket);
+/* Wait for a run (timeout_s < 0: no limit).  Returns 0 (done), 2 (the run
+ * failed; text via nrgb_server_error(srv, ticket)), 7 (timed out), 1 (unknown
+ * ticket).  stats (may be NULL) receives 14 values: the 8 of nrgb_run, then
+ * [8] latency from submission to completion (s), [9] queue wait from
+ * submission to admission (s), [10] projected bytes, [11] peak device bytes
+ * the run's data held, [12] eigensolver calls, [13] admission order. */
+int nrgb_server_wait(nrgb_server* srv, long long ticket, double timeout_s, double* stats);
+/* Error text of a failed ticket, or of the last failed call when ticket <= 0;
+ * valid until the server is destroyed. */
+const char* nrgb_server_error(nrgb_server* srv, long long ticket);
+/* out[8]: runs done, runs failed, merged eigensolver calls, eigensolver
+ * requests, blocks solved, most runs in flight at once, most projected bytes
+ * admitted at once, memory budget. */
+int nrgb_server_counters(nrgb_server* srv, double* out);
+/* Finishes every queued and running request, then frees the server. */
+int nrgb_server_destroy(nrgb_server* srv);
+/* Upper bound of the device bytes a run of workdir holds at once, from
+ * workdir/param and workdir/data (host only; no device needed).
+ * Returns 0, 1 (bad arguments) or 2 (input not readable). */
+int nrgb_project_bytes(const char* workdir, double* bytes);
 
 #ifdef __cplusplus
 }

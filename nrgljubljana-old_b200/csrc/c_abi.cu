@@ -12,17 +12,41 @@
 #include "syev.cuh"
 #include "../host/driver.h"
 
+namespace {
+// The reference's structure on the GPU: one solver call per block
+// (dsyev per invariant subspace, src/nrg.cc:2484-2507), for comparisons.
+struct PerBlockSolver : nrgb::EigSolver {
+  nrgb::SyevBatched* s = nullptr;
+  int solve(const std::vector<nrgb::SyevDesc>& probs, cudaStream_t st) override {
+    int l = 0;
+    for (const auto& p : probs) l += s->solve(std::vector<nrgb::SyevDesc>{p}, st);
+    return l;
+  }
+};
+}  // namespace
+
 struct nrgb_ctx {
   int device = 0;
   std::string err;
   cudaStream_t stream = nullptr;
   std::unique_ptr<nrgb::SyevBatched> syev;
+  PerBlockSolver per_block;
+  int eig_mode = 0;
   nrgb::DeviceArena scratch;
   nrgb::DeviceArena io;
   std::unique_ptr<nrgb::NrgDriver> driver;
 };
 
 namespace {
+
+// The solver nrgb_set_eig_mode selected for this context.
+nrgb::EigSolver* solver_of(nrgb_ctx* ctx) {
+  if (ctx->eig_mode == 1) {
+    ctx->per_block.s = ctx->syev.get();
+    return &ctx->per_block;
+  }
+  return ctx->syev.get();
+}
 
 template <class F>
 int guarded(nrgb_ctx* ctx, F&& f) {
@@ -106,7 +130,7 @@ int nrgb_syev_batched(nrgb_ctx* ctx, int nblocks, const int* n, double* const* a
       if (nn) NRGB_CUDA(cudaMemcpyAsync(A, a[b], nn * sizeof(double), cudaMemcpyHostToDevice, st));
       d[b] = nrgb::SyevDesc{n[b], A, W, Z};
     }
-    ctx->syev->run(d, st);
+    solver_of(ctx)->solve(d, st);
     for (int b = 0; b < nblocks; ++b) {
       const size_t nn = (size_t)n[b] * n[b];
       if (!nn) continue;
@@ -151,6 +175,7 @@ int nrgb_gemm_grouped_dev(nrgb_ctx* ctx, int nout, const nrgb_gemm_out* outs, in
     auto* dS = ctx->scratch.alloc_n<nrgb::GemmSeg>(S.size());
     NRGB_CUDA(cudaMemcpyAsync(dP, P.data(), P.size() * sizeof(nrgb::GemmProb), cudaMemcpyHostToDevice, st));
     NRGB_CUDA(cudaMemcpyAsync(dS, S.data(), S.size() * sizeof(nrgb::GemmSeg), cudaMemcpyHostToDevice, st));
+    nrgb::KernelStats::get().add_work("gemm_f64", nrgb::gemm_flops(P.data(), (int)P.size(), S.data()));
     NRGB_CUDA(nrgb::gemm_grouped_launch(dP, (int)P.size(), dS, tiles, st, "gemm_f64", stiles));
     NRGB_CUDA(cudaStreamSynchronize(st));
   });
@@ -193,6 +218,8 @@ void recalc_pairs(nrgb_ctx* ctx, int nops, const int* n, const int* bra, const i
   NRGB_CUDA(cudaMemcpyAsync(e1, s1.data(), s1.size() * sizeof(s1[0]), cudaMemcpyHostToDevice, st));
   NRGB_CUDA(cudaMemcpyAsync(d2, p2.data(), p2.size() * sizeof(p2[0]), cudaMemcpyHostToDevice, st));
   NRGB_CUDA(cudaMemcpyAsync(e2, s2.data(), s2.size() * sizeof(s2[0]), cudaMemcpyHostToDevice, st));
+  nrgb::KernelStats::get().add_work("gemm_f64_recalc", nrgb::gemm_flops(p1.data(), (int)p1.size(), s1.data()) +
+                                                           nrgb::gemm_flops(p2.data(), (int)p2.size(), s2.data()));
   NRGB_CUDA(nrgb::gemm_grouped_launch(d1, (int)p1.size(), e1, t1, st, "gemm_f64_recalc", u1));
   NRGB_CUDA(nrgb::gemm_grouped_launch(d2, (int)p2.size(), e2, t2, st, "gemm_f64_recalc", u2));
 }
@@ -215,7 +242,7 @@ int nrgb_eig_recalc_step_dev(nrgb_ctx* ctx, int nblocks, const int* n, double* c
         throw nrgb::CudaError("eig_recalc: operator block index out of range");
     std::vector<nrgb::SyevDesc> d(nblocks);
     for (int b = 0; b < nblocks; ++b) d[b] = nrgb::SyevDesc{n[b], a_dev[b], w_dev[b], z_dev[b]};
-    ctx->syev->run(d, st);
+    solver_of(ctx)->solve(d, st);
     ctx->scratch.reserve(recalc_scratch(nops, n, bra, ket));
     ctx->scratch.reset();
     recalc_pairs(ctx, nops, n, bra, ket, z_dev, op_dev, out_dev, ctx->scratch, st);
@@ -252,7 +279,7 @@ int nrgb_eig_recalc_step(nrgb_ctx* ctx, int nblocks, const int* n, const double*
       R[o] = ctx->io.alloc_n<double>(nn);
       if (nn) NRGB_CUDA(cudaMemcpyAsync(O[o], op[o], nn * sizeof(double), cudaMemcpyHostToDevice, st));
     }
-    ctx->syev->run(d, st);
+    solver_of(ctx)->solve(d, st);
     ctx->scratch.reserve(recalc_scratch(nops, n, bra, ket));
     ctx->scratch.reset();
     recalc_pairs(ctx, nops, n, bra, ket, Z.data(), (const double* const*)O.data(), R.data(), ctx->scratch, st);
@@ -278,10 +305,25 @@ int nrgb_kernel_stats(nrgb_ctx* ctx, const char* name, long* launches, double* m
   return guarded(ctx, [&] { nrgb::KernelStats::get().query(name ? name : "*", launches, ms); });
 }
 
+int nrgb_kernel_work(nrgb_ctx* ctx, const char* name, double* units) {
+  return guarded(ctx, [&] {
+    const double w = nrgb::KernelStats::get().work(name ? name : "*");
+    if (units) *units = w;
+  });
+}
+
 int nrgb_run(nrgb_ctx* ctx, const char* workdir, const char* outdir, double* stats) {
   return guarded(ctx, [&] {
-    if (!ctx->driver) ctx->driver.reset(new nrgb::NrgDriver(ctx->stream, ctx->syev.get()));
+    if (!ctx->driver) ctx->driver.reset(new nrgb::NrgDriver(ctx->stream, solver_of(ctx)));
     ctx->driver->run(workdir, outdir, stats);
+  });
+}
+
+int nrgb_set_eig_mode(nrgb_ctx* ctx, int mode) {
+  if (mode != 0 && mode != 1) return 1;
+  return guarded(ctx, [&] {
+    ctx->eig_mode = mode;
+    ctx->driver.reset();  // rebuilt with the chosen solver by the next nrgb_run
   });
 }
 

@@ -87,8 +87,12 @@ class KernelStats {
   int begin(const char* name, cudaStream_t s);
   void end(int slot, cudaStream_t s);
   void count(const char* name, long n = 1);
+  // algorithmic work of launches of `name` (bytes for a memory-bound
+  // kernel, flops for a contraction), stated by the launching host code
+  void add_work(const char* name, double units);
   // launches and total milliseconds of `name` ("*" = all kernels); syncs events
   void query(const char* name, long* launches, double* ms);
+  double work(const char* name);
 
  private:
   struct Rec { std::string name; cudaEvent_t a, b; };
@@ -99,6 +103,7 @@ class KernelStats {
   std::vector<cudaEvent_t> pool_;
   std::vector<std::pair<std::string, long>> counts_;
   std::vector<std::pair<std::string, double>> ms_;
+  std::vector<std::pair<std::string, double>> work_;
   cudaEvent_t ev();
   void count_locked(const char* name, long n);
   void settle();

@@ -394,6 +394,14 @@ void gemm_assign_tiles(GemmProb& p, int& tiles, int& stiles) {
   stiles += ((p.m + LBM - 1) / LBM) * p.stiles_n * ks;
 }
 
+double gemm_flops(const GemmProb* probs, int nprob, const GemmSeg* segs) {
+  double f = 0;
+  for (int p = 0; p < nprob; ++p)
+    for (int s = probs[p].seg0; s < probs[p].seg0 + probs[p].nseg; ++s)
+      f += 2.0 * probs[p].m * (double)probs[p].n * segs[s].k;
+  return f;
+}
+
 cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
                                 int total_tiles, cudaStream_t stream, const char* tag, int total_stiles) {
   if (total_tiles <= 0 || nprob <= 0) return cudaSuccess;

@@ -59,6 +59,11 @@ cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSe
 cudaError_t gemm_grouped_launch_unaccounted(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
                                             int total_tiles, cudaStream_t stream);
 
+// Algorithmic flops of a grouped launch described on the host
+// (sum over problems and their segments of 2 m n k); for the launch
+// accounting's work counters.
+double gemm_flops(const GemmProb* probs, int nprob, const GemmSeg* segs);
+
 // Tile sizes (exported so hosts can compute tile counts).
 constexpr int GEMM_BM = 64;
 constexpr int GEMM_BN = 64;

@@ -26,6 +26,7 @@ void KernelStats::enable(bool on) {
   settle();
   counts_.clear();
   ms_.clear();
+  work_.clear();
   timing_ = on;
 }
 
@@ -60,6 +61,29 @@ void KernelStats::end(int slot, cudaStream_t s) {
 void KernelStats::count(const char* name, long n) {
   std::lock_guard<std::mutex> g(m_);
   count_locked(name, n);
+}
+
+void KernelStats::add_work(const char* name, double units) {
+  std::lock_guard<std::mutex> g(m_);
+  for (auto& w : work_)
+    if (w.first == name) {
+      w.second += units;
+      return;
+    }
+  work_.push_back({name, units});
+}
+
+double KernelStats::work(const char* name) {
+  std::lock_guard<std::mutex> g(m_);
+  const bool all = strcmp(name, "*") == 0;
+  const size_t len = strlen(name);
+  const bool prefix = len > 1 && name[len - 1] == '*';
+  double t = 0;
+  for (auto& w : work_) {
+    const std::string& k = w.first;
+    if (all || (prefix ? k.compare(0, len - 1, name, len - 1) == 0 : k == name)) t += w.second;
+  }
+  return t;
 }
 
 void KernelStats::count_locked(const char* name, long n) {

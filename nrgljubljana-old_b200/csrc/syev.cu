@@ -1230,6 +1230,13 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           int j0_ = j0;
           int* fail = d_err_ + 3;
           void* args[] = {(void*)&d_tp, (void*)&np_, (void*)&j0_, (void*)&fail};
+          {
+            // algorithmic bytes: column c reads its trailing (n-c-1)^2 block once
+            double wb = 0;
+            for (const TrdProb& t : sub)
+              for (int c = j0; c < std::min(j0 + NB, t.n - 1); ++c) wb += 8.0 * (double)(t.n - c - 1) * (t.n - c - 1);
+            KernelStats::get().add_work("trd_panel", wb);
+          }
           NRGB_LAUNCH("trd_panel", st,
                       NRGB_CUDA(cudaLaunchCooperativeKernel((void*)trd_panel_kernel, dim3(tot), dim3(TRD_NT),
                                                             args, smem, st)));
@@ -1264,6 +1271,8 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
                                       cudaMemcpyHostToDevice, st));
             NRGB_CUDA(cudaMemcpyAsync(d_gs, gb.segs.data(), gb.segs.size() * sizeof(GemmSeg),
                                       cudaMemcpyHostToDevice, st));
+            KernelStats::get().add_work("gemm_f64_trailing",
+                                        gemm_flops(gb.probs.data(), (int)gb.probs.size(), gb.segs.data()));
             NRGB_CUDA(gemm_grouped_launch(d_gp, (int)gb.probs.size(), d_gs, gb.tiles, st, "gemm_f64_trailing", gb.stiles));
             ++launches_;
           }
@@ -1373,6 +1382,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(g1.segs.size());
           NRGB_CUDA(cudaMemcpyAsync(d_gp, g1.probs.data(), g1.probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
           NRGB_CUDA(cudaMemcpyAsync(d_gs, g1.segs.data(), g1.segs.size() * sizeof(GemmSeg), cudaMemcpyHostToDevice, st));
+          KernelStats::get().add_work("gemm_f64_bt", gemm_flops(g1.probs.data(), (int)g1.probs.size(), g1.segs.data()));
           NRGB_CUDA(gemm_grouped_launch(d_gp, (int)g1.probs.size(), d_gs, g1.tiles, st, "gemm_f64_bt", g1.stiles));
         }
         NRGB_LAUNCH("bt_T", st, bt_T_kernel<<<nbig, NBB, 0, st>>>(d_bp, j0));
@@ -1423,6 +1433,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(gb.segs.size());
           NRGB_CUDA(cudaMemcpyAsync(d_gp, gb.probs.data(), gb.probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
           NRGB_CUDA(cudaMemcpyAsync(d_gs, gb.segs.data(), gb.segs.size() * sizeof(GemmSeg), cudaMemcpyHostToDevice, st));
+          KernelStats::get().add_work("gemm_f64_bt", gemm_flops(gb.probs.data(), (int)gb.probs.size(), gb.segs.data()));
           NRGB_CUDA(gemm_grouped_launch(d_gp, (int)gb.probs.size(), d_gs, gb.tiles, st, "gemm_f64_bt", gb.stiles));
         }
         launches_ += 6;

@@ -30,10 +30,29 @@ struct SyevDesc {
   double* Z;   // n x n eigenvectors (ld = n); must not alias A
 };
 
-class SyevBatched {
+// Diagonalises a batch of problems whose inputs are ordered on `stream`, and
+// returns once the results are complete in device memory.  Implemented by
+// the direct solver below and by a server's batcher, which merges the
+// batches of several concurrent runs into one solver call.  Returns the
+// number of kernel launches made for the batch.  Throws CudaError on failure.
+class EigSolver {
+ public:
+  virtual ~EigSolver() = default;
+  virtual int solve(const std::vector<SyevDesc>& probs, cudaStream_t stream) = 0;
+  // A run brackets the part of its work that calls solve() (its first
+  // sweep); a merging solver waits only for runs inside that part.
+  virtual void client_enter() {}
+  virtual void client_leave() {}
+};
+
+class SyevBatched : public EigSolver {
  public:
   SyevBatched();
   ~SyevBatched();
+  int solve(const std::vector<SyevDesc>& probs, cudaStream_t stream) override {
+    run(probs, stream);
+    return launches_;
+  }
   // Solve all problems on `stream`.  Throws CudaError on failure (including
   // a convergence failure or a barrier timeout reported by the kernels).
   void run(const std::vector<SyevDesc>& probs, cudaStream_t stream);

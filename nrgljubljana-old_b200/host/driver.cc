@@ -56,10 +56,17 @@ struct DevMat {
 };
 using DevBlocks = std::map<Twoinvar, DevMat>;
 
+// Device bytes held by the slabs of one run (current and peak).
+struct MemCount {
+  size_t cur = 0, peak = 0;
+};
+// The run executing on this host thread (set for the duration of run()).
+thread_local MemCount* tl_mem = nullptr;
+
 // Stream-ordered device allocations owned by one generation of data.
 class Slab {
  public:
-  explicit Slab(cudaStream_t s) : st_(s) {}
+  explicit Slab(cudaStream_t s) : st_(s), mc_(tl_mem) {}
   ~Slab() { release(); }
   Slab(const Slab&) = delete;
   double* alloc(size_t n) {
@@ -67,16 +74,25 @@ class Slab {
     if (n == 0) return nullptr;
     NRGB_CUDA(cudaMallocAsync(&p, n * sizeof(double), st_));
     ptrs_.push_back(p);
+    bytes_ += n * sizeof(double);
+    if (mc_) {
+      mc_->cur += n * sizeof(double);
+      mc_->peak = std::max(mc_->peak, mc_->cur);
+    }
     return static_cast<double*>(p);
   }
   void release() {
     for (void* p : ptrs_) cudaFreeAsync(p, st_);
     ptrs_.clear();
+    if (mc_) mc_->cur -= bytes_;
+    bytes_ = 0;
   }
 
  private:
   cudaStream_t st_;
+  MemCount* mc_;
   std::vector<void*> ptrs_;
+  size_t bytes_ = 0;
 };
 
 struct Block {
@@ -146,7 +162,7 @@ std::string fmt_g(double x, int prec) {
 
 struct NrgDriver::Impl {
   cudaStream_t st;
-  SyevBatched* syev;
+  EigSolver* syev;
   Params P;
   DataFile D;
   std::unique_ptr<Symmetry> sym;
@@ -174,7 +190,10 @@ struct NrgDriver::Impl {
   DeviceArena desc;
   size_t desc_off = 0;
 
-  Impl(cudaStream_t s, SyevBatched* e) : st(s), syev(e) {}
+  MemCount mem;
+  double eig_calls = 0;
+
+  Impl(cudaStream_t s, EigSolver* e) : st(s), syev(e) {}
 
   // ---------------- small helpers ----------------
   template <class T>
@@ -195,6 +214,7 @@ struct NrgDriver::Impl {
     if (g.probs.empty()) return;
     GemmProb* dp = upload(g.probs);
     GemmSeg* ds = upload(g.segs);
+    KernelStats::get().add_work("gemm_f64_nrg", gemm_flops(g.probs.data(), (int)g.probs.size(), g.segs.data()));
     NRGB_CUDA(gemm_grouped_launch(dp, (int)g.probs.size(), ds, g.tiles, st, "gemm_f64_nrg", g.stiles));
     launches += 1;
   }
@@ -568,8 +588,8 @@ struct NrgDriver::Impl {
       auto t0 = Clock::now();
       NRGB_CUDA(assemble_launch(upload(ad), (int)ad.size(), upload(ao), (int)ao.size(), maxlen, maxrc, st));
       launches += 2;
-      syev->run(sd, st);
-      launches += syev->last_launches();
+      launches += syev->solve(sd, st);
+      eig_calls += 1;
       t_diag += secs(t0);
       sections["sweep1 diag"] += secs(t0);
       ts = Clock::now();
@@ -1193,19 +1213,45 @@ struct NrgDriver::Impl {
     for (const auto& x : pos) F << x.first << " " << x.second << "\n";
   }
 
-  void run(const std::string& wd, const std::string& od, double* stats) {
+  // Device data of a run: freed at its end, and on the way out of a failed run
+  // so that a server can hand the memory to the next run.
+  void release_run_data() {
+    spectra.clear();
+    rho.clear();
+    rhofdm.clear();
+    rho_slabs.clear();
+    steps.clear();
+  }
+
+  void run(const std::string& wd, const std::string& od, double* stats, RunExtra* extra) {
+    release_run_data();
+    mem = MemCount();
+    eig_calls = 0;
+    struct MemScope {
+      explicit MemScope(MemCount* m) { tl_mem = m; }
+      ~MemScope() { tl_mem = nullptr; }
+    } mem_scope(&mem);
+    try {
+      run_body(wd, od, stats);
+    } catch (...) {
+      release_run_data();
+      cudaStreamSynchronize(st);
+      throw;
+    }
+    if (extra) {
+      extra->peak_bytes = (double)mem.peak;
+      extra->eig_calls = eig_calls;
+    }
+  }
+
+  void run_body(const std::string& wd, const std::string& od, double* stats) {
     const auto t0 = Clock::now();
     t_diag = t_recalc = t_dm = t_spec = 0;
     launches = h2d = d2h = 0;
-    steps.clear();
     cluster_map.clear();
     td_rows.clear();
     expv_rows.clear();
     annotated.clear();
-    rho.clear();
-    rhofdm.clear();
-    rho_slabs.clear();
-    spectra.clear();
     sections.clear();
     std::unique_ptr<Section> sec(new Section(this, "read input"));
     desc.reserve(64 << 20);
@@ -1225,7 +1271,14 @@ struct NrgDriver::Impl {
     if (P.dm && P.T <= 0) throw std::runtime_error("density-matrix runs need T > 0");
     Slab persist(st);
     sec.reset();
-    sweep1(persist);
+    {
+      struct Client {
+        EigSolver* e;
+        explicit Client(EigSolver* e_) : e(e_) { e->client_enter(); }
+        ~Client() { e->client_leave(); }
+      } client(syev);
+      sweep1(persist);
+    }
     if (P.dm) {
       auto t1 = Clock::now();
       if (P.dmnrg) {
@@ -1247,12 +1300,7 @@ struct NrgDriver::Impl {
     write_spectra(od);
     NRGB_CUDA(cudaStreamSynchronize(st));
     sec.reset(new Section(this, "release"));
-    // release device memory of the run
-    spectra.clear();
-    rho.clear();
-    rhofdm.clear();
-    rho_slabs.clear();
-    steps.clear();
+    release_run_data();
     NRGB_CUDA(cudaStreamSynchronize(st));
     sec.reset();
     if (getenv("NRGB_TIMING")) {
@@ -1278,10 +1326,10 @@ struct NrgDriver::Impl {
   }
 };
 
-NrgDriver::NrgDriver(cudaStream_t stream, SyevBatched* syev) : impl_(new Impl(stream, syev)) {}
+NrgDriver::NrgDriver(cudaStream_t stream, EigSolver* eig) : impl_(new Impl(stream, eig)) {}
 NrgDriver::~NrgDriver() { delete impl_; }
-void NrgDriver::run(const char* workdir, const char* outdir, double* stats) {
-  impl_->run(workdir, outdir, stats);
+void NrgDriver::run(const char* workdir, const char* outdir, double* stats, RunExtra* extra) {
+  impl_->run(workdir, outdir, stats, extra);
 }
 
 }  // namespace nrgb

@@ -14,7 +14,10 @@ LIBPATH = os.path.join(HERE, "libnrgb.so")
 EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
            "nrgb_syev_batched", "nrgb_syev_batched_dev", "nrgb_gemm_grouped_dev",
            "nrgb_eig_recalc_step", "nrgb_eig_recalc_step_dev", "nrgb_profile", "nrgb_kernel_stats",
-           "nrgb_basis_change_noalloc", "nrgb_run"]
+           "nrgb_kernel_work",
+           "nrgb_basis_change_noalloc", "nrgb_run", "nrgb_set_eig_mode",
+           "nrgb_server_create", "nrgb_server_submit", "nrgb_server_wait", "nrgb_server_error",
+           "nrgb_server_counters", "nrgb_server_destroy", "nrgb_project_bytes"]
 
 
 class GemmTerm(C.Structure):
@@ -48,14 +51,24 @@ def load(path: str = LIBPATH):
     lib.nrgb_syev_batched_dev.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp]
     lib.nrgb_gemm_grouped_dev.argtypes = [vp, C.c_int, C.POINTER(GemmOut), C.c_int, C.POINTER(GemmTerm), vp]
     lib.nrgb_run.argtypes = [vp, C.c_char_p, C.c_char_p, dp]
+    lib.nrgb_set_eig_mode.argtypes = [vp, C.c_int]
     lib.nrgb_eig_recalc_step.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                          C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp)]
     lib.nrgb_eig_recalc_step_dev.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                              C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp), vp]
     lib.nrgb_profile.argtypes = [vp, C.c_int]
     lib.nrgb_kernel_stats.argtypes = [vp, C.c_char_p, C.POINTER(C.c_long), dp]
+    lib.nrgb_kernel_work.argtypes = [vp, C.c_char_p, dp]
     lib.nrgb_basis_change_noalloc.argtypes = [C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                               C.POINTER(vp), vp]
+    lib.nrgb_server_create.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(vp)]
+    lib.nrgb_server_submit.argtypes = [vp, C.c_char_p, C.c_char_p, C.POINTER(C.c_longlong)]
+    lib.nrgb_server_wait.argtypes = [vp, C.c_longlong, C.c_double, dp]
+    lib.nrgb_server_error.argtypes = [vp, C.c_longlong]
+    lib.nrgb_server_error.restype = C.c_char_p
+    lib.nrgb_server_counters.argtypes = [vp, dp]
+    lib.nrgb_server_destroy.argtypes = [vp]
+    lib.nrgb_project_bytes.argtypes = [C.c_char_p, dp]
     _lib = lib
     return lib
 
@@ -140,8 +153,79 @@ class Context:
                     "nrgb_kernel_stats")
         return n.value, ms.value
 
+    def kernel_work(self, name="*"):
+        """Algorithmic work (bytes or flops) stated for the launches of `name`."""
+        w = C.c_double()
+        self._check(self.lib.nrgb_kernel_work(self.h, name.encode(), C.byref(w)), "nrgb_kernel_work")
+        return w.value
+
+    def set_eig_mode(self, mode: int):
+        """0: one batched eigensolver call per step; 1: one call per block."""
+        self._check(self.lib.nrgb_set_eig_mode(self.h, mode), "nrgb_set_eig_mode")
+
     def run(self, workdir: str, outdir: str):
         stats = (C.c_double * 8)()
         self._check(self.lib.nrgb_run(self.h, workdir.encode(), outdir.encode(), stats), "nrgb_run")
-        keys = ["wall_s", "diag_s", "recalc_s", "dm_s", "spec_s", "launches", "h2d_bytes", "d2h_bytes"]
-        return dict(zip(keys, list(stats)))
+        return dict(zip(RUN_KEYS, list(stats)))
+
+
+RUN_KEYS = ["wall_s", "diag_s", "recalc_s", "dm_s", "spec_s", "launches", "h2d_bytes", "d2h_bytes"]
+SERVED_KEYS = RUN_KEYS + ["latency_s", "queue_s", "projected_bytes", "peak_bytes", "eig_calls", "order"]
+COUNTER_KEYS = ["done", "failed", "eig_calls", "eig_requests", "eig_blocks", "peak_running",
+                "peak_admitted_bytes", "budget_bytes"]
+
+
+def project_bytes(workdir: str) -> float:
+    """Projected device bytes of one run (host only, no device needed)."""
+    lib = load()
+    b = C.c_double()
+    rc = lib.nrgb_project_bytes(workdir.encode(), C.byref(b))
+    if rc != 0:
+        raise RuntimeError("nrgb_project_bytes failed (status %d) for %s" % (rc, workdir))
+    return b.value
+
+
+class Server:
+    """Run server on one device: submit() queues an NRG run, wait() returns
+    its statistics (SERVED_KEYS).  Thread-safe."""
+
+    def __init__(self, device: int = 0, max_runs: int = 8, mem_budget_bytes: float = 0.0,
+                 batch_window_us: float = 2000.0):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.nrgb_server_create(device, max_runs, mem_budget_bytes, batch_window_us, C.byref(h))
+        if rc != 0:
+            raise RuntimeError("nrgb_server_create failed (status %d)" % rc)
+        self.h = h
+
+    def submit(self, workdir: str, outdir: str) -> int:
+        t = C.c_longlong()
+        rc = self.lib.nrgb_server_submit(self.h, workdir.encode(), outdir.encode(), C.byref(t))
+        if rc != 0:
+            raise RuntimeError("nrgb_server_submit failed: %s" % self.lib.nrgb_server_error(self.h, 0).decode())
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float = -1.0):
+        stats = (C.c_double * 14)()
+        rc = self.lib.nrgb_server_wait(self.h, ticket, timeout_s, stats)
+        if rc == 7:
+            raise TimeoutError("run %d not finished after %.1f s" % (ticket, timeout_s))
+        if rc != 0:
+            raise RuntimeError("run %d failed: %s" % (ticket, self.lib.nrgb_server_error(self.h, ticket).decode()))
+        return dict(zip(SERVED_KEYS, list(stats)))
+
+    def counters(self):
+        out = (C.c_double * 8)()
+        self.lib.nrgb_server_counters(self.h, out)
+        return dict(zip(COUNTER_KEYS, list(out)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.nrgb_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

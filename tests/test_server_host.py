@@ -1,0 +1,44 @@
+"""Host side of the run server (no device needed): the memory projection
+used for admission, and the refusals of the C ABI without a GPU."""
+import os
+
+import pytest
+
+import inputgen
+
+
+def _run(root, keep, Nmax, fdm=True, z=1.0):
+    wd = os.path.join(root, "k%d_n%d_%d" % (keep, Nmax, fdm))
+    inputgen.make_siam(wd, 0.2, -0.1, 0.02, 2.0, Nmax, z=z,
+                       params={"keep": keep, "fdm": fdm, "dmnrg": not fdm, "T": 1e-5, "specd": "A_d-A_d"})
+    return wd
+
+
+def test_projection_grows_with_keep_and_chain_length(tmp_path):
+    import nrgb
+    p = {k: nrgb.project_bytes(_run(str(tmp_path), k, 20)) for k in (100, 200, 400)}
+    assert p[100] < p[200] < p[400]
+    # eigenvectors of every step are held: each step adds D^2 + D doubles
+    # (D = 4 (keep + safeguardmax) bounds the block dimensions) and two
+    # K'^2 density matrices with FDM
+    p40 = nrgb.project_bytes(_run(str(tmp_path), 200, 40))
+    kp = 200 + 200
+    dim = 4 * kp
+    assert p40 - p[200] == pytest.approx(8.0 * 20 * (dim * dim + dim + 2 * kp * kp), rel=1e-12)
+    assert p[200] >= 8.0 * 20 * dim * dim
+
+
+def test_projection_rejects_missing_input(tmp_path):
+    import nrgb
+    with pytest.raises(RuntimeError):
+        nrgb.project_bytes(str(tmp_path / "nothing"))
+
+
+def test_server_needs_a_device():
+    import torch
+
+    import nrgb
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(RuntimeError, match="status 3"):
+        nrgb.Server(0)
