@@ -147,7 +147,7 @@ def fp64_gemm_peak(torch, dev):
     return 2.0 * n ** 3 / best / 1e12
 
 
-KERNELS = ("trd_panel", "gemm_f64_trailing", "gemm_f64_dc", "gemm_f64_bt", "gemm_f64_recalc", "gemm_f64_nrg",
+KERNELS = ("trd_panel", "trd_cluster", "gemm_f64_trailing", "gemm_f64_dc", "gemm_f64_bt", "gemm_f64_recalc", "gemm_f64_nrg",
            "dc_prep", "dc_permute", "dc_secular", "dc_lowner", "dc_vectors", "dc_rank", "dc_copy", "dc_leaf",
            "bt_T", "bt_buildV", "syev_small", "assemble*", "spec_dmnrg", "spec_fdm", "merge_bins",
            "gather_diag", "col_scale")
@@ -173,6 +173,15 @@ def roofline(ctx, ks, torch, dev):
                 "peak_source": ("measured" if "hbm_gbs" in peaks else "fallback") + " HBM copy (MEASURED_PEAKS.json hbm_gbs)",
                 "unit": "GB/s", "frac": achieved / peak, "traffic": None, "launches": nl,
                 "avg_launch_ms": ms / nl, "algorithmic_bytes_per_launch": work / nl}
+    if name == "trd_cluster":
+        # (4/3) n^3 flops per block on the FP64 pipe (B200's FP64 vector and
+        # tensor rates are the same; the measured DGEMM rate is the peak)
+        peak = fp64_gemm_peak(torch, dev)
+        achieved = work / (ms / 1000.0) / 1e12
+        return {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": peak,
+                "peak_source": "measured cuBLAS DGEMM 8192^3 in this run", "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None, "launches": nl, "avg_launch_ms": ms / nl,
+                "algorithmic_flops_per_launch": work / nl}
     if name.startswith("gemm_f64"):
         peak = fp64_gemm_peak(torch, dev)
         achieved = work / (ms / 1000.0) / 1e12

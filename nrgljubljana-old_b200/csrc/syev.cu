@@ -13,7 +13,10 @@
 //    "middle way" model) in coordinates relative to the nearer pole, and
 //    eigenvectors from the Loewner-formula z-hat (Gu & Eisenstat 1995), which
 //    keeps them orthogonal without extra precision.
+#include <cooperative_groups.h>
 #include <math.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include <algorithm>
 #include <numeric>
@@ -30,6 +33,8 @@ constexpr int LEAF = 32;        // D&C leaf size
 constexpr int NB = 32;          // tridiagonalisation panel width
 constexpr int NBB = 64;         // back-transformation block of reflectors
 constexpr int TRD_NT = 256;     // threads of the panel kernel
+constexpr int TRDC_NT = 256;    // threads of a CTA of the cluster kernel
+constexpr size_t TRDC_SMEM = 227 * 1024;  // shared memory one CTA of the cluster kernel may use
 constexpr double EPS = 2.220446049250313e-16;
 
 // --------------------------------------------------------------------------
@@ -443,6 +448,216 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
   }
   // a barrier that gave up is reported to the host (the barriers are reset per launch)
   if (tid == 0 && *reinterpret_cast<volatile int*>(&bar->error)) atomicExch(fail, 1);
+}
+
+// --------------------------------------------------------------------------
+// Tridiagonalisation of a medium block inside one thread-block cluster.
+// --------------------------------------------------------------------------
+struct TrdClProb {
+  double* A;    // n x n, ld n: input; on return the reflectors below the subdiagonal
+  double* d;    // n
+  double* e;    // n-1
+  double* tau;  // n-1
+  int n;
+};
+
+// Leading dimension of a column held in shared memory: odd, so that 32 lanes
+// reading the same row of 32 different columns hit 32 different banks.
+__host__ __device__ inline int trdc_ld(int n) { return n | 1; }
+
+// Doubles of dynamic shared memory one CTA needs for a block of size n on
+// a cluster of cl CTAs: its columns (j = rank, rank + cl, ...) in full, then
+// v, y, w (n each), 256 partial dot products, cl partial sums, 2 x 4
+// scalars, 32 reduction slots.
+__host__ __device__ inline size_t trdc_smem_doubles(int n, int cl) {
+  return (size_t)((n + cl - 1) / cl) * trdc_ld(n) + 3 * (size_t)n + 256 + cl + 8 + 32;
+}
+
+// Unblocked Householder tridiagonalisation (the dsytd2 recurrence, lower)
+// of one block per cluster of CL CTAs.  The matrix lives in the CTAs'
+// shared memory, distributed by columns (CTA r holds the columns j with
+// j % CL == r, each in full), so the symmetric product y = A v needs no
+// reduction across CTAs: y_j is the dot product of the held column j with v.
+// Per column c, two cluster barriers:
+//   1. the owner of column c forms the reflector (norm, beta, tau) and
+//      writes its scalars into every CTA; barrier;
+//   2. every CTA reads the owner's column c through distributed shared
+//      memory to form v, computes y_j for its columns (lanes across 32
+//      columns, warps across column groups and row segments) and writes
+//      them, and its part of y^T v, into every CTA; barrier;
+//   3. every CTA forms w = tau y - tau^2/2 (y^T v) v and applies
+//      A -= v w^T + w v^T to its columns (no barrier: the next owner only
+//      reads its own, already updated, column before the next barrier).
+// Output as the panel kernel: d, e, tau, and v below the subdiagonal of A.
+template <int CL>
+__global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* __restrict__ probs) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  const TrdClProb P = probs[blockIdx.x / CL];
+  const int n = P.n;
+  const size_t ld = (size_t)n;
+  const int lds = trdc_ld(n);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int nwarps = TRDC_NT / 32;
+  const int ncol = r < n ? (n - r + CL - 1) / CL : 0;
+  extern __shared__ double sm[];
+  double* Acol = sm;                                     // ncol columns, ld lds
+  double* v = Acol + (size_t)((n + CL - 1) / CL) * lds;  // n
+  double* y = v + n;                                     // n (written by every CTA)
+  double* w = y + n;                                     // n
+  double* ypart = w + n;                                 // 256 partial column dots
+  double* part = ypart + 256;                            // CL partial sums of y^T v
+  double* misc = part + CL;                              // 2 x 4 reflector scalars
+  double* red = misc + 8;                                // 32
+
+  for (int l = 0; l < ncol; ++l) {
+    const double* src = P.A + (size_t)(r + l * CL) * ld;
+    for (int i = tid; i < n; i += TRDC_NT) Acol[(size_t)l * lds + i] = src[i];
+  }
+  cluster.sync();
+
+  for (int c = 0; c < n - 1; ++c) {
+    const int o = c % CL;
+    double* mc = misc + (c & 1) * 4;
+    // ---- 1: reflector of column c (owner) ----
+    if (r == o) {
+      const double* col = Acol + (size_t)(c / CL) * lds;
+      double ss = 0.0;
+      for (int i = c + 2 + tid; i < n; i += TRDC_NT) ss += col[i] * col[i];
+      ss = block_sum(ss, red);
+      const double alpha = col[c + 1];
+      double beta = alpha, tc = 0.0, scal = 0.0;
+      if (ss != 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + ss), alpha);
+        tc = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      if (tid < CL) {
+        double* rm = cluster.map_shared_rank(mc, tid);
+        rm[0] = tc;
+        rm[1] = scal;
+      }
+      if (tid == 0) {
+        P.d[c] = col[c];
+        P.e[c] = beta;
+        P.tau[c] = tc;
+      }
+      for (int i = c + 2 + tid; i < n; i += TRDC_NT) P.A[i + (size_t)c * ld] = col[i] * scal;
+    }
+    cluster.sync();
+    // ---- 2: v, y_j for the columns held here, y^T v ----
+    const double tc = mc[0], scal = mc[1];
+    {
+      const double* ocol = cluster.map_shared_rank(Acol, o) + (size_t)(c / CL) * lds;
+      for (int i = c + 1 + tid; i < n; i += TRDC_NT) v[i] = (i == c + 1) ? 1.0 : ocol[i] * scal;
+    }
+    __syncthreads();
+    // held columns after c: local indices l0 .. ncol-1
+    const int l0 = (c + 1 - r + CL - 1) / CL > 0 ? (c + 1 - r + CL - 1) / CL : 0;
+    const int nact = ncol > l0 ? ncol - l0 : 0;
+    const int chunks = (nact + 31) >> 5;
+    const int segs = chunks ? max(1, nwarps / chunks) : 0;
+    if (warp < chunks * segs) {
+      const int ch = warp % chunks, sg = warp / chunks;
+      const int m = n - c - 1;
+      const int per = (m + segs - 1) / segs;
+      const int i0 = c + 1 + sg * per, i1 = min(n, i0 + per);
+      const int t = ch * 32 + lane;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      if (t < nact) {
+        const double* a = Acol + (size_t)(l0 + t) * lds;
+        int i = i0;
+        for (; i + 3 < i1; i += 4) {
+          s0 += a[i] * v[i];
+          s1 += a[i + 1] * v[i + 1];
+          s2 += a[i + 2] * v[i + 2];
+          s3 += a[i + 3] * v[i + 3];
+        }
+        for (; i < i1; ++i) s0 += a[i] * v[i];
+      }
+      ypart[sg * (chunks * 32) + t] = (s0 + s1) + (s2 + s3);
+    }
+    __syncthreads();
+    double sp = 0.0;
+    for (int t = tid; t < nact; t += TRDC_NT) {
+      double yj = 0.0;
+      for (int sg = 0; sg < segs; ++sg) yj += ypart[sg * (chunks * 32) + t];
+      const int j = r + (l0 + t) * CL;
+#pragma unroll
+      for (int q = 0; q < CL; ++q) cluster.map_shared_rank(y, q)[j] = yj;
+      sp += yj * v[j];
+    }
+    sp = block_sum(sp, red);
+    if (tid < CL) cluster.map_shared_rank(part, tid)[r] = sp;
+    cluster.sync();
+    // ---- 3: w and the rank-2 update of the held columns ----
+    double ytv = 0.0;
+#pragma unroll
+    for (int q = 0; q < CL; ++q) ytv += part[q];
+    const double a2 = -0.5 * tc * tc * ytv;
+    for (int i = c + 1 + tid; i < n; i += TRDC_NT) w[i] = tc * y[i] + a2 * v[i];
+    __syncthreads();
+    if (tc != 0.0) {
+      for (int l = l0 + warp; l < ncol; l += nwarps) {
+        const int j = r + l * CL;
+        double* a = Acol + (size_t)l * lds;
+        const double vj = v[j], wj = w[j];
+        for (int i = c + 1 + lane; i < n; i += 32) a[i] -= v[i] * wj + w[i] * vj;
+      }
+    }
+    __syncthreads();
+  }
+  if (n >= 1 && r == (n - 1) % CL && tid == 0) P.d[n - 1] = Acol[(size_t)((n - 1) / CL) * lds + (n - 1)];
+  // no CTA leaves while another may still read its shared memory
+  cluster.sync();
+}
+
+template <int CL>
+cudaError_t trdc_config(size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int nprob,
+                        cudaStream_t st) {
+  cfg = cudaLaunchConfig_t{};
+  cfg.gridDim = dim3((unsigned)(nprob * CL));
+  cfg.blockDim = dim3(TRDC_NT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CL;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaFuncSetAttribute(trd_cluster_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && CL > 8)
+    e = cudaFuncSetAttribute(trd_cluster_kernel<CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  return e;
+}
+
+// Clusters of CL CTAs with `smem` bytes each that can be resident at once
+// (0: this cluster size is not usable here).
+template <int CL>
+int trdc_max_clusters(size_t smem) {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute at[1];
+  if (trdc_config<CL>(smem, cfg, at, 1, nullptr) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int nc = 0;
+  if (cudaOccupancyMaxActiveClusters(&nc, trd_cluster_kernel<CL>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nc;
+}
+
+template <int CL>
+cudaError_t trdc_launch(const TrdClProb* d, int nprob, size_t smem, cudaStream_t st) {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute at[1];
+  cudaError_t e = trdc_config<CL>(smem, cfg, at, nprob, st);
+  if (e != cudaSuccess) return e;
+  return cudaLaunchKernelEx(&cfg, trd_cluster_kernel<CL>, d);
 }
 
 // --------------------------------------------------------------------------
@@ -1024,11 +1239,35 @@ SyevBatched::SyevBatched() {
   int dev = 0;
   NRGB_CUDA(cudaGetDevice(&dev));
   NRGB_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
+  int optin = 0;
+  NRGB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cl_smem_ = std::min(TRDC_SMEM, (size_t)optin);
+  // NRGB_TRD_PATH=panel keeps every block on the cooperative panel path
+  // (comparisons, or a device where cluster launches are unavailable)
+  const char* path = getenv("NRGB_TRD_PATH");
+  if (path && strcmp(path, "panel") == 0) cl_smem_ = 0;
+  if (cl_smem_ > 0) {
+    cl_max_[0] = trdc_max_clusters<1>(cl_smem_);
+    cl_max_[1] = trdc_max_clusters<2>(cl_smem_);
+    cl_max_[2] = trdc_max_clusters<4>(cl_smem_);
+    cl_max_[3] = trdc_max_clusters<8>(cl_smem_);
+    cl_max_[4] = trdc_max_clusters<16>(cl_smem_);
+  }
+  for (int i = 0; i < NAUX; ++i) {
+    NRGB_CUDA(cudaStreamCreateWithFlags(&aux_[i], cudaStreamNonBlocking));
+    NRGB_CUDA(cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming));
+  }
+  NRGB_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
 }
 
 SyevBatched::~SyevBatched() {
   if (d_err_) cudaFree(d_err_);
   if (d_bar_) cudaFree(d_bar_);
+  for (int i = 0; i < NAUX; ++i) {
+    if (aux_[i]) cudaStreamDestroy(aux_[i]);
+    if (join_[i]) cudaEventDestroy(join_[i]);
+  }
+  if (fork_) cudaEventDestroy(fork_);
 }
 
 namespace {
@@ -1184,6 +1423,63 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       NRGB_CUDA(cudaMemsetAsync(S.Z, 0, nn * sizeof(double), st));
     }
     // ---------------- 1) tridiagonalisation ----------------
+    // Blocks whose matrix fits in the shared memory of a cluster of at most
+    // 16 CTAs: one cluster each (smallest cluster that holds the block).
+    // Launches of different cluster sizes (and, for single-CTA clusters, of
+    // different shared-memory sizes, so that small blocks share an SM) run
+    // concurrently on side streams; the panel launches for the larger
+    // blocks follow on the main stream.
+    std::vector<char> via_cluster(nbig, 0);
+    {
+      constexpr int NG = 8;  // groups: CL = 1 split at n = 64, 96, 128; CL = 2, 4, 8, 16
+      std::vector<TrdClProb> grp[NG];
+      size_t gsmem[NG] = {};
+      for (int b = 0; b < nbig; ++b) {
+        const int n = tp[b].n;
+        for (int k = 0; k < 5; ++k) {
+          const size_t bytes = trdc_smem_doubles(n, 1 << k) * sizeof(double);
+          if (cl_max_[k] > 0 && bytes <= cl_smem_) {
+            const int g = k > 0 ? k + 3 : (n <= 64 ? 0 : n <= 96 ? 1 : n <= 128 ? 2 : 3);
+            grp[g].push_back(TrdClProb{tp[b].A, tp[b].d, tp[b].e, tp[b].tau, n});
+            gsmem[g] = std::max(gsmem[g], bytes);
+            via_cluster[b] = 1;
+            break;
+          }
+        }
+      }
+      int used = 0;
+      TrdClProb* dg[NG] = {};
+      for (int g = NG - 1; g >= 0; --g) {
+        if (grp[g].empty()) continue;
+        dg[g] = arena_.alloc_n<TrdClProb>(grp[g].size());
+        NRGB_CUDA(cudaMemcpyAsync(dg[g], grp[g].data(), grp[g].size() * sizeof(TrdClProb), cudaMemcpyHostToDevice, st));
+      }
+      NRGB_CUDA(cudaEventRecord(fork_, st));
+      for (int g = NG - 1; g >= 0; --g) {
+        if (grp[g].empty()) continue;
+        cudaStream_t sx = aux_[used % NAUX];
+        if (used < NAUX) NRGB_CUDA(cudaStreamWaitEvent(sx, fork_, 0));
+        double fl = 0;
+        for (const TrdClProb& t : grp[g]) fl += 4.0 / 3.0 * (double)t.n * t.n * t.n;
+        KernelStats::get().add_work("trd_cluster", fl);
+        const int np = (int)grp[g].size();
+        const int k = g > 3 ? g - 3 : 0;
+        cudaError_t e = cudaSuccess;
+        NRGB_LAUNCH("trd_cluster", sx,
+                    e = (k == 0)   ? trdc_launch<1>(dg[g], np, gsmem[g], sx)
+                        : (k == 1) ? trdc_launch<2>(dg[g], np, gsmem[g], sx)
+                        : (k == 2) ? trdc_launch<4>(dg[g], np, gsmem[g], sx)
+                        : (k == 3) ? trdc_launch<8>(dg[g], np, gsmem[g], sx)
+                                   : trdc_launch<16>(dg[g], np, gsmem[g], sx));
+        NRGB_CUDA(e);
+        ++launches_;
+        ++used;
+      }
+      for (int i = 0; i < std::min(used, NAUX); ++i) {
+        NRGB_CUDA(cudaEventRecord(join_[i], aux_[i]));
+        NRGB_CUDA(cudaStreamWaitEvent(st, join_[i], 0));
+      }
+    }
     {
       const size_t smem = (size_t)(32 + 4 * NB + 8 + (TRD_NT / 32) * 2 * NB + nmax) * sizeof(double);
       NRGB_CUDA(cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1203,7 +1499,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       for (int j0 = 0; j0 < nmax; j0 += NB) {
         std::vector<int> act;
         for (int b : order)
-          if (tp[b].n > j0) act.push_back(b);
+          if (tp[b].n > j0 && !via_cluster[b]) act.push_back(b);
         for (size_t s0 = 0; s0 < act.size(); s0 += cap) {
           const size_t s1 = std::min(act.size(), s0 + cap);
           const int cnt = (int)(s1 - s0);

@@ -68,6 +68,12 @@ class SyevBatched : public EigSolver {
   int launches_ = 0;
   int coop_ctas_ = 0;
   int sms_ = 0;
+  int cl_max_[5] = {0, 0, 0, 0, 0};  // resident clusters of 1, 2, 4, 8, 16 CTAs (0: not usable)
+  size_t cl_smem_ = 0;                // shared memory per CTA of the cluster kernel
+  // side streams on which the cluster launches of different sizes overlap
+  static constexpr int NAUX = 6;
+  cudaStream_t aux_[NAUX] = {};
+  cudaEvent_t fork_ = nullptr, join_[NAUX] = {};
 };
 
 }  // namespace nrgb

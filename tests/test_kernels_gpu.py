@@ -76,7 +76,12 @@ def _random_sym(n, rng, kind):
     return (A + A.T) / 2
 
 
-SIZES = [1, 2, 3, 5, 16, 31, 32, 33, 40, 64, 65, 100, 129, 257, 600, 1100]
+# covers the warp path (n <= 32), the cluster path (one cluster of 1..16 CTAs
+# per block; single-CTA launches split at 64, 96, 128; the cluster size
+# changes after 167, 236, 332, 464, and blocks above 653 take the
+# cooperative panel path) and the panel path
+SIZES = [1, 2, 3, 5, 16, 31, 32, 33, 40, 64, 65, 96, 97, 100, 128, 129, 167, 168, 236, 237, 257, 332, 333,
+         464, 465, 600, 653, 654, 1100]
 
 
 @pytest.mark.parametrize("kind", ["gauss", "logspaced", "degenerate"])
@@ -94,6 +99,23 @@ def test_syev_batched_host_api(ctx, kind):
         assert res <= 1e-13 * nrm * max(10, n)
         orth = np.abs(Zi.T @ Zi - np.eye(n)).max()
         assert orth <= 1e-13 * max(10, n)
+
+
+def test_syev_per_block_mode_matches_batched(ctx):
+    """One solver call per block gives the same decomposition as one batched
+    call for all blocks (the eigenvector signs may differ)."""
+    rng = np.random.default_rng(11)
+    mats = [_random_sym(n, rng, "degenerate") for n in (40, 170, 300, 500, 700)]
+    w0, Z0 = ctx.syev_batched(mats)
+    ctx.set_eig_mode(1)
+    try:
+        w1, Z1 = ctx.syev_batched(mats)
+    finally:
+        ctx.set_eig_mode(0)
+    for A, a, b, Za, Zb in zip(mats, w0, w1, Z0, Z1):
+        nrm = np.abs(a).max()
+        assert np.max(np.abs(a - b)) <= 1e-13 * nrm * A.shape[0]
+        assert np.abs(A @ Zb - Zb * b).max() <= 1e-13 * nrm * A.shape[0]
 
 
 def test_gemm_grouped_large_tiles(ctx):
