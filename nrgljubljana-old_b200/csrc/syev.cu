@@ -454,11 +454,12 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
 // Tridiagonalisation of a medium block inside one thread-block cluster.
 // --------------------------------------------------------------------------
 struct TrdClProb {
-  double* A;    // n x n, ld n: input; on return the reflectors below the subdiagonal
+  double* A;    // n x n, leading dimension ld: input; on return the reflectors below the subdiagonal
   double* d;    // n
   double* e;    // n-1
   double* tau;  // n-1
   int n;
+  int ld;       // n for a whole block; the block's size for its trailing part
 };
 
 // Leading dimension of a column held in shared memory: odd, so that 32 lanes
@@ -467,10 +468,58 @@ __host__ __device__ inline int trdc_ld(int n) { return n | 1; }
 
 // Doubles of dynamic shared memory one CTA needs for a block of size n on
 // a cluster of cl CTAs: its columns (j = rank, rank + cl, ...) in full, then
-// v, y, w (n each), 256 partial dot products, cl partial sums, 2 x 4
-// scalars, 32 reduction slots.
+// v, y, w (n each), one partial dot product per thread, one partial sum
+// per warp and per CTA, 2 x 4 scalars.
 __host__ __device__ inline size_t trdc_smem_doubles(int n, int cl) {
-  return (size_t)((n + cl - 1) / cl) * trdc_ld(n) + 3 * (size_t)n + 256 + cl + 8 + 32;
+  return (size_t)((n + cl - 1) / cl) * trdc_ld(n) + 3 * (size_t)n + TRDC_NT + TRDC_NT / 32 + (size_t)cl + 8;
+}
+
+// Barrier over the CTAs of the cluster (a plain CTA barrier for CL = 1).
+template <int CL>
+__device__ __forceinline__ void trdc_sync() {
+  if constexpr (CL == 1) {
+    __syncthreads();
+  } else {
+    cooperative_groups::this_cluster().sync();
+  }
+}
+
+// Address of `p` in the shared memory of CTA `rank` of the cluster.
+template <int CL, class T>
+__device__ __forceinline__ T* trdc_at(T* p, int rank) {
+  if constexpr (CL == 1) {
+    return p;
+  } else {
+    return cooperative_groups::this_cluster().map_shared_rank(p, rank);
+  }
+}
+
+// Reflector of column cc, held in shared memory (`col`), by one warp of its
+// owner: beta, tau and the scale of v, written into every CTA's scalars
+// `mc`; d, e, tau to global memory.
+template <int CL>
+__device__ __forceinline__ void trdc_reflector(const TrdClProb& P, const double* col, int cc, int n, double* mc,
+                                               int lane) {
+  double ss = 0.0;
+  for (int i = cc + 2 + lane; i < n; i += 32) ss += col[i] * col[i];
+  ss = warp_sum(ss);
+  const double alpha = col[cc + 1];
+  double beta = alpha, tc = 0.0, scal = 0.0;
+  if (ss != 0.0) {
+    beta = -copysign(sqrt(alpha * alpha + ss), alpha);
+    tc = (beta - alpha) / beta;
+    scal = 1.0 / (alpha - beta);
+  }
+  if (lane < CL) {
+    double* rm = trdc_at<CL>(mc, lane);
+    rm[0] = tc;
+    rm[1] = scal;
+  }
+  if (lane == 0) {
+    P.d[cc] = col[cc];
+    P.e[cc] = beta;
+    P.tau[cc] = tc;
+  }
 }
 
 // Unblocked Householder tridiagonalisation (the dsytd2 recurrence, lower)
@@ -479,24 +528,23 @@ __host__ __device__ inline size_t trdc_smem_doubles(int n, int cl) {
 // j % CL == r, each in full), so the symmetric product y = A v needs no
 // reduction across CTAs: y_j is the dot product of the held column j with v.
 // Per column c, two cluster barriers:
-//   1. the owner of column c forms the reflector (norm, beta, tau) and
-//      writes its scalars into every CTA; barrier;
-//   2. every CTA reads the owner's column c through distributed shared
+//   a. every CTA reads the owner's column c through distributed shared
 //      memory to form v, computes y_j for its columns (lanes across 32
 //      columns, warps across column groups and row segments) and writes
 //      them, and its part of y^T v, into every CTA; barrier;
-//   3. every CTA forms w = tau y - tau^2/2 (y^T v) v and applies
-//      A -= v w^T + w v^T to its columns (no barrier: the next owner only
-//      reads its own, already updated, column before the next barrier).
+//   b. every CTA forms w = tau y - tau^2/2 (y^T v) v and applies
+//      A -= v w^T + w v^T to its columns (loads of four columns and two
+//      rows issued before their stores).  Meanwhile warp 0 of the owner of
+//      column c+1 updates that column first and forms its reflector (norm,
+//      beta, tau), writing the scalars into every CTA; barrier.
 // Output as the panel kernel: d, e, tau, and v below the subdiagonal of A.
 template <int CL>
 __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* __restrict__ probs) {
-  namespace cg = cooperative_groups;
-  cg::cluster_group cluster = cg::this_cluster();
-  const int r = (int)cluster.block_rank();
+  int r = 0;
+  if constexpr (CL > 1) r = (int)cooperative_groups::this_cluster().block_rank();
   const TrdClProb P = probs[blockIdx.x / CL];
   const int n = P.n;
-  const size_t ld = (size_t)n;
+  const size_t ld = (size_t)P.ld;
   const int lds = trdc_ld(n);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int nwarps = TRDC_NT / 32;
@@ -506,50 +554,28 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
   double* v = Acol + (size_t)((n + CL - 1) / CL) * lds;  // n
   double* y = v + n;                                     // n (written by every CTA)
   double* w = y + n;                                     // n
-  double* ypart = w + n;                                 // 256 partial column dots
-  double* part = ypart + 256;                            // CL partial sums of y^T v
+  double* ypart = w + n;                                 // TRDC_NT partial column dots
+  double* wpart = ypart + TRDC_NT;                       // nwarps parts of y^T v
+  double* part = wpart + nwarps;                         // CL parts of y^T v, one per CTA
   double* misc = part + CL;                              // 2 x 4 reflector scalars
-  double* red = misc + 8;                                // 32
 
   for (int l = 0; l < ncol; ++l) {
     const double* src = P.A + (size_t)(r + l * CL) * ld;
     for (int i = tid; i < n; i += TRDC_NT) Acol[(size_t)l * lds + i] = src[i];
   }
-  cluster.sync();
+  // every CTA of the cluster has started (and loaded) before any of them
+  // touches another's shared memory
+  trdc_sync<CL>();
+  if (n > 1 && r == 0 && warp == 0) trdc_reflector<CL>(P, Acol, 0, n, misc, lane);
+  trdc_sync<CL>();
 
   for (int c = 0; c < n - 1; ++c) {
     const int o = c % CL;
-    double* mc = misc + (c & 1) * 4;
-    // ---- 1: reflector of column c (owner) ----
-    if (r == o) {
-      const double* col = Acol + (size_t)(c / CL) * lds;
-      double ss = 0.0;
-      for (int i = c + 2 + tid; i < n; i += TRDC_NT) ss += col[i] * col[i];
-      ss = block_sum(ss, red);
-      const double alpha = col[c + 1];
-      double beta = alpha, tc = 0.0, scal = 0.0;
-      if (ss != 0.0) {
-        beta = -copysign(sqrt(alpha * alpha + ss), alpha);
-        tc = (beta - alpha) / beta;
-        scal = 1.0 / (alpha - beta);
-      }
-      if (tid < CL) {
-        double* rm = cluster.map_shared_rank(mc, tid);
-        rm[0] = tc;
-        rm[1] = scal;
-      }
-      if (tid == 0) {
-        P.d[c] = col[c];
-        P.e[c] = beta;
-        P.tau[c] = tc;
-      }
-      for (int i = c + 2 + tid; i < n; i += TRDC_NT) P.A[i + (size_t)c * ld] = col[i] * scal;
-    }
-    cluster.sync();
-    // ---- 2: v, y_j for the columns held here, y^T v ----
+    const double* mc = misc + (c & 1) * 4;
+    // ---- a: v, y_j for the columns held here, parts of y^T v ----
     const double tc = mc[0], scal = mc[1];
     {
-      const double* ocol = cluster.map_shared_rank(Acol, o) + (size_t)(c / CL) * lds;
+      const double* ocol = trdc_at<CL>(Acol, o) + (size_t)(c / CL) * lds;
       for (int i = c + 1 + tid; i < n; i += TRDC_NT) v[i] = (i == c + 1) ? 1.0 : ocol[i] * scal;
     }
     __syncthreads();
@@ -585,32 +611,89 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
       for (int sg = 0; sg < segs; ++sg) yj += ypart[sg * (chunks * 32) + t];
       const int j = r + (l0 + t) * CL;
 #pragma unroll
-      for (int q = 0; q < CL; ++q) cluster.map_shared_rank(y, q)[j] = yj;
+      for (int q = 0; q < CL; ++q) trdc_at<CL>(y, q)[j] = yj;
       sp += yj * v[j];
     }
-    sp = block_sum(sp, red);
-    if (tid < CL) cluster.map_shared_rank(part, tid)[r] = sp;
-    cluster.sync();
-    // ---- 3: w and the rank-2 update of the held columns ----
+    sp = warp_sum(sp);
+    if (lane == 0) wpart[warp] = sp;
+    __syncthreads();
+    if (warp == 0) {
+      const double x = warp_sum(lane < nwarps ? wpart[lane] : 0.0);
+      if (lane < CL) trdc_at<CL>(part, lane)[r] = x;
+    }
+    trdc_sync<CL>();
+    // ---- b: w, the rank-2 update, the next reflector ----
     double ytv = 0.0;
 #pragma unroll
     for (int q = 0; q < CL; ++q) ytv += part[q];
     const double a2 = -0.5 * tc * tc * ytv;
     for (int i = c + 1 + tid; i < n; i += TRDC_NT) w[i] = tc * y[i] + a2 * v[i];
+    if (r == o)
+      for (int i = c + 2 + tid; i < n; i += TRDC_NT) P.A[i + (size_t)c * ld] = v[i];
     __syncthreads();
-    if (tc != 0.0) {
-      for (int l = l0 + warp; l < ncol; l += nwarps) {
-        const int j = r + l * CL;
-        double* a = Acol + (size_t)l * lds;
-        const double vj = v[j], wj = w[j];
-        for (int i = c + 1 + lane; i < n; i += 32) a[i] -= v[i] * wj + w[i] * vj;
+    const int cn = c + 1;
+    const bool own_next = cn < n - 1 && r == cn % CL;  // column cn is then local column l0
+    const int wfirst = own_next ? 1 : 0;
+    if (tc != 0.0 && warp >= wfirst) {
+      const int nw = nwarps - wfirst;
+      for (int l = l0 + wfirst + 4 * (warp - wfirst); l < ncol; l += 4 * nw) {
+        const int nl = min(4, ncol - l);
+        double vj[4], wj[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int j = r + (l + min(k, nl - 1)) * CL;
+          vj[k] = v[j];
+          wj[k] = w[j];
+        }
+        double* a0 = Acol + (size_t)l * lds;
+        int i = c + 1 + lane;
+        for (; i + 32 < n; i += 64) {
+          const double v0 = v[i], w0 = w[i], v1 = v[i + 32], w1 = w[i + 32];
+          double x[8];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            x[k] = k < nl ? a0[(size_t)k * lds + i] : 0.0;
+            x[4 + k] = k < nl ? a0[(size_t)k * lds + i + 32] : 0.0;
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            x[k] -= v0 * wj[k] + w0 * vj[k];
+            x[4 + k] -= v1 * wj[k] + w1 * vj[k];
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (k < nl) {
+              a0[(size_t)k * lds + i] = x[k];
+              a0[(size_t)k * lds + i + 32] = x[4 + k];
+            }
+        }
+        if (i < n) {
+          const double v0 = v[i], w0 = w[i];
+          double x[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) x[k] = k < nl ? a0[(size_t)k * lds + i] : 0.0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) x[k] -= v0 * wj[k] + w0 * vj[k];
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (k < nl) a0[(size_t)k * lds + i] = x[k];
+        }
       }
     }
-    __syncthreads();
+    if (own_next && warp == 0) {
+      double* col = Acol + (size_t)l0 * lds;
+      if (tc != 0.0) {
+        const double vj = v[cn], wj = w[cn];
+        for (int i = c + 1 + lane; i < n; i += 32) col[i] -= v[i] * wj + w[i] * vj;
+        __syncwarp();
+      }
+      trdc_reflector<CL>(P, col, cn, n, misc + (cn & 1) * 4, lane);
+    }
+    trdc_sync<CL>();
   }
   if (n >= 1 && r == (n - 1) % CL && tid == 0) P.d[n - 1] = Acol[(size_t)((n - 1) / CL) * lds + (n - 1)];
   // no CTA leaves while another may still read its shared memory
-  cluster.sync();
+  trdc_sync<CL>();
 }
 
 template <int CL>
@@ -658,6 +741,25 @@ cudaError_t trdc_launch(const TrdClProb* d, int nprob, size_t smem, cudaStream_t
   cudaError_t e = trdc_config<CL>(smem, cfg, at, nprob, st);
   if (e != cudaSuccess) return e;
   return cudaLaunchKernelEx(&cfg, trd_cluster_kernel<CL>, d);
+}
+
+// --------------------------------------------------------------------------
+// Zero fill of many device ranges in one launch (one CTA per range of at
+// most ZERO_CHUNK doubles).
+// --------------------------------------------------------------------------
+struct ZeroSeg {
+  double* p;
+  long long n;
+};
+constexpr long long ZERO_CHUNK = 32768;
+
+__global__ void zero_kernel(const ZeroSeg* __restrict__ segs) {
+  const ZeroSeg z = segs[blockIdx.x];
+  for (long long i = threadIdx.x; i < z.n; i += blockDim.x) z.p[i] = 0.0;
+}
+
+void zero_add(std::vector<ZeroSeg>& v, double* p, long long n) {
+  for (long long o = 0; o < n; o += ZERO_CHUNK) v.push_back(ZeroSeg{p + o, std::min(ZERO_CHUNK, n - o)});
 }
 
 // --------------------------------------------------------------------------
@@ -1253,6 +1355,13 @@ SyevBatched::SyevBatched() {
     cl_max_[3] = trdc_max_clusters<8>(cl_smem_);
     cl_max_[4] = trdc_max_clusters<16>(cl_smem_);
   }
+  // largest block the cluster kernel holds
+  for (int k = 4; k >= 0 && cl_nmax_ == 0; --k) {
+    if (cl_max_[k] <= 0) continue;
+    int n = 1;
+    while (trdc_smem_doubles(n + 1, 1 << k) * sizeof(double) <= cl_smem_) ++n;
+    cl_nmax_ = n > SMALL_N ? n : 0;
+  }
   for (int i = 0; i < NAUX; ++i) {
     NRGB_CUDA(cudaStreamCreateWithFlags(&aux_[i], cudaStreamNonBlocking));
     NRGB_CUDA(cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming));
@@ -1311,6 +1420,12 @@ size_t SyevBatched::workspace_bytes(const std::vector<int>& ns) {
   for (int n : ns) nmx = std::max(nmx, n);
   // per-panel launch descriptors
   pl.add<char>((size_t)(nmx / NB + 2) * (ns.size() * (sizeof(TrdProb) + 2 * sizeof(GemmSeg) + sizeof(GemmProb)) + 2048));
+  // zero-fill descriptors: the per-problem buffers once, the split-K
+  // outputs of every back-transformation block; cluster descriptors
+  size_t zs = 0;
+  for (int n : ns) zs += 4 + (size_t)n * n / ZERO_CHUNK + 2 * (NBB * (size_t)n / ZERO_CHUNK + 2) * (n / NBB + 2);
+  pl.add<ZeroSeg>(zs);
+  pl.add<TrdClProb>(2 * ns.size() + 16);
   return pl.bytes + (size_t)ns.size() * 4096 + (1 << 20);
 }
 
@@ -1355,6 +1470,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     std::vector<DcProb> dp(nbig);
     std::vector<BtProb> bp(nbig);
     std::vector<double*> dT(nbig), eT(nbig), tauT(nbig);
+    std::vector<ZeroSeg> zeros;  // ranges that must start at zero, cleared in one launch
     for (int b = 0; b < nbig; ++b) {
       const SyevDesc& S = probs[big[b]];
       const int n = S.n;
@@ -1418,9 +1534,16 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       bt.T = T;
       bt.X = X;
       bt.Y = Y;
-      NRGB_CUDA(cudaMemsetAsync(red, 0, 2 * RED * sizeof(double), st));
-      NRGB_CUDA(cudaMemsetAsync(tauT[b], 0, n * sizeof(double), st));
-      NRGB_CUDA(cudaMemsetAsync(S.Z, 0, nn * sizeof(double), st));
+      zero_add(zeros, red, 2 * RED);
+      zero_add(zeros, tauT[b], n);
+      zero_add(zeros, S.Z, (long long)nn);
+    }
+    if (!zeros.empty()) {
+      ZeroSeg* d_z = arena_.alloc_n<ZeroSeg>(zeros.size());
+      NRGB_CUDA(cudaMemcpyAsync(d_z, zeros.data(), zeros.size() * sizeof(ZeroSeg), cudaMemcpyHostToDevice, st));
+      NRGB_LAUNCH("zero_fill", st, zero_kernel<<<(unsigned)zeros.size(), 256, 0, st>>>(d_z));
+      NRGB_CUDA(cudaGetLastError());
+      ++launches_;
     }
     // ---------------- 1) tridiagonalisation ----------------
     // Blocks whose matrix fits in the shared memory of a cluster of at most
@@ -1430,19 +1553,21 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     // concurrently on side streams; the panel launches for the larger
     // blocks follow on the main stream.
     std::vector<char> via_cluster(nbig, 0);
-    {
-      constexpr int NG = 8;  // groups: CL = 1 split at n = 64, 96, 128; CL = 2, 4, 8, 16
+    // Launch the cluster tridiagonalisation for `list`: groups by cluster size
+    // (single-CTA clusters split at n = 64, 96, 128), concurrently on side
+    // streams, joined into `st`.  Every entry must fit some cluster size.
+    auto launch_clusters = [&](const std::vector<TrdClProb>& list) {
+      constexpr int NG = 8;
       std::vector<TrdClProb> grp[NG];
       size_t gsmem[NG] = {};
-      for (int b = 0; b < nbig; ++b) {
-        const int n = tp[b].n;
+      for (const TrdClProb& t : list) {
+        const int n = t.n;
         for (int k = 0; k < 5; ++k) {
           const size_t bytes = trdc_smem_doubles(n, 1 << k) * sizeof(double);
           if (cl_max_[k] > 0 && bytes <= cl_smem_) {
             const int g = k > 0 ? k + 3 : (n <= 64 ? 0 : n <= 96 ? 1 : n <= 128 ? 2 : 3);
-            grp[g].push_back(TrdClProb{tp[b].A, tp[b].d, tp[b].e, tp[b].tau, n});
+            grp[g].push_back(t);
             gsmem[g] = std::max(gsmem[g], bytes);
-            via_cluster[b] = 1;
             break;
           }
         }
@@ -1479,6 +1604,23 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         NRGB_CUDA(cudaEventRecord(join_[i], aux_[i]));
         NRGB_CUDA(cudaStreamWaitEvent(st, join_[i], 0));
       }
+    };
+    // Larger blocks: panel launches for their leading columns until the
+    // trailing block fits a cluster, whose tridiagonalisation finishes it.
+    std::vector<int> jstop(nbig);
+    {
+      std::vector<TrdClProb> whole;
+      for (int b = 0; b < nbig; ++b) {
+        const int n = tp[b].n;
+        jstop[b] = n;
+        if (cl_nmax_ > 0 && n <= cl_nmax_) {
+          whole.push_back(TrdClProb{tp[b].A, tp[b].d, tp[b].e, tp[b].tau, n, n});
+          via_cluster[b] = 1;
+        } else if (cl_nmax_ > 0) {
+          jstop[b] = ((n - cl_nmax_ + NB - 1) / NB) * NB;
+        }
+      }
+      launch_clusters(whole);
     }
     {
       const size_t smem = (size_t)(32 + 4 * NB + 8 + (TRD_NT / 32) * 2 * NB + nmax) * sizeof(double);
@@ -1499,7 +1641,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       for (int j0 = 0; j0 < nmax; j0 += NB) {
         std::vector<int> act;
         for (int b : order)
-          if (tp[b].n > j0 && !via_cluster[b]) act.push_back(b);
+          if (tp[b].n > j0 && !via_cluster[b] && j0 < jstop[b]) act.push_back(b);
         for (size_t s0 = 0; s0 < act.size(); s0 += cap) {
           const size_t s1 = std::min(act.size(), s0 + cap);
           const int cnt = (int)(s1 - s0);
@@ -1574,6 +1716,17 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           }
         }
       }
+    }
+    // the trailing blocks A[j:, j:] (j = jstop) of the larger blocks, fully
+    // updated by the last trailing update, tridiagonalised in clusters
+    {
+      std::vector<TrdClProb> tails;
+      for (int b = 0; b < nbig; ++b) {
+        const int j = jstop[b], n = tp[b].n;
+        if (via_cluster[b] || j >= n) continue;
+        tails.push_back(TrdClProb{tp[b].A + j + (size_t)j * n, tp[b].d + j, tp[b].e + j, tp[b].tau + j, n - j, n});
+      }
+      launch_clusters(tails);
     }
     // ---------------- 2) divide and conquer ----------------
     {
@@ -1654,6 +1807,15 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         NRGB_LAUNCH("bt_buildV", st, bt_buildV_kernel<<<dim3(NBB, nbig), 128, 0, st>>>(d_bp, j0));
         NRGB_CUDA(cudaGetLastError());
         GemmBatch g1, g3, g4;
+        std::vector<ZeroSeg> bzg, bzx;
+        auto zero_launch = [&](const std::vector<ZeroSeg>& z) {
+          if (z.empty()) return;
+          ZeroSeg* d_z = arena_.alloc_n<ZeroSeg>(z.size());
+          NRGB_CUDA(cudaMemcpyAsync(d_z, z.data(), z.size() * sizeof(ZeroSeg), cudaMemcpyHostToDevice, st));
+          NRGB_LAUNCH("zero_fill", st, zero_kernel<<<(unsigned)z.size(), 256, 0, st>>>(d_z));
+          NRGB_CUDA(cudaGetLastError());
+          ++launches_;
+        };
         for (int b : act) {
           const BtProb& P = bp[b];
           const int n = P.n;
@@ -1670,9 +1832,12 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           s.k = mrows;
           s.alpha = 1.0;
           // one output tile, K = mrows: split the K loop so that many CTAs work
-          NRGB_CUDA(cudaMemsetAsync(P.G, 0, sizeof(double) * NBB * NBB, st));
-          g1.add(P.G, NBB, NBB, NBB, 0.0, {s}, std::max(1, std::min(64, mrows / 256)));
+          // (split-K accumulates with atomics into a zeroed output)
+          const int kg = std::max(1, std::min(64, mrows / 256));
+          if (kg > 1) zero_add(bzg, P.G, (long long)NBB * NBB);
+          g1.add(P.G, NBB, NBB, NBB, 0.0, {s}, kg);
         }
+        zero_launch(bzg);
         {
           GemmProb* d_gp = arena_.alloc_n<GemmProb>(g1.probs.size());
           GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(g1.segs.size());
@@ -1700,8 +1865,9 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           s.transB = 0;
           s.k = mrows;
           s.alpha = 1.0;
-          NRGB_CUDA(cudaMemsetAsync(P.X, 0, sizeof(double) * NBB * n, st));
-          gx.add(P.X, NBB, NBB, n, 0.0, {s}, std::max(1, std::min(16, mrows / 512)));
+          const int kx = std::max(1, std::min(16, mrows / 512));
+          if (kx > 1) zero_add(bzx, P.X, (long long)NBB * n);
+          gx.add(P.X, NBB, NBB, n, 0.0, {s}, kx);
           GemmSeg t{};
           t.A = P.T;
           t.lda = NBB;
@@ -1723,6 +1889,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           u.alpha = -1.0;
           gz.add(Z + r0, n, mrows, n, 1.0, {u});
         }
+        zero_launch(bzx);
         for (GemmBatch* gbp : {&gx, &gy, &gz}) {
           GemmBatch& gb = *gbp;
           GemmProb* d_gp = arena_.alloc_n<GemmProb>(gb.probs.size());

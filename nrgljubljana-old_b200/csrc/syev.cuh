@@ -70,6 +70,7 @@ class SyevBatched : public EigSolver {
   int sms_ = 0;
   int cl_max_[5] = {0, 0, 0, 0, 0};  // resident clusters of 1, 2, 4, 8, 16 CTAs (0: not usable)
   size_t cl_smem_ = 0;                // shared memory per CTA of the cluster kernel
+  int cl_nmax_ = 0;                   // largest block it holds (0: cluster path off)
   // side streams on which the cluster launches of different sizes overlap
   static constexpr int NAUX = 6;
   cudaStream_t aux_[NAUX] = {};
