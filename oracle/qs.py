@@ -15,13 +15,18 @@ from __future__ import annotations
 
 import math
 
-COMBS = {1: 4}
+import qs_derive
+
+COMBS = {1: 4, 2: 16}
 
 # In[i]: quantum-number difference between a subspace and its i-th ancestor
 # (ancestor = I + In[i]); QN[i]: quantum numbers of the states added on the
-# new site (coefnew/qs/qs-1ch-In2.dat, qs-1ch-QN.dat).
-IN = {1: [(1, 0), (0, -1), (0, 1), (-1, 0)]}
-QN = {1: [(-1, 1), (0, 2), (0, 2), (1, 1)]}
+# new site (coefnew/qs/qs-1ch-In2.dat, qs-1ch-QN.dat; for two channels the
+# combinations of qs_derive.COMBOS, which follow qs-2ch-In2.dat, qs-2ch-QN.dat).
+IN = {1: [(1, 0), (0, -1), (0, 1), (-1, 0)],
+      2: [c[2] for c in qs_derive.COMBOS[2]]}
+QN = {1: [(-1, 1), (0, 2), (0, 2), (1, 1)],
+      2: [(sum(c[0]) - 2, int(round(2 * c[1])) + 1) for c in qs_derive.COMBOS[2]]}
 
 SINGLET = (0, 1)   # InvarSinglet
 DOUBLET = (1, 2)   # Invar_f: quantum numbers of f^dag
@@ -56,9 +61,11 @@ def inverse(A):
 def offdiag_terms(nch, ss):
     """Hopping blocks of H_{N+1} in subspace with multiplicity ss:
     (i, j, ch, factor) adds factor*xi_N/SCALE(N+1) * <In[i]||f^dag_ch||In[j]>
-    to block (i, j) (qs-1ch-offdiag.dat)."""
+    to block (i, j) (qs-1ch-offdiag.dat; two channels: derived, qs_derive)."""
+    if nch == 2:
+        return qs_derive.offdiag(2, ss)
     if nch != 1:
-        raise NotImplementedError("oracle restates the 1-channel QS tables")
+        raise NotImplementedError("QS tables for 1 and 2 channels")
     return [(1, 2, 0, 1.0),
             (1, 3, 0, 1.0),
             (2, 4, 0, -math.sqrt((ss - 1) / ss)),
@@ -68,6 +75,8 @@ def offdiag_terms(nch, ss):
 def diag_terms(nch):
     """(i, ch, number): electrons added in channel ch by combination i
     (qs-1ch-diag.dat)."""
+    if nch == 2:
+        return qs_derive.tables(2).diag()
     if nch != 1:
         raise NotImplementedError
     return [(1, 0, 0), (2, 0, 1), (3, 0, 1), (4, 0, 2)]
@@ -76,6 +85,8 @@ def diag_terms(nch):
 def recalc_f_tables(nch, Ip):
     """<I1||f^dag_ch||Ip> of the new site: list of (I1, ch, [(i1, ip, factor)])
     (qs-1ch-spinupa.dat, qs-1ch-spindowna.dat; src/nrg-recalc-QS.cc:210-458)."""
+    if nch == 2:
+        return qs_derive.recalc_f(2, tuple(Ip))
     if nch != 1:
         raise NotImplementedError
     qp, ssp = Ip
@@ -91,6 +102,8 @@ def recalc_f_tables(nch, Ip):
 def doublet_tables(nch, I1):
     """Recalculation of a doublet operator: list of (Ip, [(i1, ip, factor)])
     (qs-1ch-doubletp.dat, qs-1ch-doubletm.dat; src/nrg-recalc-QS.cc:34-203)."""
+    if nch == 2:
+        return qs_derive.doublet(2, tuple(I1))
     if nch != 1:
         raise NotImplementedError
     q1, ss1 = I1
@@ -105,6 +118,8 @@ def doublet_tables(nch, I1):
 def triplet_tables(nch, I1):
     """Recalculation of a triplet (spin) operator: list of (Ip, rows)
     (qs-1ch-triplets.dat, tripletp.dat, tripletm.dat; src/nrg-recalc-QS.cc:497-697)."""
+    if nch == 2:
+        return qs_derive.triplet(2, tuple(I1))
     if nch != 1:
         raise NotImplementedError
     q1, ss1 = I1

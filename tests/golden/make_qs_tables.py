@@ -1,6 +1,6 @@
-"""Generate tests/golden/qs_tables.json from the reference's QS coefficient
-tables (coefnew/qs/qs-1ch-*.dat), evaluated numerically for a range of spin
-multiplicities.  Run in a container that has the reference checkout:
+"""Generate tests/golden/qs_tables.json and qs_tables_2ch.json from the
+reference's QS coefficient tables (coefnew/qs/qs-1ch-*.dat, qs-2ch-*.dat),
+evaluated numerically for a range of spin multiplicities.  Run in a container that has the reference checkout:
 
     python tests/golden/make_qs_tables.py /root/reference
 
@@ -56,11 +56,15 @@ def _split_args(s):
     return out
 
 
-def main(refroot, out):
+FILES_2CH = ["offdiag", "diag", "spinupa", "spinupb", "spindowna", "spindownb", "doubletp", "doubletm",
+             "triplets", "tripletp", "tripletm", "In2", "QN"]
+
+
+def main(refroot, out, channels=1, files=FILES, indent=1):
     base = os.path.join(refroot, "coefnew", "qs")
     result = {"ss_range": [1, 40], "tables": {}}
-    for name in FILES:
-        path = os.path.join(base, "qs-1ch-%s.dat" % name)
+    for name in files:
+        path = os.path.join(base, "qs-%dch-%s.dat" % (channels, name))
         rows = []
         with open(path) as fh:
             for line in fh:
@@ -81,7 +85,7 @@ def main(refroot, out):
                     rows.append({"i": int(args[0]), "ch": int(args[1]), "number": float(args[2])})
                     continue
                 args = _split_args(line[line.index("{") + 1:line.rindex("}")])
-                if name in ("spinupa", "spindowna"):
+                if name.startswith("spinup") or name.startswith("spindown"):
                     vals = {ss: _eval(args[2], ssp=ss) for ss in range(1, 41)}
                     rows.append({"i1": int(args[0]), "ip": int(args[1]), "factor": vals})
                 else:
@@ -93,9 +97,11 @@ def main(refroot, out):
                                  "factor": vals})
         result["tables"][name] = rows
     with open(out, "w") as fh:
-        json.dump(result, fh, indent=1, sort_keys=True)
+        json.dump(result, fh, indent=indent, sort_keys=True)
 
 
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    main(ref, os.path.join(os.path.dirname(os.path.abspath(__file__)), "qs_tables.json"))
+    here = os.path.dirname(os.path.abspath(__file__))
+    main(ref, os.path.join(here, "qs_tables.json"))
+    main(ref, os.path.join(here, "qs_tables_2ch.json"), channels=2, files=FILES_2CH, indent=None)

@@ -74,6 +74,67 @@ def test_kondo_energies_match_exact_diagonalisation(tmp_path):
         assert np.max(np.abs(np.sort(ev) - _nrg_levels(o.steps[N]))) < 1e-12
 
 
+def _sparse_fock(nmodes):
+    """Sparse Jordan-Wigner creation operators of `nmodes` modes and the
+    occupation table (rows: basis states)."""
+    import scipy.sparse as sp
+    dim = 1 << nmodes
+    states = np.arange(dim)
+    occ = (states[:, None] >> np.arange(nmodes)[None, :]) & 1
+    cd = []
+    for k in range(nmodes):
+        src = states[occ[:, k] == 0]
+        sign = (-1.0) ** occ[src, :k].sum(1)
+        cd.append(sp.csr_matrix((sign, (src | (1 << k), src)), shape=(dim, dim)))
+    return cd, occ
+
+
+def _sector_eigs(H, occ, keep):
+    """All eigenvalues of H on the basis states `keep`, by blocks of fixed
+    particle number and S_z (H conserves both)."""
+    n = occ.sum(1)
+    sz = occ[:, 0::2].sum(1) - occ[:, 1::2].sum(1)
+    out = []
+    for a in set(n[keep]):
+        for b in set(sz[keep]):
+            idx = np.where(keep & (n == a) & (sz == b))[0]
+            if len(idx):
+                out.append(np.linalg.eigvalsh(H[idx][:, idx].toarray()))
+    return np.sort(np.concatenate(out))
+
+
+def test_two_channel_kondo_energies_match_exact_diagonalisation(tmp_path):
+    """Two-channel QS tables (derived from spin coupling): NRG levels of the
+    first two steps equal the exact spectrum of the two-channel Kondo chain."""
+    J = [0.4, 0.25]
+    info = g.make_kondo(str(tmp_path), J, 2.5, Nmax=2, params={"keep": 100000})
+    o = O.Oracle(str(tmp_path))
+    o.setup()
+    o.sweep1()
+    for N in range(2):
+        L = N + 2                      # chain sites per channel
+        norb = 1 + 2 * L               # orbital 0: impurity; (ch, n) -> 1 + 2n + ch
+        cd, occ = _sparse_fock(2 * norb)
+        c = [x.T.tocsr() for x in cd]
+
+        def spin(o):
+            up, dn = 2 * o, 2 * o + 1
+            return cd[up] @ c[dn], cd[dn] @ c[up], 0.5 * (cd[up] @ c[up] - cd[dn] @ c[dn])
+        spd, smd, szd = spin(0)
+        H = 0 * cd[0]
+        for ch in range(2):
+            sp_, sm_, sz_ = spin(1 + ch)
+            H = H + J[ch] * (szd @ sz_ + 0.5 * (spd @ sm_ + smd @ sp_))
+            for n in range(L - 1):
+                for s_ in (0, 1):
+                    h = cd[2 * (1 + 2 * n + ch) + s_] @ c[2 * (1 + 2 * (n + 1) + ch) + s_]
+                    H = H + info["xi"][n] * (h + h.T)
+        mask = (occ[:, 0] + occ[:, 1]) == 1
+        ev = _sector_eigs(H.tocsr(), occ, mask) / O.SCALE(o.P, N + 1)
+        ev -= ev.min()
+        assert np.max(np.abs(ev - _nrg_levels(o.steps[N]))) < 1e-12
+
+
 def test_doublet_recalculation_matches_exact_diagonalisation(tmp_path):
     U, eps, Gam = 0.3, -0.1, 0.05
     info = g.make_siam(str(tmp_path), U, eps, Gam, 2.0, Nmax=3,

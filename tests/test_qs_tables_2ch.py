@@ -1,0 +1,95 @@
+"""The QS coefficient tables derived from spin coupling (oracle/qs_derive.py)
+agree with the reference's coefnew/qs/qs-1ch-*.dat and qs-2ch-*.dat
+(evaluated into tests/golden/qs_tables.json, qs_tables_2ch.json by
+tests/golden/make_qs_tables.py).
+
+A reference row may be missing from the derivation only where it multiplies
+an empty block: its ancestor subspace does not exist (SS < 1), the site spin
+cannot couple the ancestor to the subspace, or the operator's rank cannot
+connect the two spins.  Every derived row must be in the reference."""
+import json
+import os
+
+import pytest
+
+import qs_derive as QD
+
+HERE = os.path.join(os.path.dirname(__file__), "golden")
+GOLD = {1: json.load(open(os.path.join(HERE, "qs_tables.json")))["tables"],
+        2: json.load(open(os.path.join(HERE, "qs_tables_2ch.json")))["tables"]}
+TOL = 1e-12
+
+
+def _exists(T, i, I):
+    """Combination i (0-based) is a non-empty block of subspace I."""
+    A = T.anc(i, I)
+    return A[1] >= 1 and T._state(i, (I[1] - 1) / 2.0, (I[1] - 1) / 2.0) is not None
+
+
+def _compare(mine, ref, empty):
+    for k, v in mine.items():
+        assert k in ref and ref[k] is not None, ("derived row not in the reference", k, v)
+        assert abs(v - ref[k]) <= TOL * max(1.0, abs(ref[k])), (k, v, ref[k])
+    for k, v in ref.items():
+        if k not in mine and v is not None and abs(v) > TOL:
+            assert empty(k), ("reference row missing from the derivation", k, v)
+
+
+@pytest.mark.parametrize("P", [1, 2])
+def test_in_qn(P):
+    T = GOLD[P]
+    assert [tuple(r["qn"]) for r in sorted(T["In2"], key=lambda r: r["i"])] == [c[2] for c in QD.COMBOS[P]]
+    qn = [(sum(c[0]) - P, int(round(2 * c[1])) + 1) for c in QD.COMBOS[P]]
+    assert [tuple(r["qn"]) for r in sorted(T["QN"], key=lambda r: r["i"])] == qn
+
+
+@pytest.mark.parametrize("P", [1, 2])
+def test_diag(P):
+    assert sorted(QD.tables(P).diag()) == sorted((r["i"], r["ch"], r["number"]) for r in GOLD[P]["diag"])
+
+
+@pytest.mark.parametrize("P", [1, 2])
+@pytest.mark.parametrize("ss", range(1, 31))
+def test_offdiag(P, ss):
+    T = QD.tables(P)
+    I = (0, ss)
+    mine = {(i, j, ch): v for i, j, ch, v in QD.offdiag(P, ss)}
+    ref = {(r["i"], r["j"], r["ch"]): r["factor"][str(ss)] for r in GOLD[P]["offdiag"]}
+    _compare(mine, ref, lambda k: not (_exists(T, k[0] - 1, I) and _exists(T, k[1] - 1, I)))
+
+
+@pytest.mark.parametrize("P", [1, 2])
+@pytest.mark.parametrize("ssp", range(1, 31))
+def test_recalc_f(P, ssp):
+    T = QD.tables(P)
+    Ip = (0, ssp)
+    got = {(I1, ch): rows for I1, ch, rows in QD.recalc_f(P, Ip)}
+    names = [("spinupa", 1, 0), ("spindowna", -1, 0)]
+    if P == 2:
+        names += [("spinupb", 1, 1), ("spindownb", -1, 1)]
+    for name, dss, ch in names:
+        I1 = (1, ssp + dss)
+        if I1[1] < 1:
+            continue
+        mine = {(a, b): v for a, b, v in got.get((I1, ch), [])}
+        ref = {(r["i1"], r["ip"]): r["factor"][str(ssp)] for r in GOLD[P][name]}
+        _compare(mine, ref, lambda k: not (_exists(T, k[0] - 1, I1) and _exists(T, k[1] - 1, Ip)))
+
+
+@pytest.mark.parametrize("P", [1, 2])
+@pytest.mark.parametrize("ss1", range(1, 31))
+def test_chain_operator_tables(P, ss1):
+    T = QD.tables(P)
+    I1 = (0, ss1)
+    d = {Ip: rows for Ip, rows in QD.doublet(P, I1)}
+    t = {Ip: rows for Ip, rows in QD.triplet(P, I1)}
+    for name, Ip, src, rank in (("doubletp", (-1, ss1 + 1), d, 1), ("doubletm", (-1, ss1 - 1), d, 1),
+                                ("triplets", (0, ss1), t, 2), ("tripletp", (0, ss1 + 2), t, 2),
+                                ("tripletm", (0, ss1 - 2), t, 2)):
+        if Ip[1] < 1:
+            continue
+        mine = {(a, b): v for a, b, v in src.get(Ip, [])}
+        ref = {(r["i1"], r["ip"]): r["factor"][str(ss1)] for r in GOLD[P][name]}
+        # the operator's rank cannot connect the two spins: every block is empty
+        forbidden = not (abs(ss1 - Ip[1]) <= rank <= ss1 + Ip[1] - 2)
+        _compare(mine, ref, lambda k: forbidden or not (_exists(T, k[0] - 1, I1) and _exists(T, k[1] - 1, Ip)))
