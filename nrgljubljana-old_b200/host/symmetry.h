@@ -5,8 +5,9 @@
 // The host expands these tables into flat task lists (assembly terms, GEMM
 // segments) that the device executes; the kernels never see quantum numbers.
 //
-// The QS coefficient tables restate coefnew/qs/qs-1ch-*.dat, each
-// Clebsch-Gordan expression simplified to a closed form in SS; they are
+// The 1-channel QS coefficient tables restate coefnew/qs/qs-1ch-*.dat, each
+// Clebsch-Gordan expression simplified to a closed form in SS; the
+// 2-channel tables are derived from spin coupling (qs_coupling.h).  Both are
 // checked entry by entry against the reference tables by the test suite.
 #pragma once
 #include <math.h>
@@ -15,14 +16,13 @@
 #include <string>
 #include <vector>
 
+#include <memory>
+
 #include "data.h"
+#include "qs_coupling.h"
 
 namespace nrgb {
 
-struct OffdiagTerm { int i, j, ch; double factor; };   // 1-based combination indices
-struct DiagTerm { int i, ch; double number; };
-struct RecalcRow { int i1, ip; double factor; };
-struct RecalcTable { Invar Ip; int ch; std::vector<RecalcRow> rows; };
 
 class Symmetry {
  public:
@@ -57,12 +57,18 @@ class Symmetry {
 class SymmetryQS : public Symmetry {
  public:
   explicit SymmetryQS(int channels) : nch_(channels) {
-    if (channels != 1) throw std::runtime_error("QS symmetry: this build provides the 1-channel tables");
+    if (channels == 2) {
+      cpl_.reset(new QSCoupling(2));
+      in_ = cpl_->In();
+      qn_ = cpl_->QN();
+      return;
+    }
+    if (channels != 1) throw std::runtime_error("QS symmetry: this build provides the 1- and 2-channel tables");
     in_ = {{1, 0}, {0, -1}, {0, 1}, {-1, 0}};
     qn_ = {{-1, 1}, {0, 2}, {0, 2}, {1, 1}};
   }
   std::string name() const override { return "QS"; }
-  int combs() const override { return 4; }
+  int combs() const override { return cpl_ ? cpl_->combs() : 4; }
   const std::vector<Invar>& In() const override { return in_; }
   const std::vector<Invar>& QN() const override { return qn_; }
   int mult(const Invar& I) const override { return I.second; }
@@ -78,12 +84,17 @@ class SymmetryQS : public Symmetry {
   Invar triplet() const override { return {0, 3}; }
 
   std::vector<OffdiagTerm> offdiag(const Invar& I) const override {
+    if (cpl_) return cpl_->offdiag(I.second);
     const double ss = I.second;
     return {{1, 2, 0, 1.0}, {1, 3, 0, 1.0}, {2, 4, 0, -sqrt((ss - 1) / ss)}, {3, 4, 0, sqrt((ss + 1) / ss)}};
   }
-  std::vector<DiagTerm> diag() const override { return {{1, 0, 0.0}, {2, 0, 1.0}, {3, 0, 1.0}, {4, 0, 2.0}}; }
+  std::vector<DiagTerm> diag() const override {
+    if (cpl_) return cpl_->diag();
+    return {{1, 0, 0.0}, {2, 0, 1.0}, {3, 0, 1.0}, {4, 0, 2.0}};
+  }
 
   std::vector<RecalcTable> recalc_f(const Invar& Ip) const override {
+    if (cpl_) return cpl_->recalc_f(Ip);
     const int qp = Ip.first, ssp = Ip.second;
     std::vector<RecalcTable> t;
     t.push_back({{qp + 1, ssp + 1}, 0, {{2, 1, 1.0}, {4, 3, -sqrt(double(ssp) / (ssp + 1))}}});
@@ -91,12 +102,14 @@ class SymmetryQS : public Symmetry {
     return t;
   }
   std::vector<RecalcTable> recalc_doublet(const Invar& I1) const override {
+    if (cpl_) return cpl_->doublet(I1);
     const int q1 = I1.first, ss1 = I1.second;
     const double c = sqrt(double(ss1 - 1) * (ss1 + 1)) / ss1;
     return {{{q1 - 1, ss1 + 1}, 0, {{1, 1, 1.0}, {2, 2, -c}, {3, 2, 1.0 / ss1}, {3, 3, -1.0}, {4, 4, 1.0}}},
             {{q1 - 1, ss1 - 1}, 0, {{1, 1, 1.0}, {2, 2, -1.0}, {2, 3, -1.0 / ss1}, {3, 3, -c}, {4, 4, 1.0}}}};
   }
   std::vector<RecalcTable> recalc_triplet(const Invar& I1) const override {
+    if (cpl_) return cpl_->triplet(I1);
     const int q1 = I1.first, ss1 = I1.second;
     const double S = (ss1 - 1) / 2.0;
     std::vector<RecalcTable> t;
@@ -148,6 +161,7 @@ class SymmetryQS : public Symmetry {
 
  private:
   int nch_;
+  std::unique_ptr<QSCoupling> cpl_;  // derived tables (2 channels)
   std::vector<Invar> in_, qn_;
 };
 

@@ -26,6 +26,11 @@ CASES = {
                         params={"keep": 500, "keepenergy": 10.0, "dmnrg": True, "T": 1e-8,
                                 "specd": "A_d-A_d", "bins": 50, "savebins": True, "broaden": True,
                                 "dumpannotated": 20}),
+    # two-channel Kondo model (QS tables derived from spin coupling): spin and
+    # channel-0 f spectra, DM-NRG and FDM
+    "kondo2ch": dict(model="kondo", J=[0.2, 0.2], Lambda=3.0, Nmax=10,
+                     params={"keep": 300, "dmnrg": True, "fdm": True, "T": 1e-3, "spect": "SZd-SZd",
+                             "specd": "A_f0-A_f0", "bins": 30, "savebins": True, "broaden": False}),
     # one run of the served z-averaging workload (z = 5/8, Nmax = 40), at its
     # smallest Nkeep: FDM A(omega)
     "siam_zshift": dict(model="siam", U=0.2, eps_d=-0.1, Gamma=0.02, Lambda=2.0, Nmax=40, z=0.625,
