@@ -1277,6 +1277,7 @@ struct NrgDriver::Impl {
         explicit Client(EigSolver* e_) : e(e_) { e->client_enter(); }
         ~Client() { e->client_leave(); }
       } client(syev);
+      Section x(this, "sweep1 (all)");
       sweep1(persist);
     }
     if (P.dm) {
@@ -1291,6 +1292,7 @@ struct NrgDriver::Impl {
         calc_fulldensitymatrix();
       }
       t_dm += secs(t1);
+      Section x(this, "sweep2 (all)");
       sweep2(persist);
     }
     sec.reset(new Section(this, "write output"));
@@ -1309,7 +1311,7 @@ struct NrgDriver::Impl {
       fprintf(stderr, "Timing report\n=============\n%20s: %.4f s\n", "All", all);
       for (const auto& kv : sections) {
         fprintf(stderr, "%20s: %.4f s\n", kv.first.c_str(), kv.second);
-        sum += kv.second;
+        if (kv.first.find("(all)") == std::string::npos) sum += kv.second;
       }
       fprintf(stderr, "%20s: %.4f s\n", "Other", all - sum);
     }
