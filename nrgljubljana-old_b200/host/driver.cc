@@ -63,36 +63,51 @@ struct MemCount {
 // The run executing on this host thread (set for the duration of run()).
 thread_local MemCount* tl_mem = nullptr;
 
-// Stream-ordered device allocations owned by one generation of data.
+// Stream-ordered device memory owned by one generation of data.  Requests
+// are carved out of chunks (256-byte aligned) so that thousands of operator
+// blocks per step cost a handful of cudaMallocAsync/cudaFreeAsync calls;
+// chunks grow geometrically from 1 MiB to 64 MiB (a larger request gets a
+// chunk of its own size).
 class Slab {
  public:
   explicit Slab(cudaStream_t s) : st_(s), mc_(tl_mem) {}
   ~Slab() { release(); }
   Slab(const Slab&) = delete;
   double* alloc(size_t n) {
-    void* p = nullptr;
     if (n == 0) return nullptr;
-    NRGB_CUDA(cudaMallocAsync(&p, n * sizeof(double), st_));
-    ptrs_.push_back(p);
-    bytes_ += n * sizeof(double);
-    if (mc_) {
-      mc_->cur += n * sizeof(double);
-      mc_->peak = std::max(mc_->peak, mc_->cur);
+    const size_t bytes = (n * sizeof(double) + 255) & ~size_t(255);
+    if (chunks_.empty() || off_ + bytes > chunks_.back().second) {
+      const size_t sz = std::max(bytes, next_);
+      next_ = std::min(next_ * 2, size_t(64) << 20);
+      void* p = nullptr;
+      NRGB_CUDA(cudaMallocAsync(&p, sz, st_));
+      chunks_.push_back({p, sz});
+      off_ = 0;
+      if (mc_) {
+        mc_->cur += sz;
+        mc_->peak = std::max(mc_->peak, mc_->cur);
+      }
     }
-    return static_cast<double*>(p);
+    char* p = static_cast<char*>(chunks_.back().first) + off_;
+    off_ += bytes;
+    return reinterpret_cast<double*>(p);
   }
   void release() {
-    for (void* p : ptrs_) cudaFreeAsync(p, st_);
-    ptrs_.clear();
-    if (mc_) mc_->cur -= bytes_;
-    bytes_ = 0;
+    for (auto& c : chunks_) {
+      cudaFreeAsync(c.first, st_);
+      if (mc_) mc_->cur -= c.second;
+    }
+    chunks_.clear();
+    off_ = 0;
+    next_ = size_t(1) << 20;
   }
 
  private:
   cudaStream_t st_;
   MemCount* mc_;
-  std::vector<void*> ptrs_;
-  size_t bytes_ = 0;
+  std::vector<std::pair<void*, size_t>> chunks_;
+  size_t off_ = 0;
+  size_t next_ = size_t(1) << 20;
 };
 
 struct Block {
