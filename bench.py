@@ -226,6 +226,20 @@ def mix_rate(per_keep_s, mix):
     return 3600.0 / sum(f * per_keep_s[k] for k, f in mix.items())
 
 
+def max_over_ranks(dist, values, device):
+    """Max over the ranks of each value (the timed spans of the replicas)."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def replica_value(world, runs, span_s):
+    """Whole-job runs/hour of `world` replicas that each served `runs` runs,
+    timed as the slowest replica's span."""
+    return world * 3600.0 * runs / span_s
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -239,7 +253,7 @@ def run_ours(args, rank, world):
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     tmp = tempfile.mkdtemp(prefix="nrgb_bench_")
     try:
         reqs = serve.prepare(stream_waves(args.steps), os.path.join(tmp, "timed"))
@@ -265,11 +279,9 @@ def run_ours(args, rank, world):
         ctx.profile(False)
         span, cspan = res["span_s"], res["client_span_s"]
         if dist:
-            t = torch.tensor([span, cspan], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            span, cspan = float(t[0].item()), float(t[1].item())
-        value = world * 3600.0 * len(reqs) / span
-        e2e_value = world * 3600.0 * len(reqs) / cspan
+            span, cspan = max_over_ranks(dist, [span, cspan], dev)
+        value = replica_value(world, len(reqs), span)
+        e2e_value = replica_value(world, len(reqs), cspan)
         # ---- latency under Poisson arrivals near capacity ----
         latres = serve.serve(srv, lat, LOAD * len(reqs) / res["span_s"])
         cnt = srv.counters()

@@ -207,6 +207,7 @@ struct NrgDriver::Impl {
 
   MemCount mem;
   double eig_calls = 0;
+  std::vector<double> wstage;  // host staging of per-step eigenvalue uploads
 
   Impl(cudaStream_t s, EigSolver* e) : st(s), syev(e) {}
 
@@ -568,6 +569,9 @@ struct NrgDriver::Impl {
       std::vector<AsmOff> ao;
       std::vector<SyevDesc> sd;
       size_t hoff = 0;
+      size_t wtot = 0, woff = 0;
+      for (const auto& kv : S.blocks) wtot += kv.second.dim;
+      double* wall = S.slab->alloc(wtot);
       int maxlen = 0, maxrc = 0;
       for (auto& kv : S.blocks) {
         const Invar& I = kv.first;
@@ -575,7 +579,8 @@ struct NrgDriver::Impl {
         double* Hb = H + hoff;
         hoff += (size_t)b.dim * b.dim;
         b.Z = S.slab->alloc((size_t)b.dim * b.dim);
-        b.w = S.slab->alloc(b.dim);
+        b.w = wall + woff;  // the eigenvalues of a step are contiguous: one copy each way
+        woff += b.dim;
         for (int i = 0; i < sym->combs(); ++i) {
           if (!b.rmax[i]) continue;
           double shift = 0.0;
@@ -609,8 +614,13 @@ struct NrgDriver::Impl {
       sections["sweep1 diag"] += secs(t0);
       ts = Clock::now();
       // eigenvalues to the host: ground state, clusters, truncation
-      for (auto& kv : S.blocks) {
-        kv.second.value = download(kv.second.w, kv.second.dim);
+      {
+        const std::vector<double> wh = download(wall, wtot);
+        size_t o = 0;
+        for (auto& kv : S.blocks) {
+          kv.second.value.assign(wh.begin() + o, wh.begin() + o + kv.second.dim);
+          o += kv.second.dim;
+        }
       }
       double Egs = 1e300;
       for (const auto& kv : S.blocks) Egs = std::min(Egs, kv.second.value[0] + kv.second.shift);
@@ -622,10 +632,14 @@ struct NrgDriver::Impl {
       find_clusters(sorted_energies(S));
       if (fix_splittings(S)) find_clusters(sorted_energies(S));
       truncate_prepare(S, N, false);
-      for (auto& kv : S.blocks) {
-        NRGB_CUDA(cudaMemcpyAsync(kv.second.w, kv.second.value.data(), kv.second.dim * sizeof(double),
-                                  cudaMemcpyHostToDevice, st));
-        h2d += kv.second.dim * sizeof(double);
+      {
+        // the fixed values replace the eigenvalues on the device (one copy);
+        // the staging vector lives until the copy has completed (the next
+        // download synchronises the stream)
+        wstage.clear();
+        for (const auto& kv : S.blocks) wstage.insert(wstage.end(), kv.second.value.begin(), kv.second.value.end());
+        NRGB_CUDA(cudaMemcpyAsync(wall, wstage.data(), wstage.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        h2d += wstage.size() * sizeof(double);
       }
       totalenergy += Egs * scale1;
       for (auto& kv : S.blocks) {
@@ -978,13 +992,15 @@ struct NrgDriver::Impl {
       // absolute energies shifted by the absolute ground state (FDM)
       std::map<Invar, double*> absdev;
       if (P.fdm) {
+        wstage.clear();
+        for (const auto& kv : S.blocks)
+          for (int r = 0; r < kv.second.dim; ++r) wstage.push_back(kv.second.absE[r] - GSenergy);
+        double* d = nslab->alloc(wstage.size());
+        NRGB_CUDA(cudaMemcpyAsync(d, wstage.data(), wstage.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        h2d += wstage.size() * sizeof(double);
         for (const auto& kv : S.blocks) {
-          std::vector<double> a(kv.second.dim);
-          for (int r = 0; r < kv.second.dim; ++r) a[r] = kv.second.absE[r] - GSenergy;
-          double* d = nslab->alloc(a.size());
-          NRGB_CUDA(cudaMemcpyAsync(d, a.data(), a.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-          h2d += a.size() * sizeof(double);
           absdev[kv.first] = d;
+          d += kv.second.dim;
         }
       }
       for (Spec& sp : spectra) {
