@@ -55,7 +55,7 @@ METRIC = "NRG runs/hour and p50/p99 latency, served vs plain FP64 (spectra <=1e-
 WAVE = 32           # requests per step (one z value x 32 eps_d)
 LOAD = 0.85         # Poisson rate for the latency pass, as a fraction of capacity
 LAT_RUNS = 64       # requests in the latency pass
-MAX_RUNS = 8        # worker slots of the server
+MAX_RUNS = 12       # worker slots of the server (best of 8, 12, 16, 24 measured)
 
 # microbenchmark: 40 dense blocks per step, 6 operators per block pair
 NBLOCKS = 40

@@ -245,4 +245,45 @@ cudaError_t col_scale_launch(const ColScale* d_cs, int ncs, int max_rows, int ma
   return cudaGetLastError();
 }
 
+// --------------------------------------------------------------------------
+// Broadening of binned spectra on a mesh
+// --------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ double br_new(double e, double ept, double alpha, double gamma, double omega0) {
+  const double sqpi = 1.7724538509055160273;
+  double pl = 0.0;
+  if (!((e < 0.0 && ept > 0.0) || (e > 0.0 && ept < 0.0) || ept == 0.0)) {
+    const double x = log(e / ept) / alpha - gamma;
+    pl = exp(-x * x) / (alpha * fabs(e) * sqpi);
+  }
+  if (fabs(e) > omega0) return pl;
+  const double l = log(fabs(e) / omega0) / alpha;
+  const double h = exp(-l * l);
+  const double gx = (e - ept) / omega0;
+  return pl * h + exp(-gx * gx) / (omega0 * sqpi) * (1.0 - h);
+}
+
+__global__ void broaden_kernel(const double* __restrict__ e, const double* __restrict__ w, int nb,
+                               const double* __restrict__ mesh, int nmesh, double alpha, double gamma,
+                               double omega0, double* __restrict__ out) {
+  __shared__ double scratch[32];
+  const int k = blockIdx.x;
+  const double E = k < nmesh ? mesh[k] : -mesh[k - nmesh];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) s += w[i] * br_new(E, e[i], alpha, gamma, omega0);
+  s = block_sum(s, scratch);
+  if (threadIdx.x == 0) out[k] = s;
+}
+
+}  // namespace
+
+cudaError_t broaden_launch(const double* d_e, const double* d_w, int nb, const double* d_mesh, int nmesh,
+                           double alpha, double gamma, double omega0, double* d_out, cudaStream_t st) {
+  if (nmesh <= 0) return cudaSuccess;
+  NRGB_LAUNCH("broaden", st,
+              broaden_kernel<<<2 * nmesh, 256, 0, st>>>(d_e, d_w, nb, d_mesh, nmesh, alpha, gamma, omega0, d_out));
+  return cudaGetLastError();
+}
+
 }  // namespace nrgb

@@ -87,4 +87,13 @@ struct ColScale {
 };
 cudaError_t col_scale_launch(const ColScale* d_cs, int ncs, int max_rows, int max_cols, cudaStream_t st);
 
+// Broadened spectral function on a mesh (SpectrumRealFreq::continuous with
+// the BR_NEW kernel, src/spectrumrealfreq.cc:271-306, src/spectral.h:70-102):
+// out[k] = sum_i w[i] K(E_k, e[i]) for E_k = mesh[k] (k < nmesh) and
+// E_k = -mesh[k - nmesh], with K the log-Gaussian of width alpha (shifted by
+// gamma) blended into a Gaussian of width omega0 below |E| = omega0.
+// e[] are the signed bin energies, w[] their weights.  One CTA per point.
+cudaError_t broaden_launch(const double* d_e, const double* d_w, int nb, const double* d_mesh, int nmesh,
+                           double alpha, double gamma, double omega0, double* d_out, cudaStream_t st);
+
 }  // namespace nrgb

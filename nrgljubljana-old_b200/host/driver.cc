@@ -1201,40 +1201,41 @@ struct NrgDriver::Impl {
     }
   }
   // SpectrumRealFreq::continuous with BR_NEW (src/spectrumrealfreq.cc:271-306,
-  // src/spectral.h:70-102): log-Gaussian kernel, Gaussian below omega0.
+  // src/spectral.h:70-102): log-Gaussian kernel, Gaussian below omega0,
+  // evaluated on the device (broaden_kernel) for the mesh
+  // E = broaden_max / broaden_ratio^k down to broaden_min (both signs).
   void write_broadened(const std::string& fn, const std::vector<double>& ep, const std::vector<double>& wp,
                        const std::vector<double>& en, const std::vector<double>& wn_) {
     const double alpha = P.alpha, gamma = alpha / 4.0;
     const double omega0 = P.omega0 < 0.0 ? P.omega0_ratio * P.T : P.omega0;
     const double bmin = P.broaden_min <= 0.0 ? P.broaden_min_ratio * scale_of(P, Nmax) : P.broaden_min;
-    const double sqpi = 1.7724538509055160273;
-    auto brl = [&](double e, double ept) {
-      if ((e < 0.0 && ept > 0.0) || (e > 0.0 && ept < 0.0)) return 0.0;
-      if (ept == 0.0) return 0.0;
-      const double x = log(e / ept) / alpha - gamma;
-      return exp(-x * x) / (alpha * fabs(e) * sqpi);
-    };
-    auto br = [&](double e, double ept) {
-      const double pl = brl(e, ept);
-      if (fabs(e) > omega0) return pl;
-      const double l = log(fabs(e) / omega0) / alpha;
-      const double h = exp(-l * l);
-      const double gx = (e - ept) / omega0;
-      return pl * h + exp(-gx * gx) / (omega0 * sqpi) * (1.0 - h);
-    };
+    std::vector<double> mesh;
+    for (double E = P.broaden_max; E > bmin; E /= P.broaden_ratio) mesh.push_back(E);
+    std::vector<double> e(ep), w(wp);
+    for (size_t i = 0; i < en.size(); ++i) {
+      e.push_back(-en[i]);
+      w.push_back(wn_[i]);
+    }
+    const int nmesh = (int)mesh.size(), nb = (int)e.size();
+    std::vector<double> vals(2 * (size_t)nmesh, 0.0);
+    if (nmesh > 0 && nb > 0) {
+      Slab tmp(st);
+      double* d_e = tmp.alloc(nb);
+      double* d_w = tmp.alloc(nb);
+      double* d_m = tmp.alloc(nmesh);
+      double* d_o = tmp.alloc(2 * (size_t)nmesh);
+      NRGB_CUDA(cudaMemcpyAsync(d_e, e.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+      NRGB_CUDA(cudaMemcpyAsync(d_w, w.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+      NRGB_CUDA(cudaMemcpyAsync(d_m, mesh.data(), nmesh * sizeof(double), cudaMemcpyHostToDevice, st));
+      h2d += (2.0 * nb + nmesh) * sizeof(double);
+      NRGB_CUDA(broaden_launch(d_e, d_w, nb, d_m, nmesh, alpha, gamma, omega0, d_o, st));
+      launches += 1;
+      vals = download(d_o, 2 * (size_t)nmesh);
+    }
     std::vector<std::pair<double, double>> pos, neg;
-    for (double E = P.broaden_max; E > bmin; E /= P.broaden_ratio) {
-      double vp = 0, vn = 0;
-      for (size_t i = 0; i < ep.size(); ++i) {
-        vp += wp[i] * br(E, ep[i]);
-        vn += wp[i] * br(-E, ep[i]);
-      }
-      for (size_t i = 0; i < en.size(); ++i) {
-        vn += wn_[i] * br(-E, -en[i]);
-        vp += wn_[i] * br(E, -en[i]);
-      }
-      pos.push_back({E, vp});
-      neg.push_back({-E, vn});
+    for (int k = 0; k < nmesh; ++k) {
+      pos.push_back({mesh[k], vals[k]});
+      neg.push_back({-mesh[k], vals[nmesh + k]});
     }
     std::sort(pos.begin(), pos.end());
     std::sort(neg.begin(), neg.end());

@@ -133,7 +133,9 @@ void EigBatcher::run_batch(const std::vector<Req*>& batch) {
 // and the density matrices need them), one density matrix per step (two
 // with FDM) of at most K'^2, and transients of a few D^2: the Hamiltonian,
 // the recalculated operators and their intermediates.
-double project_run_bytes(const std::string& wd) {
+double project_run_bytes(const std::string& wd) { return run_shape(wd).bound; }
+
+RunShape run_shape(const std::string& wd) {
   Params P;
   P.read(wd + "/param");
   DataFile D;
@@ -147,7 +149,11 @@ double project_run_bytes(const std::string& wd) {
   for (const auto& k : D.ops) nops += (double)k.second.size();
   const double per_step = dim * dim + dim + (P.fdm ? 2.0 : 1.0) * kp * kp;
   const double transient = (3.0 + 2.0 * (nops + (double)D.channels)) * dim * dim;
-  return 8.0 * (steps * per_step + transient) + 64.0 * (1 << 20);
+  RunShape r;
+  r.bound = 8.0 * (steps * per_step + transient) + 64.0 * (1 << 20);
+  r.key = std::to_string(P.keep) + "/" + std::to_string(Nmax - P.Ninit) + "/" + std::to_string(D.channels) + "/" +
+          std::to_string((int)nops) + (P.fdm ? "/fdm" : "") + (P.dmnrg ? "/dmnrg" : "");
+  return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -180,7 +186,9 @@ long long Server::submit(const std::string& wd, const std::string& od) {
   std::unique_ptr<Job> j(new Job);
   j->wd = wd;
   j->od = od;
-  j->proj = project_run_bytes(wd);  // throws when the input cannot be read
+  const RunShape shape = run_shape(wd);  // throws when the input cannot be read
+  j->bound = shape.bound;
+  j->key = shape.key;
   j->t_submit = Clock::now();
   std::lock_guard<std::mutex> g(m_);
   if (stop_) throw std::runtime_error("server is shutting down");
@@ -207,6 +215,7 @@ void Server::worker() {
         if (queue_.empty()) break;
         j = queue_.front();
         queue_.pop_front();
+        j->proj = projection(*j);
         in_use_ += j->proj;
         ++running_;
         peak_in_use_ = std::max(peak_in_use_, in_use_);
@@ -223,21 +232,46 @@ void Server::worker() {
         status = 2;
         err = e.what();
       }
+      bool requeued = false;
       {
         std::lock_guard<std::mutex> g(m_);
         in_use_ -= j->proj;
         --running_;
-        j->status = status;
-        j->err = err;
-        j->t_done = Clock::now();
-        j->finished = true;
-        if (status) ++failed_; else ++done_;
+        if (status == 0 && j->bound > 0) {
+          double& r = ratio_[j->key];
+          r = std::max(r, j->ex.peak_bytes / j->bound);
+        }
+        if (status != 0 && !j->full_bound && j->proj < j->bound &&
+            err.find("out of memory") != std::string::npos) {
+          // admitted on a learned projection and out of memory: once more,
+          // at the head of the queue, on the full bound
+          j->full_bound = true;
+          queue_.push_front(j);
+          requeued = true;
+        } else {
+          j->status = status;
+          j->err = err;
+          j->t_done = Clock::now();
+          j->finished = true;
+          if (status) ++failed_; else ++done_;
+        }
+      }
+      if (requeued) {
+        work_cv_.notify_all();
+        continue;
       }
       done_cv_.notify_all();
       work_cv_.notify_all();
     }
   }
   cudaStreamDestroy(st);
+}
+
+double Server::projection(const Job& j) const {
+  if (j.full_bound) return j.bound;
+  auto it = ratio_.find(j.key);
+  if (it == ratio_.end()) return j.bound;
+  return std::min(j.bound, LEARN_MARGIN * it->second * j.bound);
 }
 
 int Server::wait(long long ticket, double timeout_s, double* stats, std::string* err) {

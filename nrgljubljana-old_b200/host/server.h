@@ -4,12 +4,15 @@
 // an output directory).  Requests queue in arrival order; a free worker slot
 // admits the head of the queue when its projected device memory fits in the
 // budget next to the runs already admitted (a run always starts when nothing
-// else runs).  Each worker drives its run with its own stream and host
+// else runs).  The projection starts as an upper bound computed from the
+// run's input and is then learned from the measured peaks of finished runs
+// of the same shape; a run that runs out of memory on a learned projection
+// is admitted once more on the bound.  Each worker drives its run with its own stream and host
 // thread, so the GEMM, spectrum and binning work of different runs overlaps
 // on the device.  The block eigensolves of all runs that are in their first
 // sweep go through one batcher, which merges the blocks of the runs that
 // are waiting into a single call of the batched solver: one set of
-// cooperative panel launches then advances every run's blocks together.
+// cluster and panel launches then advance every run's blocks together.
 // Runs that arrive while others are on the GPU join the next merged call.
 //
 // The reference has no counterpart: it runs one calculation per process
@@ -73,6 +76,14 @@ class EigBatcher : public EigSolver {
 // and `data` (keep, Nmax, channels, tracked operators and spectra).
 double project_run_bytes(const std::string& workdir);
 
+// The bound and the shape of a run (keep, chain length, channels, tracked
+// operators, density-matrix kind): runs of one shape hold similar memory.
+struct RunShape {
+  double bound = 0;
+  std::string key;
+};
+RunShape run_shape(const std::string& workdir);
+
 class Server {
  public:
   // mem_budget <= 0: 85% of the device memory free at creation.
@@ -94,7 +105,10 @@ class Server {
   struct Job {
     long long id = 0;
     std::string wd, od;
-    double proj = 0;
+    double bound = 0;       // upper bound of the run's device bytes
+    std::string key;        // its shape (RunShape::key)
+    double proj = 0;        // projection it was admitted with
+    bool full_bound = false;  // admit on the bound (after running out of memory)
     Clock::time_point t_submit, t_admit, t_done;
     bool finished = false;
     int status = 0;
@@ -104,7 +118,12 @@ class Server {
     long long order = 0;
   };
   void worker();
-  bool fits(const Job& j) const { return running_ == 0 || in_use_ + j.proj <= budget_; }
+  // Admission projection: the bound until a run of the same shape has
+  // finished, then LEARN_MARGIN times the largest peak / bound ratio seen
+  // for that shape (never above the bound).
+  static constexpr double LEARN_MARGIN = 2.0;
+  double projection(const Job& j) const;
+  bool fits(const Job& j) const { return running_ == 0 || in_use_ + projection(j) <= budget_; }
 
   int device_;
   double budget_ = 0;
@@ -116,6 +135,7 @@ class Server {
   long long next_id_ = 1, admitted_ = 0;
   double in_use_ = 0, peak_in_use_ = 0;
   int running_ = 0, peak_running_ = 0;
+  std::map<std::string, double> ratio_;  // shape -> largest peak / bound seen
   long done_ = 0, failed_ = 0;
   bool stop_ = false;
   std::vector<std::thread> workers_;

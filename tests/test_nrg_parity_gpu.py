@@ -65,3 +65,12 @@ def test_nrg_run_matches_oracle(ctx, tmp_path, name):
         wmax = max(abs(v) for v in da.values())
         err = max(abs(da.get(k, 0.0) - db.get(k, 0.0)) for k in keys)
         assert err <= RTOL * wmax, (os.path.basename(bo), err, wmax)
+    # broadened spectra (.dat, 10 significant digits), broadened on the device
+    dat_o = sorted(glob.glob(os.path.join(out_o, "*_dens_*.dat")))
+    dat_g = sorted(glob.glob(os.path.join(out_g, "*_dens_*.dat")))
+    assert [os.path.basename(b) for b in dat_o] == [os.path.basename(b) for b in dat_g]
+    for do, dg in zip(dat_o, dat_g):
+        a, b = cases.read_table(do), cases.read_table(dg)
+        assert a.shape == b.shape and np.allclose(a[:, 0], b[:, 0], rtol=1e-9, atol=0)
+        amax = np.max(np.abs(a[:, 1]))
+        assert np.all(np.abs(a[:, 1] - b[:, 1]) <= RTOL * amax + 1e-9 * np.abs(a[:, 1])), os.path.basename(do)

@@ -112,6 +112,33 @@ def test_admission_respects_memory_budget(tmp_path):
     assert [s["order"] for s in stats] == [1, 2, 3, 4]
 
 
+def test_projection_is_learned_from_finished_runs(tmp_path):
+    """A budget that holds one run by its bound holds several once a run of
+    the same shape has finished and its measured peak is known."""
+    import nrgb
+    r = dict(RUNS[0])
+    wds = [make_run(str(tmp_path), i, dict(r, eps_d=r["eps_d"] - 0.01 * i)) for i in range(4)]
+    bound = nrgb.project_bytes(wds[0])
+    srv = nrgb.Server(0, max_runs=4, mem_budget_bytes=1.5 * bound)
+    outs = []
+    for i in range(4):
+        od = str(tmp_path / ("o%d" % i))
+        os.makedirs(od)
+        outs.append(od)
+    first = srv.wait(srv.submit(wds[0], outs[0]), 600)
+    assert first["projected_bytes"] == bound and 0 < first["peak_bytes"] <= bound
+    rest = [srv.submit(wd, od) for wd, od in zip(wds[1:], outs[1:])]
+    stats = [srv.wait(t, 600) for t in rest]
+    cnt = srv.counters()
+    srv.close()
+    assert cnt["done"] == 4 and cnt["failed"] == 0
+    for s_ in stats:
+        # learned: twice the measured peak ratio, below the bound
+        assert s_["projected_bytes"] == pytest.approx(2.0 * first["peak_bytes"], rel=1e-9)
+        assert s_["peak_bytes"] <= s_["projected_bytes"]
+    assert cnt["peak_running"] >= 2
+
+
 def test_failing_run_is_isolated(tmp_path):
     import nrgb
     good = [make_run(str(tmp_path), i, r) for i, r in enumerate(RUNS[:2])]
