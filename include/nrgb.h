@@ -159,12 +159,13 @@ int nrgb_set_eig_mode(nrgb_ctx* ctx, int mode);
  * ------------------------------------------------------------------------- */
 typedef struct nrgb_server nrgb_server;
 
-/* Admission projection: nrgb_project_bytes (an upper bound) until a run of
- * the same shape (keep, chain length, channels, operators, density-matrix
- * kind) has finished, then twice the largest measured peak / bound ratio of
- * that shape times the bound (never above the bound); a run that runs out of
- * device memory on a learned projection is queued once more, first, on the
- * bound.
+/* Admission projection, never above the upper bound nrgb_project_bytes:
+ * twice the largest measured peak / bound ratio of finished runs of the same
+ * shape (keep, chain length, channels, operators, density-matrix kind)
+ * times the bound; four times the largest ratio of any shape while none of
+ * this shape has finished; the bound while no run has finished.  A run that
+ * runs out of device memory on a learned projection is queued once more,
+ * first, on the bound.
  * mem_budget_bytes <= 0: 85% of the device memory free at creation.
  * Returns 0, 1 (bad arguments), 2 (CUDA error), 3 (no device), 4 (bad device). */
 int nrgb_server_create(int device, int max_runs, double mem_budget_bytes, double batch_window_us,

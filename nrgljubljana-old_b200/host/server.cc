@@ -268,10 +268,14 @@ void Server::worker() {
 }
 
 double Server::projection(const Job& j) const {
-  if (j.full_bound) return j.bound;
+  if (j.full_bound || ratio_.empty()) return j.bound;
   auto it = ratio_.find(j.key);
-  if (it == ratio_.end()) return j.bound;
-  return std::min(j.bound, LEARN_MARGIN * it->second * j.bound);
+  if (it != ratio_.end()) return std::min(j.bound, LEARN_MARGIN * it->second * j.bound);
+  // no run of this shape has finished yet: the largest ratio of any shape,
+  // with a wider margin
+  double r = 0;
+  for (const auto& kv : ratio_) r = std::max(r, kv.second);
+  return std::min(j.bound, 2.0 * LEARN_MARGIN * r * j.bound);
 }
 
 int Server::wait(long long ticket, double timeout_s, double* stats, std::string* err) {

@@ -118,9 +118,10 @@ class Server {
     long long order = 0;
   };
   void worker();
-  // Admission projection: the bound until a run of the same shape has
-  // finished, then LEARN_MARGIN times the largest peak / bound ratio seen
-  // for that shape (never above the bound).
+  // Admission projection: LEARN_MARGIN times the largest peak / bound ratio
+  // measured for runs of the same shape, or twice that margin times the
+  // largest ratio of any shape while none of this shape has finished, or
+  // the bound while no run has finished (never above the bound).
   static constexpr double LEARN_MARGIN = 2.0;
   double projection(const Job& j) const;
   bool fits(const Job& j) const { return running_ == 0 || in_use_ + projection(j) <= budget_; }

@@ -106,9 +106,10 @@ def test_admission_respects_memory_budget(tmp_path):
     cnt = srv.counters()
     srv.close()
     assert cnt["done"] == 4
-    assert cnt["peak_running"] == 1
     assert cnt["peak_admitted_bytes"] <= budget
-    # first come, first served
+    # while no run had finished, projections were the bounds and the second
+    # run waited for the first; first come, first served throughout
+    assert stats[1]["queue_s"] >= stats[0]["latency_s"] - 0.05
     assert [s["order"] for s in stats] == [1, 2, 3, 4]
 
 
