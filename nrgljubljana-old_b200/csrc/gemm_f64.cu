@@ -5,6 +5,7 @@
 // double-buffered shared memory (k-major, padded so the DMMA fragment loads
 // are bank-conflict free).  mma.sync.m8n8k4.f64: A fragment A[g][t],
 // B fragment B[t][g], accumulator C[g][2t..2t+1] with g = lane/4, t = lane%4.
+#include <atomic>
 #include "common.cuh"
 #include "gemm_f64.cuh"
 
@@ -408,10 +409,16 @@ cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSe
   // 128x128 tiles when they cover at most 30% more area than the 64x64 ones
   // and still give enough CTAs to fill the GPU
   if (kUseLargeTiles && total_stiles > 0 && 4.0 * total_stiles <= 1.3 * total_tiles && total_stiles >= 120) {
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(gemm_grouped_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LSMEM);
-      attr = true;
+    // once per device (function attributes belong to the device's context);
+    // every caller sets the same value, so threads that race here agree
+    static std::atomic<bool> attr[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 64 || !attr[dev].load(std::memory_order_acquire)) {
+      const cudaError_t e =
+          cudaFuncSetAttribute(gemm_grouped_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LSMEM);
+      if (e != cudaSuccess) return e;
+      if (dev < 64) attr[dev].store(true, std::memory_order_release);
     }
     NRGB_LAUNCH(tag, stream,
                 gemm_grouped_large_kernel<<<total_stiles, LNT, LSMEM, stream>>>(d_probs, nprob, d_segs));

@@ -13,6 +13,8 @@
 //    "middle way" model) in coordinates relative to the nearer pole, and
 //    eigenvectors from the Loewner-formula z-hat (Gu & Eisenstat 1995), which
 //    keeps them orthogonal without extra precision.
+#include <map>
+#include <mutex>
 #include <cooperative_groups.h>
 #include <math.h>
 #include <stdlib.h>
@@ -697,8 +699,12 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
 }
 
 template <int CL>
+// The kernel's attributes (largest dynamic shared memory, non-portable
+// cluster size) are set once per device, at the largest size any launch uses,
+// by the solver's constructor (set_attr): setting them per launch to the
+// launch's own size would race between solver instances on other threads.
 cudaError_t trdc_config(size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int nprob,
-                        cudaStream_t st) {
+                        cudaStream_t st, bool set_attr) {
   cfg = cudaLaunchConfig_t{};
   cfg.gridDim = dim3((unsigned)(nprob * CL));
   cfg.blockDim = dim3(TRDC_NT);
@@ -710,6 +716,7 @@ cudaError_t trdc_config(size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribut
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
+  if (!set_attr) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(trd_cluster_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess && CL > 8)
     e = cudaFuncSetAttribute(trd_cluster_kernel<CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -717,12 +724,13 @@ cudaError_t trdc_config(size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribut
 }
 
 // Clusters of CL CTAs with `smem` bytes each that can be resident at once
-// (0: this cluster size is not usable here).
+// (0: this cluster size is not usable here); sets the kernel's attributes
+// for launches of up to `smem` bytes.
 template <int CL>
 int trdc_max_clusters(size_t smem) {
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute at[1];
-  if (trdc_config<CL>(smem, cfg, at, 1, nullptr) != cudaSuccess) {
+  if (trdc_config<CL>(smem, cfg, at, 1, nullptr, true) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -738,9 +746,26 @@ template <int CL>
 cudaError_t trdc_launch(const TrdClProb* d, int nprob, size_t smem, cudaStream_t st) {
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute at[1];
-  cudaError_t e = trdc_config<CL>(smem, cfg, at, nprob, st);
+  cudaError_t e = trdc_config<CL>(smem, cfg, at, nprob, st, false);
   if (e != cudaSuccess) return e;
   return cudaLaunchKernelEx(&cfg, trd_cluster_kernel<CL>, d);
+}
+
+// The panel kernel's largest dynamic shared memory on the current device only
+// grows: solvers on other threads may launch it with more than this call
+// needs, and lowering the attribute under them would fail their launches.
+cudaError_t raise_panel_smem(int bytes) {
+  static std::mutex mu;
+  static std::map<int, int> set;  // device -> bytes set
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(mu);
+  int& cur = set[dev];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
 }
 
 // --------------------------------------------------------------------------
@@ -1624,8 +1649,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     }
     {
       const size_t smem = (size_t)(32 + 4 * NB + 8 + (TRD_NT / 32) * 2 * NB + nmax) * sizeof(double);
-      NRGB_CUDA(cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+      NRGB_CUDA(raise_panel_smem((int)smem));
       int per_sm = 0;
       NRGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_NT, smem));
       per_sm = std::max(1, std::min(per_sm, 4));

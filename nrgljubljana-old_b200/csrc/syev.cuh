@@ -60,6 +60,9 @@ class SyevBatched : public EigSolver {
   static size_t workspace_bytes(const std::vector<int>& n);
   // Launch statistics of the last run().
   int last_launches() const { return launches_; }
+  // Largest block the cluster tridiagonalisation holds (0: cluster path off);
+  // larger blocks also take the cooperative panel launches.
+  int cluster_nmax() const { return cl_nmax_; }
 
  private:
   DeviceArena arena_;

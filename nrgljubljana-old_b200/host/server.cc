@@ -18,8 +18,12 @@ namespace nrgb {
 // ---------------------------------------------------------------------------
 EigBatcher::EigBatcher(int device, double window_us) : device_(device), window_us_(window_us) {
   NRGB_CUDA(cudaSetDevice(device_));
-  NRGB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-  th_ = std::thread([this] { loop(); });
+  for (int l = 0; l < NLANE; ++l) {
+    lanes_[l].syev.reset(new SyevBatched());
+    NRGB_CUDA(cudaStreamCreateWithFlags(&lanes_[l].stream, cudaStreamNonBlocking));
+  }
+  cluster_nmax_ = lanes_[0].syev->cluster_nmax();
+  for (int l = 0; l < NLANE; ++l) lanes_[l].th = std::thread([this, l] { loop(l); });
 }
 
 EigBatcher::~EigBatcher() {
@@ -28,8 +32,11 @@ EigBatcher::~EigBatcher() {
     stop_ = true;
   }
   cv_.notify_all();
-  if (th_.joinable()) th_.join();
-  if (stream_) cudaStreamDestroy(stream_);
+  for (Lane& L : lanes_) {
+    if (L.th.joinable()) L.th.join();
+    L.syev.reset();
+    if (L.stream) cudaStreamDestroy(L.stream);
+  }
 }
 
 void EigBatcher::client_enter() {
@@ -52,14 +59,23 @@ void EigBatcher::counters(double* calls, double* requests, double* problems) {
   *problems = (double)problems_;
 }
 
+int EigBatcher::pending_locked() const {
+  int n = 0;
+  for (const Lane& L : lanes_) n += (int)L.q.size() + L.inflight;
+  return n;
+}
+
 int EigBatcher::solve(const std::vector<SyevDesc>& probs, cudaStream_t stream) {
   Req r;
   r.probs = &probs;
+  int nmax = 0;
+  for (const SyevDesc& d : probs) nmax = std::max(nmax, d.n);
+  const int lane = (cluster_nmax_ > 0 && nmax <= cluster_nmax_) ? 0 : 1;
   NRGB_CUDA(cudaEventCreateWithFlags(&r.ready, cudaEventDisableTiming));
   NRGB_CUDA(cudaEventRecord(r.ready, stream));  // the blocks are assembled on the caller's stream
   {
     std::unique_lock<std::mutex> lk(m_);
-    q_.push_back(&r);
+    lanes_[lane].q.push_back(&r);
     cv_.notify_all();
     done_cv_.wait(lk, [&] { return r.done; });
   }
@@ -68,23 +84,26 @@ int EigBatcher::solve(const std::vector<SyevDesc>& probs, cudaStream_t stream) {
   return r.launches;
 }
 
-void EigBatcher::loop() {
+void EigBatcher::loop(int lane) {
   cudaSetDevice(device_);
+  Lane& L = lanes_[lane];
   std::unique_lock<std::mutex> lk(m_);
   for (;;) {
-    cv_.wait(lk, [&] { return stop_ || !q_.empty(); });
-    if (q_.empty()) return;  // stop requested and nothing pending
+    cv_.wait(lk, [&] { return stop_ || !L.q.empty(); });
+    if (L.q.empty()) return;  // stop requested and nothing pending
     // gather: wait (at most the window) until every run inside its first
-    // sweep has its blocks queued
+    // sweep has its blocks queued or being solved, in either lane
     const auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds((long)window_us_);
-    while (!stop_ && (int)q_.size() < clients_) {
+    while (!stop_ && pending_locked() < clients_) {
       if (cv_.wait_until(lk, deadline) == std::cv_status::timeout) break;
     }
-    std::vector<Req*> batch(q_.begin(), q_.end());
-    q_.clear();
+    std::vector<Req*> batch(L.q.begin(), L.q.end());
+    L.q.clear();
+    L.inflight = (int)batch.size();
     lk.unlock();
-    run_batch(batch);
+    run_batch(L, batch);
     lk.lock();
+    L.inflight = 0;
     ++calls_;
     requests_ += (long)batch.size();
     for (Req* r : batch) {
@@ -92,20 +111,22 @@ void EigBatcher::loop() {
       r->done = true;
     }
     done_cv_.notify_all();
+    cv_.notify_all();
   }
 }
 
-void EigBatcher::run_batch(const std::vector<Req*>& batch) {
+void EigBatcher::run_batch(Lane& L, const std::vector<Req*>& batch) {
   std::vector<SyevDesc> all;
   try {
     for (Req* r : batch) {
-      NRGB_CUDA(cudaStreamWaitEvent(stream_, r->ready, 0));
+      NRGB_CUDA(cudaStreamWaitEvent(L.stream, r->ready, 0));
       all.insert(all.end(), r->probs->begin(), r->probs->end());
     }
-    const int l = syev_.solve(all, stream_);
+    const int l = L.syev->solve(all, L.stream);
     for (Req* r : batch) r->launches = l;
     return;
   } catch (const std::exception& e) {
+    cudaGetLastError();  // a launch error stays in this thread's last error until read
     if (batch.size() == 1) {
       batch[0]->err = e.what();
       return;
@@ -115,8 +136,9 @@ void EigBatcher::run_batch(const std::vector<Req*>& batch) {
   // run whose blocks fail gets the error
   for (Req* r : batch) {
     try {
-      r->launches = syev_.solve(*r->probs, stream_);
+      r->launches = L.syev->solve(*r->probs, L.stream);
     } catch (const std::exception& e) {
+      cudaGetLastError();
       r->err = e.what();
     }
   }

@@ -36,7 +36,13 @@
 
 namespace nrgb {
 
-// Merges the eigensolver batches of concurrent runs (see above).
+// Merges the eigensolver batches of concurrent runs (see above).  Two lanes,
+// each with its own thread, stream and solver: requests whose blocks all fit
+// the cluster tridiagonalisation, and requests with larger blocks (which
+// also need the cooperative panel launches).  Merged calls of the two lanes
+// overlap on the device, so runs with small blocks do not wait for the
+// panel phase of large ones, and cooperative launches come from one lane
+// only.
 class EigBatcher : public EigSolver {
  public:
   EigBatcher(int device, double window_us);
@@ -55,21 +61,28 @@ class EigBatcher : public EigSolver {
     int launches = 0;
     std::string err;
   };
-  void loop();
-  void run_batch(const std::vector<Req*>& batch);
+  struct Lane {
+    std::unique_ptr<SyevBatched> syev;
+    cudaStream_t stream = nullptr;
+    std::deque<Req*> q;
+    int inflight = 0;  // requests in the lane's running merged call
+    std::thread th;
+  };
+  static constexpr int NLANE = 2;
+  void loop(int lane);
+  void run_batch(Lane& L, const std::vector<Req*>& batch);
+  int pending_locked() const;
 
   int device_;
   double window_us_;
-  SyevBatched syev_;
-  cudaStream_t stream_ = nullptr;
+  int cluster_nmax_ = 0;  // blocks up to this size take the small lane
+  Lane lanes_[NLANE];
   std::mutex m_;
   std::condition_variable cv_;       // a request arrived, or stop
   std::condition_variable done_cv_;  // a merged call finished
-  std::deque<Req*> q_;
   int clients_ = 0;  // runs inside their first sweep
   bool stop_ = false;
   long calls_ = 0, requests_ = 0, problems_ = 0;
-  std::thread th_;
 };
 
 // Upper bound of the device bytes one run holds at once, from its `param`
