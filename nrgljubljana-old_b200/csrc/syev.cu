@@ -751,19 +751,19 @@ cudaError_t trdc_launch(const TrdClProb* d, int nprob, size_t smem, cudaStream_t
   return cudaLaunchKernelEx(&cfg, trd_cluster_kernel<CL>, d);
 }
 
-// The panel kernel's largest dynamic shared memory on the current device only
-// grows: solvers on other threads may launch it with more than this call
-// needs, and lowering the attribute under them would fail their launches.
-cudaError_t raise_panel_smem(int bytes) {
+// A kernel's largest dynamic shared memory on the current device only grows:
+// solvers on other threads may launch it with more than this call needs, and
+// lowering the attribute under them would fail their launches.
+cudaError_t raise_smem_attr(const void* func, int bytes) {
   static std::mutex mu;
-  static std::map<int, int> set;  // device -> bytes set
+  static std::map<std::pair<int, const void*>, int> set;  // (device, kernel) -> bytes set
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> g(mu);
-  int& cur = set[dev];
+  int& cur = set[{dev, func}];
   if (bytes <= cur) return cudaSuccess;
-  e = cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess) cur = bytes;
   return e;
 }
@@ -872,20 +872,32 @@ __global__ void __launch_bounds__(64) dc_leaf_kernel(const DcProb* __restrict__ 
 }
 
 // Merge, step 1: z, sort, deflation, rotations, compaction.  One CTA per node.
+// The sorted d and z and the deflation flags live in a work area: dynamic
+// shared memory when the node has at most `cap` entries (the launch's
+// shared memory holds 2 cap doubles and cap ints), else the node's slices
+// of zhat, tau and flag in global memory, which are free at this point.  The
+// two sequential scans (deflation, compaction order) run on the work area.
 constexpr int DC_NT = 256;
+constexpr int DC_PREP_CAP = 8192;  // largest node staged in shared memory (160 KB)
+
+__host__ __device__ inline size_t dc_prep_smem(int cap) { return (size_t)cap * (2 * sizeof(double) + sizeof(int)); }
 
 __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict__ probs,
                                                         const DcNode* __restrict__ nodes,
-                                                        GemmProb* gprob, GemmSeg* gseg) {
-  __shared__ double scratch[32];
+                                                        GemmProb* gprob, GemmSeg* gseg, int cap) {
+  extern __shared__ double dcsm[];
+  __shared__ double mx[2][DC_NT / 32];
   __shared__ int sk[2];
   const DcNode N = nodes[blockIdx.x];
   const DcProb P = probs[N.prob];
   const int n = P.n, lo = N.lo, mid = N.mid, hi = N.hi;
   const int n1 = mid - lo, np = hi - lo;
   const size_t ld = (size_t)n;
-  (void)ld;
   const int tid = threadIdx.x;
+  const bool staged = np <= cap;
+  double* wd = staged ? dcsm : P.zhat + lo;
+  double* wz = staged ? dcsm + cap : P.tau + lo;
+  int* wf = staged ? reinterpret_cast<int*>(dcsm + 2 * (size_t)cap) : P.flag + lo;
   const double beta = P.e[mid - 1];
   const double rho = 2.0 * fabs(beta);
   const double sgn = beta >= 0.0 ? 1.0 : -1.0;
@@ -914,63 +926,49 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
       }
       pos = (i - n1) + a;
     }
-    P.ds[lo + pos] = di;
-    P.zs[lo + pos] = zi;
+    wd[pos] = di;
+    wz[pos] = zi;
     P.src[lo + pos] = i;
     dmax = fmax(dmax, fabs(di));
     zmax = fmax(zmax, fabs(zi));
   }
-  __syncthreads();
   // block max of |d| and |z|
-  {
-    // reuse block_sum machinery for max via two passes
-    __shared__ double mx[2][32];
-    double a = dmax, b = zmax;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
-      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
-    }
-    if ((tid & 31) == 0) {
-      mx[0][tid >> 5] = a;
-      mx[1][tid >> 5] = b;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      for (int w = 1; w < DC_NT / 32; ++w) {
-        a = fmax(a, mx[0][w]);
-        b = fmax(b, mx[1][w]);
-      }
-      scratch[0] = a;
-      scratch[1] = b;
-    }
-    __syncthreads();
-    dmax = scratch[0];
-    zmax = scratch[1];
+  for (int o = 16; o > 0; o >>= 1) {
+    dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    zmax = fmax(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
+  }
+  if ((tid & 31) == 0) {
+    mx[0][tid >> 5] = dmax;
+    mx[1][tid >> 5] = zmax;
   }
   __syncthreads();
-  // deflation scan (sequential)
   if (tid == 0) {
+    for (int w = 1; w < DC_NT / 32; ++w) {
+      dmax = fmax(dmax, mx[0][w]);
+      zmax = fmax(zmax, mx[1][w]);
+    }
+    // deflation scan (sequential)
     const double tol = 8.0 * EPS * fmax(dmax, rho * zmax);
     int nr = 0, k = 0, prev = -1;
     for (int j = 0; j < np; ++j) {
-      P.flag[lo + j] = 0;
-      if (rho * fabs(P.zs[lo + j]) <= tol) continue;  // deflated by small z
+      wf[j] = 0;
+      if (rho * fabs(wz[j]) <= tol) continue;  // deflated by small z
       if (prev < 0) {
         prev = j;
         continue;
       }
-      double s = P.zs[lo + prev], c = P.zs[lo + j];
+      double s = wz[prev], c = wz[j];
       const double t = hypot(c, s);
-      const double dt = P.ds[lo + j] - P.ds[lo + prev];
+      const double dt = wd[j] - wd[prev];
       c /= t;
       s = -s / t;
       if (fabs(dt * c * s) <= tol) {
-        P.zs[lo + j] = t;
-        P.zs[lo + prev] = 0.0;
-        const double dp = P.ds[lo + prev], dj = P.ds[lo + j];
-        P.ds[lo + prev] = dp * c * c + dj * s * s;
-        P.ds[lo + j] = dp * s * s + dj * c * c;
+        wz[j] = t;
+        wz[prev] = 0.0;
+        const double dp = wd[prev], dj = wd[j];
+        wd[prev] = dp * c * c + dj * s * s;
+        wd[j] = dp * s * s + dj * c * c;
         P.rotp[lo + nr] = prev;
         P.rotj[lo + nr] = j;
         P.rotc[lo + nr] = c;
@@ -978,13 +976,13 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
         ++nr;
         prev = j;  // prev deflated (flag stays 0)
       } else {
-        P.flag[lo + prev] = 1;
+        wf[prev] = 1;
         ++k;
         prev = j;
       }
     }
     if (prev >= 0) {
-      P.flag[lo + prev] = 1;
+      wf[prev] = 1;
       ++k;
     }
     sk[0] = k;
@@ -992,15 +990,12 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
     P.kcnt[lo] = k;
     P.rho[lo] = rho;
     P.nrot[lo] = nr;
-  }
-  __syncthreads();
-  const int k = sk[0];
-  // compaction targets: nondeflated first (in order), then deflated (in order)
-  if (tid == 0) {
+    // compaction order: nondeflated first (in order), then deflated (in
+    // order); rank holds, for now, the sorted position of each target
     int kk = 0, dd = 0;
     for (int j = 0; j < np; ++j) {
-      if (P.flag[lo + j]) {
-        P.rank[lo + kk] = j;  // temporarily: source sorted position of K-th
+      if (wf[j]) {
+        P.rank[lo + kk] = j;
         ++kk;
       } else {
         P.rank[lo + k + dd] = j;
@@ -1009,19 +1004,15 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
     }
   }
   __syncthreads();
-  // compact values (dK into tau scratch first to avoid overlap, then copy back)
+  const int k = sk[0];
+  // compact the values out of the work area
   for (int a = tid; a < np; a += DC_NT) {
     const int j = P.rank[lo + a];
-    P.zhat[lo + a] = P.ds[lo + j];
-    P.tau[lo + a] = P.zs[lo + j];
-  }
-  __syncthreads();
-  for (int a = tid; a < np; a += DC_NT) {
     if (a < k) {
-      P.ds[lo + a] = P.zhat[lo + a];
-      P.zs[lo + a] = P.tau[lo + a];
+      P.ds[lo + a] = wd[j];
+      P.zs[lo + a] = wz[j];
     } else {
-      P.dD[lo + a] = P.zhat[lo + a];
+      P.dD[lo + a] = wd[j];
     }
   }
   // GEMM descriptor: W1[lo:hi, lo:lo+k] = Q[lo:hi, lo:lo+k] * U[lo:lo+k, lo:lo+k]
@@ -1046,22 +1037,39 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
   }
 }
 
-// Merge, step 2 (one thread per row of the node's block): gather the child
-// eigenvector columns in sorted order, apply the deflation rotations in
-// order, and compact (nondeflated first) into Q[lo:hi, lo:hi].  Rows are
-// independent, so the sequential rotation list costs O(nrot) per row.
-__global__ void dc_permute_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes) {
-  const int node = blockIdx.y;
-  const DcNode N = nodes[node];
+// Merge, step 2, in three launches over the node's block Q[lo:hi, lo:hi]
+// (rows independent throughout):
+//   gather:  W1[:, pos] = Q[:, src[pos]], the child eigenvector columns in
+//            sorted order (a CTA per 128 rows x DC_PCOLS columns);
+//   rotate:  the deflation rotations in order, one thread per row (nothing
+//            to do when the node has none);
+//   compact: Q[:, a] = W1[:, rank[a]], nondeflated columns first.
+constexpr int DC_PCOLS = 8;
+
+__global__ void dc_gather_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes, int compact) {
+  const DcNode N = nodes[blockIdx.z];
   const DcProb P = probs[N.prob];
   const int lo = N.lo, np = N.hi - N.lo;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= np) return;
+  const int c0 = blockIdx.y * DC_PCOLS;
+  if (r >= np || c0 >= np) return;
   const size_t ld = (size_t)P.n;
-  double* w1 = P.W1 + (size_t)(lo + r) + (size_t)lo * ld;   // row r, columns lo..hi
-  const double* q = P.Q + (size_t)(lo + r) + (size_t)lo * ld;
-  for (int pos = 0; pos < np; ++pos) w1[(size_t)pos * ld] = q[(size_t)P.src[lo + pos] * ld];
+  const int* map = compact ? P.rank + lo : P.src + lo;
+  const double* from = (compact ? P.W1 : P.Q) + (size_t)(lo + r) + (size_t)lo * ld;
+  double* to = (compact ? P.Q : P.W1) + (size_t)(lo + r) + (size_t)lo * ld;
+  const int c1 = min(np, c0 + DC_PCOLS);
+  for (int c = c0; c < c1; ++c) to[(size_t)c * ld] = from[(size_t)map[c] * ld];
+}
+
+__global__ void dc_rotate_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes) {
+  const DcNode N = nodes[blockIdx.y];
+  const DcProb P = probs[N.prob];
+  const int lo = N.lo, np = N.hi - N.lo;
   const int nr = P.nrot[lo];
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nr == 0 || r >= np) return;
+  const size_t ld = (size_t)P.n;
+  double* w1 = P.W1 + (size_t)(lo + r) + (size_t)lo * ld;  // row r, columns lo..hi
   for (int t = 0; t < nr; ++t) {
     const size_t pc = (size_t)P.rotp[lo + t] * ld, jc = (size_t)P.rotj[lo + t] * ld;
     const double c = P.rotc[lo + t], s = P.rots[lo + t];
@@ -1069,8 +1077,6 @@ __global__ void dc_permute_kernel(const DcProb* __restrict__ probs, const DcNode
     w1[pc] = c * x + s * y;
     w1[jc] = c * y - s * x;
   }
-  double* qo = P.Q + (size_t)(lo + r) + (size_t)lo * ld;
-  for (int a = 0; a < np; ++a) qo[(size_t)a * ld] = w1[(size_t)P.rank[lo + a] * ld];
 }
 
 // Secular equation roots, one warp per root: lanes share the pole sums.
@@ -1280,58 +1286,99 @@ struct BtProb {
   int n;
   const double* A;    // reflectors below the subdiagonal
   const double* tau;  // n-1
-  double* Vb;         // n x NBB
-  double* G;          // NBB x NBB
-  double* T;          // NBB x NBB
-  double* X;          // NBB x n
-  double* Y;          // NBB x n
+  double* V;          // n x n (ld n): reflector c in column c, c <= n-2
+  double* G;          // nblk blocks of NBB x NBB: V_k^T V_k
+  double* T;          // nblk blocks of NBB x NBB: the WY factors
 };
 
-__global__ void bt_buildV_kernel(const BtProb* __restrict__ probs, int j0) {
+// Reflectors of block k (columns j0 = k NBB .. j0 + nb - 1, nb <= NBB).
+__host__ __device__ inline int bt_nblk(int n) { return n > 1 ? (n - 2) / NBB + 1 : 0; }
+
+// V[:, c] = (0, .., 0, 1, A[c+2:, c]) for every reflector c of every problem
+// (a CTA per column).
+__global__ void bt_buildV_kernel(const BtProb* __restrict__ probs) {
   const BtProb P = probs[blockIdx.y];
-  const int kcol = blockIdx.x;  // reflector index within block
-  const int c = j0 + kcol;
+  const int c = blockIdx.x;
   const int n = P.n;
-  double* col = P.Vb + (size_t)kcol * n;
-  const bool valid = c <= n - 2;
+  if (c > n - 2) return;
+  double* col = P.V + (size_t)c * n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double v = 0.0;
-    if (valid) {
-      if (i == c + 1) v = 1.0;
-      else if (i > c + 1) v = P.A[i + (size_t)c * n];
-    }
+    if (i == c + 1) v = 1.0;
+    else if (i > c + 1) v = P.A[i + (size_t)c * n];
     col[i] = v;
   }
 }
 
-__global__ void bt_T_kernel(const BtProb* __restrict__ probs, int j0) {
-  const BtProb P = probs[blockIdx.x];
+// T of the compact WY form of the reflectors j0 .. j0+nb-1 (the dlarft
+// recurrence T[0:j, j] = -tau_j T[0:j, 0:j] G[0:j, j], G = V^T V), with G and
+// T in shared memory; four threads per row of T share its dot products.
+constexpr int BT_T_NT = 4 * NBB;
+constexpr size_t BT_T_SMEM = 2 * (size_t)NBB * (NBB + 1) * sizeof(double);
+
+// One CTA per block k (x) of every problem (y).
+__global__ void __launch_bounds__(BT_T_NT) bt_T_kernel(const BtProb* __restrict__ probs) {
+  const BtProb P = probs[blockIdx.y];
   const int n = P.n;
-  const int nb = min(NBB, max(0, n - 1 - j0));
-  __shared__ double Ts[NBB][NBB + 1];
-  for (int idx = threadIdx.x; idx < NBB * NBB; idx += blockDim.x) Ts[idx % NBB][idx / NBB] = 0.0;
+  const int j0 = blockIdx.x * NBB;
+  const int nb = min(NBB, n - 1 - j0);
+  if (nb <= 0) return;
+  const double* G = P.G + (size_t)blockIdx.x * NBB * NBB;
+  double* T = P.T + (size_t)blockIdx.x * NBB * NBB;
+  extern __shared__ double btsm[];
+  double(*Ts)[NBB + 1] = reinterpret_cast<double(*)[NBB + 1]>(btsm);
+  double(*Gs)[NBB + 1] = reinterpret_cast<double(*)[NBB + 1]>(btsm + NBB * (NBB + 1));
+  for (int idx = threadIdx.x; idx < NBB * NBB; idx += BT_T_NT) {
+    const int r = idx % NBB, c = idx / NBB;
+    Ts[r][c] = 0.0;
+    Gs[r][c] = G[r + c * NBB];
+  }
   __syncthreads();
-  const int i = threadIdx.x;
+  const int i = threadIdx.x >> 2, q = threadIdx.x & 3;
   for (int j = 0; j < nb; ++j) {
-    const double tj = P.tau[j0 + j];
-    // T[0:j, j] = -tau_j T[0:j,0:j] G[0:j, j]   (G = V^T V, column-major NBB x NBB)
     double acc = 0.0;
-    if (i < j)
-      for (int l = i; l < j; ++l) acc += Ts[i][l] * P.G[l + j * NBB];
-    __syncthreads();
-    if (i < j) Ts[i][j] = -tj * acc;
-    if (i == j) Ts[j][j] = tj;
+    for (int l = i + q; l < j; l += 4) acc += Ts[i][l] * Gs[l][j];
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    // column j is written here and read only from step j+1 on
+    if (q == 0) {
+      const double tj = P.tau[j0 + j];
+      if (i < j) Ts[i][j] = -tj * acc;
+      else if (i == j) Ts[j][j] = tj;
+    }
     __syncthreads();
   }
-  for (int idx = threadIdx.x; idx < NBB * NBB; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < NBB * NBB; idx += BT_T_NT) {
     const int r = idx % NBB, c = idx / NBB;
-    P.T[r + c * NBB] = Ts[r][c];
+    T[r + c * NBB] = Ts[r][c];
   }
 }
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
 // Host helper that batches GEMM problems and launches them.
+// Launch descriptors of several launches gathered on the host and sent to
+// the device in one copy (instead of one small copy per launch).
+class DescPack {
+ public:
+  template <class T>
+  size_t add(const std::vector<T>& v) {
+    const size_t off = (buf_.size() + 255) & ~size_t(255);
+    buf_.resize(off + v.size() * sizeof(T));
+    if (!v.empty()) memcpy(buf_.data() + off, v.data(), v.size() * sizeof(T));
+    return off;
+  }
+  // device copy (stream-ordered); offsets from add() index into it
+  char* upload(DeviceArena& arena, cudaStream_t st) {
+    char* dev = static_cast<char*>(arena.alloc(buf_.size() + 256));
+    if (!buf_.empty()) NRGB_CUDA(cudaMemcpyAsync(dev, buf_.data(), buf_.size(), cudaMemcpyHostToDevice, st));
+    return dev;
+  }
+
+ private:
+  std::vector<char> buf_;
+};
+
 struct GemmBatch {
   std::vector<GemmProb> probs;
   std::vector<GemmSeg> segs;
@@ -1436,9 +1483,9 @@ size_t SyevBatched::workspace_bytes(const std::vector<int>& ns) {
     pl.add<double>((size_t)n * 16);
     pl.add<int>((size_t)n * 10);
     pl.add<double>(2 * RED);
-    pl.add<double>((size_t)n * NBB);
-    pl.add<double>((size_t)NBB * NBB * 2);
-    pl.add<double>((size_t)NBB * n * 2);
+    pl.add<double>((size_t)NBB * NBB * std::max(1, bt_nblk(n)));  // G
+    pl.add<double>((size_t)NBB * NBB * std::max(1, bt_nblk(n)));  // T
+    pl.add<double>((size_t)NBB * n * 2);                          // X (last block), Y
   }
   pl.add<double>(64 * 1024);
   int nmx = 0;
@@ -1446,10 +1493,23 @@ size_t SyevBatched::workspace_bytes(const std::vector<int>& ns) {
   // per-panel launch descriptors
   pl.add<char>((size_t)(nmx / NB + 2) * (ns.size() * (sizeof(TrdProb) + 2 * sizeof(GemmSeg) + sizeof(GemmProb)) + 2048));
   // zero-fill descriptors: the per-problem buffers once, the split-K
-  // outputs of every back-transformation block; cluster descriptors
+  // outputs of the back-transformation once; cluster descriptors
   size_t zs = 0;
-  for (int n : ns) zs += 4 + (size_t)n * n / ZERO_CHUNK + 2 * (NBB * (size_t)n / ZERO_CHUNK + 2) * (n / NBB + 2);
+  for (int n : ns)
+    zs += 6 + (size_t)n * n / ZERO_CHUNK + (size_t)NBB * NBB * bt_nblk(n) / ZERO_CHUNK +
+          (NBB * (size_t)n / ZERO_CHUNK + 2) * (n / NBB + 3);
   pl.add<ZeroSeg>(zs);
+  // divide-and-conquer descriptors (one copy): problems, leaves, and per
+  // merge node a node, a GEMM problem and a segment; 3 aligned arrays per level
+  size_t ndc = 0;
+  for (int n : ns) ndc += 2 * (size_t)(n / LEAF + 2);
+  pl.add<char>(ns.size() * sizeof(DcProb) + ndc * (sizeof(DcNode) + sizeof(GemmProb) + sizeof(GemmSeg)) +
+               256 * 3 * 40 + 1024);
+  // back-transformation GEMM descriptors (4 batches per block of reflectors)
+  size_t nbt = 0;
+  for (int n : ns) nbt += 4 * (size_t)(bt_nblk(n) + 1);
+  pl.add<char>(ns.size() * sizeof(BtProb) + nbt * (sizeof(GemmProb) + sizeof(GemmSeg)) +
+               256 * 6 * (size_t)(nmx / NBB + 4));
   pl.add<TrdClProb>(2 * ns.size() + 16);
   return pl.bytes + (size_t)ns.size() * 4096 + (1 << 20);
 }
@@ -1494,7 +1554,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     std::vector<TrdProb> tp(nbig);
     std::vector<DcProb> dp(nbig);
     std::vector<BtProb> bp(nbig);
-    std::vector<double*> dT(nbig), eT(nbig), tauT(nbig);
+    std::vector<double*> dT(nbig), eT(nbig), tauT(nbig), bt_X(nbig), bt_Y(nbig);
     std::vector<ZeroSeg> zeros;  // ranges that must start at zero, cleared in one launch
     for (int b = 0; b < nbig; ++b) {
       const SyevDesc& S = probs[big[b]];
@@ -1507,11 +1567,11 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       double* vec = arena_.alloc_n<double>((size_t)n * 16);
       int* ivec = arena_.alloc_n<int>((size_t)n * 10);
       double* red = arena_.alloc_n<double>(2 * RED);
-      double* Vb = arena_.alloc_n<double>((size_t)n * NBB);
-      double* G = arena_.alloc_n<double>((size_t)NBB * NBB);
-      double* T = arena_.alloc_n<double>((size_t)NBB * NBB);
-      double* X = arena_.alloc_n<double>((size_t)NBB * n);
-      double* Y = arena_.alloc_n<double>((size_t)NBB * n);
+      const int nblk = std::max(1, bt_nblk(n));
+      double* G = arena_.alloc_n<double>((size_t)NBB * NBB * nblk);
+      double* T = arena_.alloc_n<double>((size_t)NBB * NBB * nblk);
+      bt_X[b] = arena_.alloc_n<double>((size_t)NBB * n);
+      bt_Y[b] = arena_.alloc_n<double>((size_t)NBB * n);
       dT[b] = vec;
       eT[b] = vec + n;
       tauT[b] = vec + 2 * n;
@@ -1554,11 +1614,9 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       bt.n = n;
       bt.A = S.A;
       bt.tau = tauT[b];
-      bt.Vb = Vb;
+      bt.V = W1;  // free once divide and conquer is done
       bt.G = G;
       bt.T = T;
-      bt.X = X;
-      bt.Y = Y;
       zero_add(zeros, red, 2 * RED);
       zero_add(zeros, tauT[b], n);
       zero_add(zeros, S.Z, (long long)nn);
@@ -1649,7 +1707,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     }
     {
       const size_t smem = (size_t)(32 + 4 * NB + 8 + (TRD_NT / 32) * 2 * NB + nmax) * sizeof(double);
-      NRGB_CUDA(raise_panel_smem((int)smem));
+      NRGB_CUDA(raise_smem_attr((const void*)trd_panel_kernel, (int)smem));
       int per_sm = 0;
       NRGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trd_panel_kernel, TRD_NT, smem));
       per_sm = std::max(1, std::min(per_sm, 4));
@@ -1753,6 +1811,9 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       launch_clusters(tails);
     }
     // ---------------- 2) divide and conquer ----------------
+    // Leaves in one launch, then the merges level by level (all problems'
+    // nodes of a level together); every level's descriptors go to the
+    // device in one copy up front.
     {
       std::vector<DcNode> leaves;
       std::vector<std::pair<int, DcNode>> merges;
@@ -1762,39 +1823,57 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         plan_tree(b, 0, dp[b].n, leaves, merges, h);
         hmax = std::max(hmax, h);
       }
-      DcProb* d_dp = arena_.alloc_n<DcProb>(nbig);
-      NRGB_CUDA(cudaMemcpyAsync(d_dp, dp.data(), nbig * sizeof(DcProb), cudaMemcpyHostToDevice, st));
-      DcNode* d_leaves = arena_.alloc_n<DcNode>(leaves.size());
-      NRGB_CUDA(cudaMemcpyAsync(d_leaves, leaves.data(), leaves.size() * sizeof(DcNode),
-                                cudaMemcpyHostToDevice, st));
+      struct Level {
+        std::vector<DcNode> nodes;
+        GemmBatch gb;
+        int maxnp = 0;
+        size_t o_nodes = 0, o_gp = 0, o_gs = 0;
+      };
+      std::vector<Level> levels(hmax + 1);
+      for (auto& m : merges) levels[m.first].nodes.push_back(m.second);
+      DescPack pk;
+      const size_t o_dp = pk.add(dp);
+      const size_t o_leaves = pk.add(leaves);
+      for (int h = 1; h <= hmax; ++h) {
+        Level& L = levels[h];
+        for (auto& nd : L.nodes) {
+          const int np = nd.hi - nd.lo;
+          L.maxnp = std::max(L.maxnp, np);
+          GemmSeg sg{};
+          L.gb.add(nullptr, 0, np, np, 0.0, {sg});  // shapes fixed on device (n = k <= np)
+        }
+        // segments too, even though dc_prep fills them in: the copy sizes them
+        L.o_nodes = pk.add(L.nodes);
+        L.o_gp = pk.add(L.gb.probs);
+        L.o_gs = pk.add(L.gb.segs);
+      }
+      char* dev = pk.upload(arena_, st);
+      const DcProb* d_dp = reinterpret_cast<const DcProb*>(dev + o_dp);
       NRGB_LAUNCH("dc_leaf", st,
-                  dc_leaf_kernel<<<ceil_div((int)leaves.size(), 2), 64, 0, st>>>(d_dp, d_leaves,
-                                                                                 (int)leaves.size(), d_err_ + 1));
+                  dc_leaf_kernel<<<ceil_div((int)leaves.size(), 2), 64, 0, st>>>(
+                      d_dp, reinterpret_cast<const DcNode*>(dev + o_leaves), (int)leaves.size(), d_err_ + 1));
       NRGB_CUDA(cudaGetLastError());
       ++launches_;
+      NRGB_CUDA(raise_smem_attr((const void*)dc_prep_kernel, (int)dc_prep_smem(DC_PREP_CAP)));
       for (int h = 1; h <= hmax; ++h) {
-        std::vector<DcNode> lv;
-        for (auto& m : merges)
-          if (m.first == h) lv.push_back(m.second);
-        if (lv.empty()) continue;
-        const int nn = (int)lv.size();
-        int maxnp = 0;
-        GemmBatch gb;
-        for (auto& nd : lv) {
-          const int np = nd.hi - nd.lo;
-          maxnp = std::max(maxnp, np);
-          GemmSeg s{};
-          gb.add(nullptr, 0, np, np, 0.0, {s});  // shapes fixed on device (n = k <= np)
-        }
-        DcNode* d_nodes = arena_.alloc_n<DcNode>(nn);
-        GemmProb* d_gp = arena_.alloc_n<GemmProb>(nn);
-        GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(nn);
-        NRGB_CUDA(cudaMemcpyAsync(d_nodes, lv.data(), nn * sizeof(DcNode), cudaMemcpyHostToDevice, st));
-        NRGB_CUDA(cudaMemcpyAsync(d_gp, gb.probs.data(), nn * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
-        NRGB_LAUNCH("dc_prep", st, dc_prep_kernel<<<nn, DC_NT, 0, st>>>(d_dp, d_nodes, d_gp, d_gs));
+        Level& L = levels[h];
+        if (L.nodes.empty()) continue;
+        const int nn = (int)L.nodes.size();
+        const int maxnp = L.maxnp;
+        const DcNode* d_nodes = reinterpret_cast<const DcNode*>(dev + L.o_nodes);
+        GemmProb* d_gp = reinterpret_cast<GemmProb*>(dev + L.o_gp);
+        GemmSeg* d_gs = reinterpret_cast<GemmSeg*>(dev + L.o_gs);
+        const int cap = maxnp <= DC_PREP_CAP ? maxnp : 0;
+        NRGB_LAUNCH("dc_prep", st,
+                    dc_prep_kernel<<<nn, DC_NT, dc_prep_smem(cap), st>>>(d_dp, d_nodes, d_gp, d_gs, cap));
         NRGB_CUDA(cudaGetLastError());
         dim3 g1(ceil_div(maxnp, 128), nn);
-        NRGB_LAUNCH("dc_permute", st, dc_permute_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
+        dim3 gp(ceil_div(maxnp, 128), ceil_div(maxnp, DC_PCOLS), nn);
+        NRGB_LAUNCH("dc_permute", st, dc_gather_kernel<<<gp, 128, 0, st>>>(d_dp, d_nodes, 0));
+        NRGB_CUDA(cudaGetLastError());
+        NRGB_LAUNCH("dc_permute", st, dc_rotate_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
+        NRGB_CUDA(cudaGetLastError());
+        NRGB_LAUNCH("dc_permute", st, dc_gather_kernel<<<gp, 128, 0, st>>>(d_dp, d_nodes, 1));
         NRGB_CUDA(cudaGetLastError());
         dim3 gw(ceil_div(maxnp, 8), nn);
         NRGB_LAUNCH("dc_secular", st, dc_secular_warp_kernel<<<gw, 256, 0, st>>>(d_dp, d_nodes, d_err_ + 2));
@@ -1804,7 +1883,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         dim3 g2(ceil_div(maxnp, 8), nn);
         NRGB_LAUNCH("dc_vectors", st, dc_vectors_kernel<<<g2, 256, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
-        NRGB_CUDA(gemm_grouped_launch(d_gp, nn, d_gs, gb.tiles, st, "gemm_f64_dc", gb.stiles));
+        NRGB_CUDA(gemm_grouped_launch(d_gp, nn, d_gs, L.gb.tiles, st, "gemm_f64_dc", L.gb.stiles));
         NRGB_LAUNCH("dc_rank", st, dc_rank_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
         dim3 g3(maxnp, nn);
@@ -1812,76 +1891,66 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         NRGB_CUDA(cudaGetLastError());
         NRGB_LAUNCH("dc_copy", st, dc_copy_kernel<<<g3, 128, 0, st>>>(d_dp, d_nodes, 1));
         NRGB_CUDA(cudaGetLastError());
-        launches_ += 9;
+        launches_ += 11;
       }
       // problems that are a single leaf already have D, Q in place
     }
     // ---------------- 3) back-transformation ----------------
+    // Z = H_0 H_1 ... H_{n-2} Z in blocks of NBB reflectors, last block
+    // first: Z[r0:, :] -= V_k T_k (V_k^T Z[r0:, :]).  V (all reflectors, in
+    // W1), every G_k = V_k^T V_k and every T_k are formed up front in four
+    // launches; then three GEMMs per block.  Split-K outputs X_k live in
+    // their own slots (U, free after divide and conquer, holds blocks
+    // k with (k+1) NBB <= n; the last block uses X), zeroed once.  All
+    // descriptors go to the device in one copy.
     {
-      BtProb* d_bp = arena_.alloc_n<BtProb>(nbig);
-      NRGB_CUDA(cudaMemcpyAsync(d_bp, bp.data(), nbig * sizeof(BtProb), cudaMemcpyHostToDevice, st));
-      const int last = ((std::max(0, nmax - 2)) / NBB) * NBB;
-      for (int j0 = last; j0 >= 0; j0 -= NBB) {
-        // problems with reflectors in this block: n - 2 >= j0
-        std::vector<int> act;
-        for (int b = 0; b < nbig; ++b)
-          if (bp[b].n - 2 >= j0) act.push_back(b);
-        if (act.empty()) continue;
-        // V blocks (for all problems; inactive ones write zeros harmlessly)
-        NRGB_LAUNCH("bt_buildV", st, bt_buildV_kernel<<<dim3(NBB, nbig), 128, 0, st>>>(d_bp, j0));
-        NRGB_CUDA(cudaGetLastError());
-        GemmBatch g1, g3, g4;
-        std::vector<ZeroSeg> bzg, bzx;
-        auto zero_launch = [&](const std::vector<ZeroSeg>& z) {
-          if (z.empty()) return;
-          ZeroSeg* d_z = arena_.alloc_n<ZeroSeg>(z.size());
-          NRGB_CUDA(cudaMemcpyAsync(d_z, z.data(), z.size() * sizeof(ZeroSeg), cudaMemcpyHostToDevice, st));
-          NRGB_LAUNCH("zero_fill", st, zero_kernel<<<(unsigned)z.size(), 256, 0, st>>>(d_z));
-          NRGB_CUDA(cudaGetLastError());
-          ++launches_;
-        };
-        for (int b : act) {
-          const BtProb& P = bp[b];
-          const int n = P.n;
-          const int r0 = j0 + 1;
-          const int mrows = n - r0;
+      int kmax = 0;
+      for (int b = 0; b < nbig; ++b) kmax = std::max(kmax, bt_nblk(bp[b].n));
+      auto xslot = [&](int b, int k) {
+        const int n = bp[b].n;
+        return (k + 1) * NBB <= n ? dp[b].U + (size_t)k * NBB * n : bt_X[b];
+      };
+      auto xsplit = [](int mrows) { return std::max(1, std::min(16, mrows / 128)); };
+      auto gsplit = [](int mrows) { return std::max(1, std::min(16, mrows / 256)); };
+      std::vector<ZeroSeg> bz;
+      GemmBatch gg;  // every G_k
+      for (int b = 0; b < nbig; ++b) {
+        const BtProb& P = bp[b];
+        const int n = P.n;
+        for (int k = 0; k < bt_nblk(n); ++k) {
+          const int j0 = k * NBB, nb = std::min(NBB, n - 1 - j0), r0 = j0 + 1, mrows = n - r0;
           GemmSeg s{};
-          // G = Vb^T Vb  (rows r0..n)
-          s.A = P.Vb + r0;
+          s.A = P.V + r0 + (size_t)j0 * n;
           s.lda = n;
           s.transA = 1;
-          s.B = P.Vb + r0;
+          s.B = s.A;
           s.ldb = n;
           s.transB = 0;
           s.k = mrows;
           s.alpha = 1.0;
-          // one output tile, K = mrows: split the K loop so that many CTAs work
-          // (split-K accumulates with atomics into a zeroed output)
-          const int kg = std::max(1, std::min(64, mrows / 256));
-          if (kg > 1) zero_add(bzg, P.G, (long long)NBB * NBB);
-          g1.add(P.G, NBB, NBB, NBB, 0.0, {s}, kg);
+          const int kg = gsplit(mrows);
+          double* Gk = P.G + (size_t)k * NBB * NBB;
+          if (kg > 1) zero_add(bz, Gk, (long long)NBB * NBB);
+          gg.add(Gk, NBB, nb, nb, 0.0, {s}, kg);
+          if (xsplit(mrows) > 1) zero_add(bz, xslot(b, k), (long long)NBB * n);
         }
-        zero_launch(bzg);
-        {
-          GemmProb* d_gp = arena_.alloc_n<GemmProb>(g1.probs.size());
-          GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(g1.segs.size());
-          NRGB_CUDA(cudaMemcpyAsync(d_gp, g1.probs.data(), g1.probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
-          NRGB_CUDA(cudaMemcpyAsync(d_gs, g1.segs.data(), g1.segs.size() * sizeof(GemmSeg), cudaMemcpyHostToDevice, st));
-          KernelStats::get().add_work("gemm_f64_bt", gemm_flops(g1.probs.data(), (int)g1.probs.size(), g1.segs.data()));
-          NRGB_CUDA(gemm_grouped_launch(d_gp, (int)g1.probs.size(), d_gs, g1.tiles, st, "gemm_f64_bt", g1.stiles));
-        }
-        NRGB_LAUNCH("bt_T", st, bt_T_kernel<<<nbig, NBB, 0, st>>>(d_bp, j0));
-        NRGB_CUDA(cudaGetLastError());
-        // X = Vb^T Z ; Y = T X ; Z -= Vb Y   (rows r0..n of Z)
+      }
+      // per block k (descending): X_k = V_k^T Z, Y = T_k X_k, Z -= V_k Y
+      struct Step {
         GemmBatch gx, gy, gz;
-        for (int b : act) {
+      };
+      std::vector<Step> steps(kmax);
+      for (int k = kmax - 1; k >= 0; --k) {
+        Step& S = steps[k];
+        for (int b = 0; b < nbig; ++b) {
           const BtProb& P = bp[b];
           const int n = P.n;
-          const int r0 = j0 + 1;
-          const int mrows = n - r0;
+          if (k >= bt_nblk(n)) continue;
+          const int j0 = k * NBB, nb = std::min(NBB, n - 1 - j0), r0 = j0 + 1, mrows = n - r0;
           double* Z = probs[big[b]].Z;
+          double* Xk = xslot(b, k);
           GemmSeg s{};
-          s.A = P.Vb + r0;
+          s.A = P.V + r0 + (size_t)j0 * n;
           s.lda = n;
           s.transA = 1;
           s.B = Z + r0;
@@ -1889,41 +1958,73 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           s.transB = 0;
           s.k = mrows;
           s.alpha = 1.0;
-          const int kx = std::max(1, std::min(16, mrows / 512));
-          if (kx > 1) zero_add(bzx, P.X, (long long)NBB * n);
-          gx.add(P.X, NBB, NBB, n, 0.0, {s}, kx);
+          S.gx.add(Xk, NBB, nb, n, 0.0, {s}, xsplit(mrows));
           GemmSeg t{};
-          t.A = P.T;
+          t.A = P.T + (size_t)k * NBB * NBB;
           t.lda = NBB;
           t.transA = 0;
-          t.B = P.X;
+          t.B = Xk;
           t.ldb = NBB;
           t.transB = 0;
-          t.k = NBB;
+          t.k = nb;
           t.alpha = 1.0;
-          gy.add(P.Y, NBB, NBB, n, 0.0, {t});
+          S.gy.add(bt_Y[b], NBB, nb, n, 0.0, {t});
           GemmSeg u{};
-          u.A = P.Vb + r0;
+          u.A = P.V + r0 + (size_t)j0 * n;
           u.lda = n;
           u.transA = 0;
-          u.B = P.Y;
+          u.B = bt_Y[b];
           u.ldb = NBB;
           u.transB = 0;
-          u.k = NBB;
+          u.k = nb;
           u.alpha = -1.0;
-          gz.add(Z + r0, n, mrows, n, 1.0, {u});
+          S.gz.add(Z + r0, n, mrows, n, 1.0, {u});
         }
-        zero_launch(bzx);
-        for (GemmBatch* gbp : {&gx, &gy, &gz}) {
-          GemmBatch& gb = *gbp;
-          GemmProb* d_gp = arena_.alloc_n<GemmProb>(gb.probs.size());
-          GemmSeg* d_gs = arena_.alloc_n<GemmSeg>(gb.segs.size());
-          NRGB_CUDA(cudaMemcpyAsync(d_gp, gb.probs.data(), gb.probs.size() * sizeof(GemmProb), cudaMemcpyHostToDevice, st));
-          NRGB_CUDA(cudaMemcpyAsync(d_gs, gb.segs.data(), gb.segs.size() * sizeof(GemmSeg), cudaMemcpyHostToDevice, st));
-          KernelStats::get().add_work("gemm_f64_bt", gemm_flops(gb.probs.data(), (int)gb.probs.size(), gb.segs.data()));
-          NRGB_CUDA(gemm_grouped_launch(d_gp, (int)gb.probs.size(), d_gs, gb.tiles, st, "gemm_f64_bt", gb.stiles));
+      }
+      // one upload: problems, zero ranges, then the GEMM batches
+      DescPack pk;
+      const size_t o_bp = pk.add(bp);
+      const size_t o_bz = pk.add(bz);
+      std::vector<std::pair<size_t, size_t>> og;  // (probs, segs) offsets, batch order below
+      auto put = [&](const GemmBatch& g) { og.push_back({pk.add(g.probs), pk.add(g.segs)}); };
+      put(gg);
+      for (int k = kmax - 1; k >= 0; --k) {
+        put(steps[k].gx);
+        put(steps[k].gy);
+        put(steps[k].gz);
+      }
+      char* dev = pk.upload(arena_, st);
+      const BtProb* d_bp = reinterpret_cast<const BtProb*>(dev + o_bp);
+      size_t gi = 0;
+      auto gemm = [&](const GemmBatch& g) {
+        const std::pair<size_t, size_t> o = og[gi++];
+        if (g.empty()) return;
+        KernelStats::get().add_work("gemm_f64_bt", gemm_flops(g.probs.data(), (int)g.probs.size(), g.segs.data()));
+        NRGB_CUDA(gemm_grouped_launch(reinterpret_cast<const GemmProb*>(dev + o.first), (int)g.probs.size(),
+                                      reinterpret_cast<const GemmSeg*>(dev + o.second), g.tiles, st, "gemm_f64_bt",
+                                      g.stiles));
+        ++launches_;
+      };
+      if (kmax > 0) {
+        NRGB_LAUNCH("bt_buildV", st, bt_buildV_kernel<<<dim3(std::max(1, nmax - 1), nbig), 128, 0, st>>>(d_bp));
+        NRGB_CUDA(cudaGetLastError());
+        ++launches_;
+        if (!bz.empty()) {
+          NRGB_LAUNCH("zero_fill", st,
+                      zero_kernel<<<(unsigned)bz.size(), 256, 0, st>>>(reinterpret_cast<const ZeroSeg*>(dev + o_bz)));
+          NRGB_CUDA(cudaGetLastError());
+          ++launches_;
         }
-        launches_ += 6;
+        gemm(gg);
+        NRGB_CUDA(raise_smem_attr((const void*)bt_T_kernel, (int)BT_T_SMEM));
+        NRGB_LAUNCH("bt_T", st, bt_T_kernel<<<dim3(kmax, nbig), BT_T_NT, BT_T_SMEM, st>>>(d_bp));
+        NRGB_CUDA(cudaGetLastError());
+        ++launches_;
+        for (int k = kmax - 1; k >= 0; --k) {
+          gemm(steps[k].gx);
+          gemm(steps[k].gy);
+          gemm(steps[k].gz);
+        }
       }
     }
   }
