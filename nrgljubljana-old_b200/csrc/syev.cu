@@ -51,10 +51,11 @@ struct SmallProb {
 
 constexpr int SMALL_WARPS = 2;
 
+// Implicit symmetric QR with Wilkinson shift on tridiagonal (d, e),
+// rotations accumulated into the columns of Z (Z <- Z G^T).  dn, en: 32
+// doubles each of scratch (the step's new d, e).
 __device__ void givens_qr_sweep_warp(double* d, double* e, double (*Z)[33], int n, int lane,
-                                     double* cs, int* fail) {
-  // Implicit symmetric QR with Wilkinson shift on tridiagonal (d, e),
-  // rotations accumulated into the columns of Z (Z <- Z G^T).
+                                     double* cs, double* dn, double* en, int* fail) {
   int iter = 0;
   const int maxiter = 40 * n + 40;
   int hi = n - 1;
@@ -81,49 +82,60 @@ __device__ void givens_qr_sweep_warp(double* d, double* e, double (*Z)[33], int 
       if (lane == 0) atomicExch(fail, 1);
       break;
     }
-    // one implicit QR step on [lo, hi]
-    double x = 0.0, z = 0.0, bulge = 0.0;
+    // One implicit QR step on [lo, hi].  Every lane runs the same scalar
+    // recurrence (so no lane waits for another's rotation), carrying the
+    // running d[k], e[k], the bulge and the next x in registers.  The step
+    // reads only d, e and stores only into dn, en (lane 0), which are copied
+    // back after the step, so lanes need no synchronisation inside it.
+    double a = d[lo], b = e[lo];
+    double x, z = b;
+    {
+      const double dl = (d[hi - 1] - d[hi]) * 0.5;
+      const double eh = e[hi - 1];
+      const double den = dl + copysign(hypot(dl, eh), dl == 0.0 ? 1.0 : dl);
+      x = a - (d[hi] - eh * eh / den);
+    }
     for (int k = lo; k < hi; ++k) {
-      if (lane == 0) {
-        if (k == lo) {
-          const double dl = (d[hi - 1] - d[hi]) * 0.5;
-          const double eh = e[hi - 1];
-          const double den = dl + copysign(hypot(dl, eh), dl == 0.0 ? 1.0 : dl);
-          const double mu = d[hi] - eh * eh / den;
-          x = d[lo] - mu;
-          z = e[lo];
-        } else {
-          x = e[k - 1];
-          z = bulge;
-        }
-        const double r = hypot(x, z);
-        double c = 1.0, s = 0.0;
-        if (r != 0.0) {
-          c = x / r;
-          s = z / r;
-        }
-        if (k > lo) e[k - 1] = r;
-        // rotate the 2x2 block [[d_k, e_k],[e_k, d_k1]] by R = [[c, s],[-s, c]]
-        const double a = d[k], b = e[k], dd = d[k + 1];
-        d[k] = c * c * a + 2.0 * c * s * b + s * s * dd;
-        d[k + 1] = s * s * a - 2.0 * c * s * b + c * c * dd;
-        e[k] = c * s * (dd - a) + (c * c - s * s) * b;
-        if (k + 1 < hi) {
-          bulge = s * e[k + 1];
-          e[k + 1] = c * e[k + 1];
-        }
-        cs[0] = c;
-        cs[1] = s;
+      const double dd = d[k + 1];
+      const double ekn = (k + 1 < hi) ? e[k + 1] : 0.0;
+      double c = 1.0, s = 0.0, r = 0.0;
+      const double r2 = x * x + z * z;
+      if (r2 > 0.0 && r2 < 1e300) {
+        r = sqrt(r2);
+        const double ri = 1.0 / r;
+        c = x * ri;
+        s = z * ri;
+      } else if (x != 0.0 || z != 0.0) {  // squares out of range
+        r = hypot(x, z);
+        c = x / r;
+        s = z / r;
       }
-      __syncwarp();
-      const double c = cs[0], s = cs[1];
+      const double cc = c * c, ss = s * s, csb = 2.0 * c * s * b;
+      const double dk = cc * a + csb + ss * dd;
+      const double dk1 = ss * a - csb + cc * dd;
+      const double ek = c * s * (dd - a) + (cc - ss) * b;
+      if (lane == 0) {
+        if (k > lo) en[k - 1] = r;
+        dn[k] = dk;
+      }
       if (lane < n) {
         const double zk = Z[lane][k], zk1 = Z[lane][k + 1];
         Z[lane][k] = c * zk + s * zk1;
         Z[lane][k + 1] = -s * zk + c * zk1;
       }
-      __syncwarp();
+      a = dk1;  // d[k+1]
+      x = ek;   // e[k], the next rotation's x
+      b = c * ekn;
+      z = s * ekn;  // bulge
     }
+    if (lane == 0) {
+      dn[hi] = a;
+      en[hi - 1] = x;
+    }
+    __syncwarp();
+    if (lane >= lo && lane <= hi) d[lane] = dn[lane];
+    if (lane >= lo && lane < hi) e[lane] = en[lane];
+    __syncwarp();
   }
   __syncwarp();
 }
@@ -196,7 +208,7 @@ __global__ void __launch_bounds__(32 * SMALL_WARPS) syev_small_kernel(const Smal
     }
     __syncwarp();
   }
-  givens_qr_sweep_warp(d, e, Z, n, lane, csv[warp], fail);
+  givens_qr_sweep_warp(d, e, Z, n, lane, csv[warp], v, w, fail);
   // sort ascending (selection sort by lane 0, swap columns by all lanes)
   for (int i = 0; i < n - 1; ++i) {
     if (lane == 0) {
@@ -825,7 +837,7 @@ __global__ void __launch_bounds__(64) dc_leaf_kernel(const DcProb* __restrict__ 
                                                      const DcNode* __restrict__ leaves, int nleaf,
                                                      int* fail) {
   __shared__ double Zs[2][32][33];
-  __shared__ double dv[2][32], ev[2][32], csv[2][4];
+  __shared__ double dv[2][32], ev[2][32], csv[2][4], dnv[2][32], env[2][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int li = blockIdx.x * 2 + warp;
   if (li >= nleaf) return;
@@ -844,7 +856,7 @@ __global__ void __launch_bounds__(64) dc_leaf_kernel(const DcProb* __restrict__ 
   }
   for (int j = 0; j < s; ++j) Z[lane][j] = (lane == j) ? 1.0 : 0.0;
   __syncwarp();
-  givens_qr_sweep_warp(d, e, Z, s, lane, csv[warp], fail);
+  givens_qr_sweep_warp(d, e, Z, s, lane, csv[warp], dnv[warp], env[warp], fail);
   for (int i = 0; i < s - 1; ++i) {
     if (lane == 0) {
       int kmin = i;
@@ -1188,10 +1200,11 @@ __global__ void dc_secular_warp_kernel(const DcProb* __restrict__ probs, const D
   }
 }
 
-// Loewner z-hat.  One thread per i.
+// Loewner z-hat.  One warp per i; lanes share the product over j.
 __global__ void dc_lowner_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes) {
   const int node = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   const DcNode N = nodes[node];
   const DcProb P = probs[N.prob];
   const int lo = N.lo;
@@ -1201,10 +1214,12 @@ __global__ void dc_lowner_kernel(const DcProb* __restrict__ probs, const DcNode*
   const double rho = P.rho[lo];
   const double di = d[i];
   auto lam_minus = [&](int j) { return (d[P.orig[lo + j]] - di) + P.tau[lo + j]; };
-  double prod = lam_minus(k - 1) / rho;
-  for (int j = 0; j < i; ++j) prod *= lam_minus(j) / (d[j] - di);
-  for (int j = i; j < k - 1; ++j) prod *= lam_minus(j) / (d[j + 1] - di);
-  P.zhat[lo + i] = copysign(sqrt(fmax(prod, 0.0)), P.zs[lo + i]);
+  double prod = 1.0;
+  for (int j = lane; j < k - 1; j += 32) prod *= lam_minus(j) / ((j < i ? d[j] : d[j + 1]) - di);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) prod *= __shfl_xor_sync(0xffffffffu, prod, o);
+  prod *= lam_minus(k - 1) / rho;
+  if (lane == 0) P.zhat[lo + i] = copysign(sqrt(fmax(prod, 0.0)), P.zs[lo + i]);
 }
 
 // Eigenvectors of the rank-one problem.  One warp per column j.
@@ -1232,10 +1247,12 @@ __global__ void dc_vectors_kernel(const DcProb* __restrict__ probs, const DcNode
   for (int i = lane; i < k; i += 32) col[i] *= inv;
 }
 
-// Final order: rank of every eigenvalue of the node; writes D and the source.
+// Final order: rank of every eigenvalue of the node (one warp per value,
+// lanes share the comparisons); writes D and the rank.
 __global__ void dc_rank_kernel(const DcProb* __restrict__ probs, const DcNode* __restrict__ nodes) {
   const int node = blockIdx.y;
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const int a = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   const DcNode N = nodes[node];
   const DcProb P = probs[N.prob];
   const int lo = N.lo, np = N.hi - N.lo;
@@ -1246,13 +1263,16 @@ __global__ void dc_rank_kernel(const DcProb* __restrict__ probs, const DcNode* _
     return b < k ? d[P.orig[lo + b]] + P.tau[lo + b] : P.dD[lo + b];
   };
   const double x = val(a);
-  int r = 0;
-  for (int b = 0; b < np; ++b) {
+  unsigned r = 0;
+  for (int b = lane; b < np; b += 32) {
     const double y = val(b);
     r += (y < x) || (y == x && b < a);
   }
-  P.rank[lo + a] = r;
-  P.D[lo + r] = x;
+  r = __reduce_add_sync(0xffffffffu, r);
+  if (lane == 0) {
+    P.rank[lo + a] = (int)r;
+    P.D[lo + r] = x;
+  }
 }
 
 // Deflated columns Q[:, lo+a] (a >= k) -> W1[:, lo+a]; then all columns of
@@ -1439,6 +1459,8 @@ SyevBatched::SyevBatched() {
     NRGB_CUDA(cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming));
   }
   NRGB_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+  NRGB_CUDA(cudaStreamCreateWithFlags(&small_st_, cudaStreamNonBlocking));
+  NRGB_CUDA(cudaEventCreateWithFlags(&small_done_, cudaEventDisableTiming));
 }
 
 SyevBatched::~SyevBatched() {
@@ -1449,6 +1471,8 @@ SyevBatched::~SyevBatched() {
     if (join_[i]) cudaEventDestroy(join_[i]);
   }
   if (fork_) cudaEventDestroy(fork_);
+  if (small_done_) cudaEventDestroy(small_done_);
+  if (small_st_) cudaStreamDestroy(small_st_);
 }
 
 namespace {
@@ -1539,10 +1563,14 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     for (int i : small) sp.push_back(SmallProb{probs[i].A, probs[i].w, probs[i].Z, probs[i].n});
     SmallProb* d_sp = arena_.alloc_n<SmallProb>(sp.size());
     NRGB_CUDA(cudaMemcpyAsync(d_sp, sp.data(), sp.size() * sizeof(SmallProb), cudaMemcpyHostToDevice, st));
-    NRGB_LAUNCH("syev_small", st,
-                syev_small_kernel<<<ceil_div((int)sp.size(), SMALL_WARPS), 32 * SMALL_WARPS, 0, st>>>(
+    // on its own stream, beside the larger blocks; joined before the flags are read
+    NRGB_CUDA(cudaEventRecord(fork_, st));
+    NRGB_CUDA(cudaStreamWaitEvent(small_st_, fork_, 0));
+    NRGB_LAUNCH("syev_small", small_st_,
+                syev_small_kernel<<<ceil_div((int)sp.size(), SMALL_WARPS), 32 * SMALL_WARPS, 0, small_st_>>>(
                     d_sp, (int)sp.size(), d_err_));
     NRGB_CUDA(cudaGetLastError());
+    NRGB_CUDA(cudaEventRecord(small_done_, small_st_));
     ++launches_;
   }
 
@@ -1878,13 +1906,13 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         dim3 gw(ceil_div(maxnp, 8), nn);
         NRGB_LAUNCH("dc_secular", st, dc_secular_warp_kernel<<<gw, 256, 0, st>>>(d_dp, d_nodes, d_err_ + 2));
         NRGB_CUDA(cudaGetLastError());
-        NRGB_LAUNCH("dc_lowner", st, dc_lowner_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
+        NRGB_LAUNCH("dc_lowner", st, dc_lowner_kernel<<<gw, 256, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
         dim3 g2(ceil_div(maxnp, 8), nn);
         NRGB_LAUNCH("dc_vectors", st, dc_vectors_kernel<<<g2, 256, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
         NRGB_CUDA(gemm_grouped_launch(d_gp, nn, d_gs, L.gb.tiles, st, "gemm_f64_dc", L.gb.stiles));
-        NRGB_LAUNCH("dc_rank", st, dc_rank_kernel<<<g1, 128, 0, st>>>(d_dp, d_nodes));
+        NRGB_LAUNCH("dc_rank", st, dc_rank_kernel<<<gw, 256, 0, st>>>(d_dp, d_nodes));
         NRGB_CUDA(cudaGetLastError());
         dim3 g3(maxnp, nn);
         NRGB_LAUNCH("dc_copy", st, dc_copy_kernel<<<g3, 128, 0, st>>>(d_dp, d_nodes, 0));
@@ -2028,6 +2056,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       }
     }
   }
+  if (!small.empty()) NRGB_CUDA(cudaStreamWaitEvent(st, small_done_, 0));
   // error flags
   int herr[4] = {0, 0, 0, 0};
   GridBarrier hb{};

@@ -78,6 +78,9 @@ class SyevBatched : public EigSolver {
   static constexpr int NAUX = 6;
   cudaStream_t aux_[NAUX] = {};
   cudaEvent_t fork_ = nullptr, join_[NAUX] = {};
+  // the warp solver for blocks up to 32 runs beside the larger blocks' work
+  cudaStream_t small_st_ = nullptr;
+  cudaEvent_t small_done_ = nullptr;
 };
 
 }  // namespace nrgb
