@@ -31,7 +31,7 @@ namespace nrgb {
 namespace {
 
 constexpr int SMALL_N = 32;     // warp-per-problem path
-constexpr int LEAF = 32;        // D&C leaf size
+constexpr int LEAF = 16;        // D&C leaf size
 constexpr int NB = 32;          // tridiagonalisation panel width
 constexpr int NBB = 64;         // back-transformation block of reflectors
 constexpr int TRD_NT = 256;     // threads of the panel kernel
