@@ -482,11 +482,18 @@ __host__ __device__ inline int trdc_ld(int n) { return n | 1; }
 
 // Doubles of dynamic shared memory one CTA needs for a block of size n on
 // a cluster of cl CTAs: its columns (j = rank, rank + cl, ...) in full, then
-// v, y, w (n each), one partial dot product per thread, one partial sum
-// per warp and per CTA, 2 x 4 scalars.
+// v and y (n each), one partial column dot per thread, one partial sum of
+// y^T v per warp of every CTA, 2 x 4 scalars.
 __host__ __device__ inline size_t trdc_smem_doubles(int n, int cl) {
-  return (size_t)((n + cl - 1) / cl) * trdc_ld(n) + 3 * (size_t)n + TRDC_NT + TRDC_NT / 32 + (size_t)cl + 8;
+  return (size_t)((n + cl - 1) / cl) * trdc_ld(n) + 2 * (size_t)n + TRDC_NT + (size_t)cl * (TRDC_NT / 32) + 8;
 }
+
+// Active held columns up to this count take the warp-per-column-group
+// product (lanes across rows, shuffle reductions, no CTA barrier); more take
+// lanes across columns (no shuffles) with a CTA barrier before the sums.
+#ifndef TRDC_WARPCOL_MAX
+#define TRDC_WARPCOL_MAX 32
+#endif
 
 // Barrier over the CTAs of the cluster (a plain CTA barrier for CL = 1).
 template <int CL>
@@ -543,14 +550,19 @@ __device__ __forceinline__ void trdc_reflector(const TrdClProb& P, const double*
 // reduction across CTAs: y_j is the dot product of the held column j with v.
 // Per column c, two cluster barriers:
 //   a. every CTA reads the owner's column c through distributed shared
-//      memory to form v, computes y_j for its columns (lanes across 32
-//      columns, warps across column groups and row segments) and writes
-//      them, and its part of y^T v, into every CTA; barrier;
-//   b. every CTA forms w = tau y - tau^2/2 (y^T v) v and applies
-//      A -= v w^T + w v^T to its columns (loads of four columns and two
-//      rows issued before their stores).  Meanwhile warp 0 of the owner of
-//      column c+1 updates that column first and forms its reflector (norm,
-//      beta, tau), writing the scalars into every CTA; barrier.
+//      memory to form v (CTA barrier) and computes y_j for its columns:
+//      with few active columns each warp takes four columns at a time
+//      (lanes across rows, shuffle reductions); with many, lanes take
+//      columns and warps row segments, summed after a CTA barrier.  Each
+//      y_j goes into every CTA, and each warp's part of y^T v into its own
+//      slot of every CTA; cluster barrier;
+//   b. every warp sums the slots (all in the same order, so every CTA
+//      holds the same y^T v) and applies A -= v w^T + w v^T to its columns
+//      with w = tau y - tau^2/2 (y^T v) v formed on the fly (loads of four
+//      columns and two rows issued before their stores).  Meanwhile warp 0
+//      of the owner of column c+1 updates that column first and forms its
+//      reflector (norm, beta, tau), writing the scalars into every CTA;
+//      cluster barrier.
 // Output as the panel kernel: d, e, tau, and v below the subdiagonal of A.
 template <int CL>
 __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* __restrict__ probs) {
@@ -567,11 +579,9 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
   double* Acol = sm;                                     // ncol columns, ld lds
   double* v = Acol + (size_t)((n + CL - 1) / CL) * lds;  // n
   double* y = v + n;                                     // n (written by every CTA)
-  double* w = y + n;                                     // n
-  double* ypart = w + n;                                 // TRDC_NT partial column dots
-  double* wpart = ypart + TRDC_NT;                       // nwarps parts of y^T v
-  double* part = wpart + nwarps;                         // CL parts of y^T v, one per CTA
-  double* misc = part + CL;                              // 2 x 4 reflector scalars
+  double* ypart = y + n;                                 // TRDC_NT partial column dots
+  double* part = ypart + TRDC_NT;                        // CL x nwarps parts of y^T v
+  double* misc = part + CL * nwarps;                     // 2 x 4 reflector scalars
 
   for (int l = 0; l < ncol; ++l) {
     const double* src = P.A + (size_t)(r + l * CL) * ld;
@@ -596,55 +606,81 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
     // held columns after c: local indices l0 .. ncol-1
     const int l0 = (c + 1 - r + CL - 1) / CL > 0 ? (c + 1 - r + CL - 1) / CL : 0;
     const int nact = ncol > l0 ? ncol - l0 : 0;
-    const int chunks = (nact + 31) >> 5;
-    const int segs = chunks ? max(1, nwarps / chunks) : 0;
-    if (warp < chunks * segs) {
-      const int ch = warp % chunks, sg = warp / chunks;
-      const int m = n - c - 1;
-      const int per = (m + segs - 1) / segs;
-      const int i0 = c + 1 + sg * per, i1 = min(n, i0 + per);
-      const int t = ch * 32 + lane;
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-      if (t < nact) {
-        const double* a = Acol + (size_t)(l0 + t) * lds;
-        int i = i0;
-        for (; i + 3 < i1; i += 4) {
-          s0 += a[i] * v[i];
-          s1 += a[i + 1] * v[i + 1];
-          s2 += a[i + 2] * v[i + 2];
-          s3 += a[i + 3] * v[i + 3];
-        }
-        for (; i < i1; ++i) s0 += a[i] * v[i];
-      }
-      ypart[sg * (chunks * 32) + t] = (s0 + s1) + (s2 + s3);
-    }
-    __syncthreads();
     double sp = 0.0;
-    for (int t = tid; t < nact; t += TRDC_NT) {
-      double yj = 0.0;
-      for (int sg = 0; sg < segs; ++sg) yj += ypart[sg * (chunks * 32) + t];
-      const int j = r + (l0 + t) * CL;
+    if (nact <= TRDC_WARPCOL_MAX) {
+      // warp w: active columns t = w, w + nwarps, ..., four at a time
+      for (int t0 = warp; t0 < nact; t0 += 4 * nwarps) {
+        const double* a[4];
+        bool on[4];
 #pragma unroll
-      for (int q = 0; q < CL; ++q) trdc_at<CL>(y, q)[j] = yj;
-      sp += yj * v[j];
+        for (int k = 0; k < 4; ++k) {
+          const int t = t0 + k * nwarps;
+          on[k] = t < nact;
+          a[k] = Acol + (size_t)(l0 + (on[k] ? t : t0)) * lds;
+        }
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = c + 1 + lane; i < n; i += 32) {
+          const double vi = v[i];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc[k] += a[k][i] * vi;
+        }
+#pragma unroll
+        for (int o2 = 16; o2 > 0; o2 >>= 1) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o2);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (!on[k]) continue;
+          const int j = r + (l0 + t0 + k * nwarps) * CL;
+          if (lane < CL) trdc_at<CL>(y, lane)[j] = acc[k];
+          sp += acc[k] * v[j];
+        }
+      }
+    } else {
+      // lanes across 32 columns, warps across column groups and row segments
+      const int chunks = (nact + 31) >> 5;
+      const int segs = max(1, nwarps / chunks);
+      if (warp < chunks * segs) {
+        const int ch = warp % chunks, sg = warp / chunks;
+        const int m = n - c - 1;
+        const int per = (m + segs - 1) / segs;
+        const int i0 = c + 1 + sg * per, i1 = min(n, i0 + per);
+        const int t = ch * 32 + lane;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        if (t < nact) {
+          const double* a = Acol + (size_t)(l0 + t) * lds;
+          int i = i0;
+          for (; i + 3 < i1; i += 4) {
+            s0 += a[i] * v[i];
+            s1 += a[i + 1] * v[i + 1];
+            s2 += a[i + 2] * v[i + 2];
+            s3 += a[i + 3] * v[i + 3];
+          }
+          for (; i < i1; ++i) s0 += a[i] * v[i];
+        }
+        ypart[sg * (chunks * 32) + t] = (s0 + s1) + (s2 + s3);
+      }
+      __syncthreads();
+      for (int t = tid; t < nact; t += TRDC_NT) {
+        double yj = 0.0;
+        for (int sg = 0; sg < segs; ++sg) yj += ypart[sg * (chunks * 32) + t];
+        const int j = r + (l0 + t) * CL;
+#pragma unroll
+        for (int q = 0; q < CL; ++q) trdc_at<CL>(y, q)[j] = yj;
+        sp += yj * v[j];
+      }
+      sp = warp_sum(sp);
     }
-    sp = warp_sum(sp);
-    if (lane == 0) wpart[warp] = sp;
-    __syncthreads();
-    if (warp == 0) {
-      const double x = warp_sum(lane < nwarps ? wpart[lane] : 0.0);
-      if (lane < CL) trdc_at<CL>(part, lane)[r] = x;
-    }
+    if (lane < CL) trdc_at<CL>(part, lane)[r * nwarps + warp] = sp;
     trdc_sync<CL>();
-    // ---- b: w, the rank-2 update, the next reflector ----
+    // ---- b: the rank-2 update with w on the fly, the next reflector ----
     double ytv = 0.0;
-#pragma unroll
-    for (int q = 0; q < CL; ++q) ytv += part[q];
+    for (int q = lane; q < CL * nwarps; q += 32) ytv += part[q];
+    ytv = warp_sum(ytv);
     const double a2 = -0.5 * tc * tc * ytv;
-    for (int i = c + 1 + tid; i < n; i += TRDC_NT) w[i] = tc * y[i] + a2 * v[i];
     if (r == o)
       for (int i = c + 2 + tid; i < n; i += TRDC_NT) P.A[i + (size_t)c * ld] = v[i];
-    __syncthreads();
     const int cn = c + 1;
     const bool own_next = cn < n - 1 && r == cn % CL;  // column cn is then local column l0
     const int wfirst = own_next ? 1 : 0;
@@ -657,12 +693,13 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
         for (int k = 0; k < 4; ++k) {
           const int j = r + (l + min(k, nl - 1)) * CL;
           vj[k] = v[j];
-          wj[k] = w[j];
+          wj[k] = tc * y[j] + a2 * v[j];
         }
         double* a0 = Acol + (size_t)l * lds;
         int i = c + 1 + lane;
         for (; i + 32 < n; i += 64) {
-          const double v0 = v[i], w0 = w[i], v1 = v[i + 32], w1 = w[i + 32];
+          const double v0 = v[i], v1 = v[i + 32];
+          const double w0 = tc * y[i] + a2 * v0, w1 = tc * y[i + 32] + a2 * v1;
           double x[8];
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
@@ -682,7 +719,8 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
             }
         }
         if (i < n) {
-          const double v0 = v[i], w0 = w[i];
+          const double v0 = v[i];
+          const double w0 = tc * y[i] + a2 * v0;
           double x[4];
 #pragma unroll
           for (int k = 0; k < 4; ++k) x[k] = k < nl ? a0[(size_t)k * lds + i] : 0.0;
@@ -697,8 +735,8 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
     if (own_next && warp == 0) {
       double* col = Acol + (size_t)l0 * lds;
       if (tc != 0.0) {
-        const double vj = v[cn], wj = w[cn];
-        for (int i = c + 1 + lane; i < n; i += 32) col[i] -= v[i] * wj + w[i] * vj;
+        const double vj = v[cn], wj = tc * y[cn] + a2 * v[cn];
+        for (int i = c + 1 + lane; i < n; i += 32) col[i] -= v[i] * wj + (tc * y[i] + a2 * v[i]) * vj;
         __syncwarp();
       }
       trdc_reflector<CL>(P, col, cn, n, misc + (cn & 1) * 4, lane);

@@ -78,10 +78,10 @@ def _random_sym(n, rng, kind):
 
 # covers the warp path (n <= 32), the cluster path (one cluster of 1..16 CTAs
 # per block; single-CTA launches split at 64, 96, 128; the cluster size
-# changes after 167, 236, 332, 464, and blocks above 653 take the
+# changes after 168, 237, 333, 469, and blocks above 656 take the
 # cooperative panel path) and the panel path
-SIZES = [1, 2, 3, 5, 16, 31, 32, 33, 40, 64, 65, 96, 97, 100, 128, 129, 167, 168, 236, 237, 257, 332, 333,
-         464, 465, 600, 653, 654, 1100]
+SIZES = [1, 2, 3, 5, 16, 31, 32, 33, 40, 64, 65, 96, 97, 100, 128, 129, 168, 169, 237, 238, 257, 333, 334,
+         469, 470, 600, 656, 657, 1100]
 
 
 @pytest.mark.parametrize("kind", ["gauss", "logspaced", "degenerate"])
