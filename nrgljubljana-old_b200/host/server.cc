@@ -19,6 +19,7 @@ namespace nrgb {
 EigBatcher::EigBatcher(int device, double window_us) : device_(device), window_us_(window_us) {
   NRGB_CUDA(cudaSetDevice(device_));
   for (int l = 0; l < NLANE; ++l) {
+    lanes_[l].cls = l < NSMALL ? 0 : 1;
     lanes_[l].syev.reset(new SyevBatched());
     NRGB_CUDA(cudaStreamCreateWithFlags(&lanes_[l].stream, cudaStreamNonBlocking));
   }
@@ -60,8 +61,8 @@ void EigBatcher::counters(double* calls, double* requests, double* problems) {
 }
 
 int EigBatcher::pending_locked() const {
-  int n = 0;
-  for (const Lane& L : lanes_) n += (int)L.q.size() + L.inflight;
+  int n = (int)q_[0].size() + (int)q_[1].size();
+  for (const Lane& L : lanes_) n += L.inflight;
   return n;
 }
 
@@ -70,12 +71,12 @@ int EigBatcher::solve(const std::vector<SyevDesc>& probs, cudaStream_t stream) {
   r.probs = &probs;
   int nmax = 0;
   for (const SyevDesc& d : probs) nmax = std::max(nmax, d.n);
-  const int lane = (cluster_nmax_ > 0 && nmax <= cluster_nmax_) ? 0 : 1;
+  const int cls = (cluster_nmax_ > 0 && nmax <= cluster_nmax_) ? 0 : 1;
   NRGB_CUDA(cudaEventCreateWithFlags(&r.ready, cudaEventDisableTiming));
   NRGB_CUDA(cudaEventRecord(r.ready, stream));  // the blocks are assembled on the caller's stream
   {
     std::unique_lock<std::mutex> lk(m_);
-    lanes_[lane].q.push_back(&r);
+    q_[cls].push_back(&r);
     cv_.notify_all();
     done_cv_.wait(lk, [&] { return r.done; });
   }
@@ -87,18 +88,22 @@ int EigBatcher::solve(const std::vector<SyevDesc>& probs, cudaStream_t stream) {
 void EigBatcher::loop(int lane) {
   cudaSetDevice(device_);
   Lane& L = lanes_[lane];
+  const int k = L.cls;
+  std::deque<Req*>& q = q_[k];
   std::unique_lock<std::mutex> lk(m_);
   for (;;) {
-    cv_.wait(lk, [&] { return stop_ || !L.q.empty(); });
-    if (L.q.empty()) return;  // stop requested and nothing pending
+    cv_.wait(lk, [&] { return (stop_ && q.empty()) || (!q.empty() && !gathering_[k]); });
+    if (q.empty()) return;  // stop requested and nothing pending in this class
     // gather: wait (at most the window) until every run inside its first
-    // sweep has its blocks queued or being solved, in either lane
+    // sweep has its blocks queued or being solved, in any lane
+    gathering_[k] = true;
     const auto deadline = std::chrono::steady_clock::now() + std::chrono::microseconds((long)window_us_);
     while (!stop_ && pending_locked() < clients_) {
       if (cv_.wait_until(lk, deadline) == std::cv_status::timeout) break;
     }
-    std::vector<Req*> batch(L.q.begin(), L.q.end());
-    L.q.clear();
+    gathering_[k] = false;
+    std::vector<Req*> batch(q.begin(), q.end());
+    q.clear();
     L.inflight = (int)batch.size();
     lk.unlock();
     run_batch(L, batch);

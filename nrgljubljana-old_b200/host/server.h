@@ -36,13 +36,15 @@
 
 namespace nrgb {
 
-// Merges the eigensolver batches of concurrent runs (see above).  Two lanes,
-// each with its own thread, stream and solver: requests whose blocks all fit
-// the cluster tridiagonalisation, and requests with larger blocks (which
-// also need the cooperative panel launches).  Merged calls of the two lanes
-// overlap on the device, so runs with small blocks do not wait for the
-// panel phase of large ones, and cooperative launches come from one lane
-// only.
+// Merges the eigensolver batches of concurrent runs (see above).  Requests
+// fall in two classes: those whose blocks all fit the cluster
+// tridiagonalisation, and those with larger blocks (which also need the
+// cooperative panel launches).  Each class has its own queue and lanes; a
+// lane is a thread with its own stream and solver.  The small class has
+// NSMALL lanes, so a new merged call starts while the previous one still
+// runs (these calls are latency-bound and leave most SMs free); the large
+// class has one lane, so cooperative launches come from one lane only.
+// Only one lane of a class gathers at a time.
 class EigBatcher : public EigSolver {
  public:
   EigBatcher(int device, double window_us);
@@ -62,23 +64,26 @@ class EigBatcher : public EigSolver {
     std::string err;
   };
   struct Lane {
+    int cls = 0;  // 0: blocks that fit a cluster; 1: larger blocks
     std::unique_ptr<SyevBatched> syev;
     cudaStream_t stream = nullptr;
-    std::deque<Req*> q;
     int inflight = 0;  // requests in the lane's running merged call
     std::thread th;
   };
-  static constexpr int NLANE = 2;
+  static constexpr int NSMALL = 2;
+  static constexpr int NLANE = NSMALL + 1;
   void loop(int lane);
   void run_batch(Lane& L, const std::vector<Req*>& batch);
   int pending_locked() const;
 
   int device_;
   double window_us_;
-  int cluster_nmax_ = 0;  // blocks up to this size take the small lane
+  int cluster_nmax_ = 0;  // blocks up to this size take the small class
   Lane lanes_[NLANE];
+  std::deque<Req*> q_[2];              // queued requests per class
+  bool gathering_[2] = {false, false};  // a lane of the class is gathering
   std::mutex m_;
-  std::condition_variable cv_;       // a request arrived, or stop
+  std::condition_variable cv_;       // a request arrived, a call ended, or stop
   std::condition_variable done_cv_;  // a merged call finished
   int clients_ = 0;  // runs inside their first sweep
   bool stop_ = false;
