@@ -51,6 +51,8 @@ class DeviceArena {
   template <class T>
   T* alloc_n(size_t n) { return static_cast<T*>(alloc(n * sizeof(T) + 8)); }
   size_t used() const { return off_; }
+  // byte offset of a pointer handed out by alloc()
+  size_t offset_of(const void* p) const { return (size_t)(static_cast<const char*>(p) - static_cast<const char*>(base_)); }
   size_t capacity() const { return cap_; }
   void reset() { off_ = 0; }
   void release() {

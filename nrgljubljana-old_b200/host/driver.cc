@@ -21,6 +21,7 @@
 
 #include <math.h>
 #include <stdio.h>
+#include <string.h>
 
 #include <algorithm>
 #include <chrono>
@@ -210,14 +211,35 @@ struct NrgDriver::Impl {
   std::vector<double> wstage;  // host staging of per-step eigenvalue uploads
 
   Impl(cudaStream_t s, EigSolver* e) : st(s), syev(e) {}
+  ~Impl() {
+    if (desc_pin) {
+      cudaStreamSynchronize(st);
+      cudaFreeHost(desc_pin);
+    }
+  }
+  Impl(const Impl&) = delete;
+  Impl& operator=(const Impl&) = delete;
 
   // ---------------- small helpers ----------------
+  // Launch descriptors: the first DESC_PINNED bytes of the descriptor arena
+  // have a pinned host mirror, so their uploads are plain DMA (a pageable
+  // source goes through the CUDA driver's staging buffer, which the run
+  // threads of a server share).  The mirror is rewritten only after
+  // desc_reset(), which waits for the stream.
+  static constexpr size_t DESC_PINNED = 4 << 20;
+  char* desc_pin = nullptr;
   template <class T>
   T* upload(const std::vector<T>& v) {
     if (v.empty()) return nullptr;
     const size_t bytes = v.size() * sizeof(T);
     T* d = static_cast<T*>(desc.alloc(bytes));
-    NRGB_CUDA(cudaMemcpyAsync(d, v.data(), bytes, cudaMemcpyHostToDevice, st));
+    const size_t off = desc.offset_of(d);
+    if (desc_pin && off + bytes <= DESC_PINNED) {
+      memcpy(desc_pin + off, v.data(), bytes);
+      NRGB_CUDA(cudaMemcpyAsync(d, desc_pin + off, bytes, cudaMemcpyHostToDevice, st));
+    } else {
+      NRGB_CUDA(cudaMemcpyAsync(d, v.data(), bytes, cudaMemcpyHostToDevice, st));
+    }
     h2d += bytes;
     return d;
   }
@@ -1288,6 +1310,7 @@ struct NrgDriver::Impl {
     std::unique_ptr<Section> sec(new Section(this, "read input"));
     desc.reserve(64 << 20);
     desc.reset();
+    if (!desc_pin) NRGB_CUDA(cudaMallocHost(&desc_pin, DESC_PINNED));
     P = Params();
     P.read(wd + "/param");
     D = DataFile();
