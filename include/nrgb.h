@@ -93,6 +93,12 @@ int nrgb_eig_recalc_step_dev(nrgb_ctx* ctx, int nblocks, const int* n, double* c
 /* Launch accounting: enable != 0 turns on per-kernel timing with CUDA events
  * (and resets all counters); enable == 0 turns it off. */
 int nrgb_profile(nrgb_ctx* ctx, int enable);
+/* As nrgb_profile(ctx, 1), but only launches of kernel `name` (or of a prefix
+ * ending in '*') are timed; all launches are still counted.  Each timed
+ * launch records two CUDA events, so timing every launch of a many-threaded
+ * caller (a run server) slows it down; timing one kernel keeps that cost to
+ * its own launches.  No counterpart in the reference. */
+int nrgb_profile_only(nrgb_ctx* ctx, const char* name);
 /* Launches and total device milliseconds of kernel `name` since the last
  * nrgb_profile call ("*" = all kernels of the library; ms is 0 unless timing
  * is on).  Names: trd_panel, gemm_f64, syev_small, dc_*, bt_*, assemble_*,

@@ -301,6 +301,11 @@ int nrgb_profile(nrgb_ctx* ctx, int enable) {
   return guarded(ctx, [&] { nrgb::KernelStats::get().enable(enable != 0); });
 }
 
+int nrgb_profile_only(nrgb_ctx* ctx, const char* name) {
+  if (!name) return 1;
+  return guarded(ctx, [&] { nrgb::KernelStats::get().enable(true, name); });
+}
+
 int nrgb_kernel_stats(nrgb_ctx* ctx, const char* name, long* launches, double* ms) {
   return guarded(ctx, [&] { nrgb::KernelStats::get().query(name ? name : "*", launches, ms); });
 }

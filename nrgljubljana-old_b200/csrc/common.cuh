@@ -82,7 +82,9 @@ struct ArenaPlan {
 class KernelStats {
  public:
   static KernelStats& get();
-  void enable(bool on);              // resets all counters
+  // resets all counters; with `only` (a name, or a prefix ending in '*'),
+  // only launches of that name are timed, the others are just counted
+  void enable(bool on, const char* only = nullptr);
   bool timing() const { return timing_; }
   // bracket one launch: begin() before (counts it and, with timing on,
   // records the start event and returns a slot), end(slot) after
@@ -100,6 +102,7 @@ class KernelStats {
   struct Rec { std::string name; cudaEvent_t a, b; };
   std::mutex m_;
   bool timing_ = false;
+  std::string only_;  // empty: time every launch
   std::vector<Rec> open_, done_;
   std::vector<int> free_;
   std::vector<cudaEvent_t> pool_;

@@ -21,19 +21,31 @@ cudaEvent_t KernelStats::ev() {
   return e;
 }
 
-void KernelStats::enable(bool on) {
+namespace {
+// `name` matches `pat`: "*" (everything), a prefix ending in '*', or the
+// name itself
+bool name_matches(const char* name, const char* pat) {
+  const size_t len = strlen(pat);
+  if (len == 1 && pat[0] == '*') return true;
+  if (len > 1 && pat[len - 1] == '*') return strncmp(name, pat, len - 1) == 0;
+  return strcmp(name, pat) == 0;
+}
+}  // namespace
+
+void KernelStats::enable(bool on, const char* only) {
   std::lock_guard<std::mutex> g(m_);
   settle();
   counts_.clear();
   ms_.clear();
   work_.clear();
   timing_ = on;
+  only_ = only ? only : "";
 }
 
 int KernelStats::begin(const char* name, cudaStream_t s) {
   std::lock_guard<std::mutex> g(m_);
   count_locked(name, 1);
-  if (!timing_) return -1;
+  if (!timing_ || (!only_.empty() && !name_matches(name, only_.c_str()))) return -1;
   int slot;
   if (!free_.empty()) {
     slot = free_.back();

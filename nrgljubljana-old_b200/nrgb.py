@@ -13,7 +13,7 @@ LIBPATH = os.path.join(HERE, "libnrgb.so")
 
 EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
            "nrgb_syev_batched", "nrgb_syev_batched_dev", "nrgb_gemm_grouped_dev",
-           "nrgb_eig_recalc_step", "nrgb_eig_recalc_step_dev", "nrgb_profile", "nrgb_kernel_stats",
+           "nrgb_eig_recalc_step", "nrgb_eig_recalc_step_dev", "nrgb_profile", "nrgb_profile_only", "nrgb_kernel_stats",
            "nrgb_kernel_work",
            "nrgb_basis_change_noalloc", "nrgb_run", "nrgb_set_eig_mode",
            "nrgb_server_create", "nrgb_server_submit", "nrgb_server_wait", "nrgb_server_error",
@@ -57,6 +57,7 @@ def load(path: str = LIBPATH):
     lib.nrgb_eig_recalc_step_dev.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                              C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp), vp]
     lib.nrgb_profile.argtypes = [vp, C.c_int]
+    lib.nrgb_profile_only.argtypes = [vp, C.c_char_p]
     lib.nrgb_kernel_stats.argtypes = [vp, C.c_char_p, C.POINTER(C.c_long), dp]
     lib.nrgb_kernel_work.argtypes = [vp, C.c_char_p, dp]
     lib.nrgb_basis_change_noalloc.argtypes = [C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
@@ -143,8 +144,13 @@ class Context:
             no, (C.c_int * no)(*bra), (C.c_int * no)(*ket), self._ptrs(op), self._ptrs(out),
             C.c_void_p(stream)), "nrgb_eig_recalc_step_dev")
 
-    def profile(self, enable=True):
-        self._check(self.lib.nrgb_profile(self.h, 1 if enable else 0), "nrgb_profile")
+    def profile(self, enable=True, only=None):
+        """Launch accounting on (counters reset) or off; with `only` (a kernel
+        name, or a prefix ending in '*'), only those launches are timed."""
+        if enable and only:
+            self._check(self.lib.nrgb_profile_only(self.h, only.encode()), "nrgb_profile_only")
+        else:
+            self._check(self.lib.nrgb_profile(self.h, 1 if enable else 0), "nrgb_profile")
 
     def kernel_stats(self, name="*"):
         n = C.c_long()
