@@ -491,9 +491,7 @@ __host__ __device__ inline size_t trdc_smem_doubles(int n, int cl) {
 // Active held columns up to this count take the warp-per-column-group
 // product (lanes across rows, shuffle reductions, no CTA barrier); more take
 // lanes across columns (no shuffles) with a CTA barrier before the sums.
-#ifndef TRDC_WARPCOL_MAX
-#define TRDC_WARPCOL_MAX 32
-#endif
+constexpr int TRDC_WARPCOL_MAX = 32;
 
 // Barrier over the CTAs of the cluster (a plain CTA barrier for CL = 1).
 template <int CL>
@@ -748,11 +746,12 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
   trdc_sync<CL>();
 }
 
+// Launch configuration of the cluster kernel for `nprob` blocks.  The
+// kernel's attributes (largest dynamic shared memory, non-portable cluster
+// size) are set once per device, at the largest size any launch uses, by the
+// solver's constructor (set_attr): setting them per launch to the launch's
+// own size would race between solver instances on other threads.
 template <int CL>
-// The kernel's attributes (largest dynamic shared memory, non-portable
-// cluster size) are set once per device, at the largest size any launch uses,
-// by the solver's constructor (set_attr): setting them per launch to the
-// launch's own size would race between solver instances on other threads.
 cudaError_t trdc_config(size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int nprob,
                         cudaStream_t st, bool set_attr) {
   cfg = cudaLaunchConfig_t{};

@@ -118,6 +118,31 @@ def test_syev_per_block_mode_matches_batched(ctx):
         assert np.abs(A @ Zb - Zb * b).max() <= 1e-13 * nrm * A.shape[0]
 
 
+def test_profile_only_times_one_kernel(ctx):
+    """With timing restricted to one kernel, every launch is still counted but
+    only that kernel's launches carry CUDA-event time."""
+    rng = np.random.default_rng(12)
+    mats = [_random_sym(n, rng, "degenerate") for n in (100, 200)]
+    ctx.profile(True, only="trd_cluster")
+    try:
+        ctx.syev_batched(mats)
+        n_cl, ms_cl = ctx.kernel_stats("trd_cluster")
+        n_dc, ms_dc = ctx.kernel_stats("dc_*")
+        n_all, _ = ctx.kernel_stats("*")
+    finally:
+        ctx.profile(False)
+    assert n_cl >= 1 and ms_cl > 0
+    assert n_dc >= 1 and ms_dc == 0
+    assert n_all > n_cl + n_dc - 1
+    ctx.profile(True)
+    try:
+        ctx.syev_batched(mats)
+        n_dc2, ms_dc2 = ctx.kernel_stats("dc_*")
+    finally:
+        ctx.profile(False)
+    assert n_dc2 == n_dc and ms_dc2 > 0
+
+
 def test_gemm_grouped_large_tiles(ctx):
     """Problems large enough that the launch uses the 128x128-tile kernel."""
     import nrgb
