@@ -1007,12 +1007,14 @@ __global__ void __launch_bounds__(DC_NT) dc_prep_kernel(const DcProb* __restrict
         prev = j;
         continue;
       }
-      double s = wz[prev], c = wz[j];
-      const double t = hypot(c, s);
+      // |dt c s| <= tol with c = z_j / t, s = -z_p / t, t = |(z_j, z_p)|,
+      // tested as |dt z_j z_p| <= tol t^2: no root or division for the
+      // entries that stay (both |z| exceed tol / rho here, so t^2 is normal)
+      const double zp = wz[prev], zj = wz[j];
       const double dt = wd[j] - wd[prev];
-      c /= t;
-      s = -s / t;
-      if (fabs(dt * c * s) <= tol) {
+      if (fabs(dt * zj * zp) <= tol * (zj * zj + zp * zp)) {
+        const double t = hypot(zj, zp);
+        const double c = zj / t, s = -zp / t;
         wz[j] = t;
         wz[prev] = 0.0;
         const double dp = wd[prev], dj = wd[j];
