@@ -28,6 +28,24 @@ def test_projection_grows_with_keep_and_chain_length(tmp_path):
     assert p[200] >= 8.0 * 20 * dim * dim
 
 
+def test_projection_of_two_channel_runs(tmp_path):
+    """Two channels: 16 combinations per subspace, so the block dimension bound
+    is D = 16 (keep + safeguardmax); each extra step adds D^2 + D doubles of
+    eigenvectors and, with FDM, two K'^2 density matrices."""
+    import nrgb
+    p = {}
+    for nmax in (8, 12):
+        wd = os.path.join(str(tmp_path), "kondo2_%d" % nmax)
+        inputgen.make_kondo(wd, [0.2, 0.2], 3.0, nmax, params={"keep": 300, "fdm": True, "T": 1e-3})
+        p[nmax] = nrgb.project_bytes(wd)
+    kp = 300 + 200
+    dim = 16 * kp
+    assert p[12] - p[8] == pytest.approx(8.0 * 4 * (dim * dim + dim + 2 * kp * kp), rel=1e-12)
+    # one channel with the same keep and chain length needs far less
+    one = nrgb.project_bytes(_run(str(tmp_path), 300, 12))
+    assert p[12] > 10 * one
+
+
 def test_projection_rejects_missing_input(tmp_path):
     import nrgb
     with pytest.raises(RuntimeError):
