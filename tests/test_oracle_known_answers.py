@@ -205,3 +205,27 @@ def test_dmnrg_density_matrix_traces_and_fdm_agreement(tmp_path):
     wf = fdm.pos.w + fdm.neg.w
     for i in range(40, len(wd), 10):
         assert abs(wd[i:i + 10].sum() - wf[i:i + 10].sum()) < 0.03
+
+
+def test_broadening_kernel_weight_and_log_shift():
+    """BR_NEW broadening of one peak well above omega0 is the log-Gaussian
+    kernel of src/spectral.h:70-102: it carries the peak's whole weight onto
+    the positive mesh, none onto the negative one, and shifts the mean of
+    ln E by alpha * gamma = alpha^2 / 4 (substitute x = ln(E/E0) / alpha)."""
+    P = {"alpha": 0.3, "omega0": 1e-6, "omega0_ratio": 1.0, "T": 1e-6, "Nmax": 30, "discretization": "Y",
+         "Lambda": 2.0, "z": 1.0, "bandrescale": 1.0, "broaden_min": 1e-5, "broaden_min_ratio": 3.0,
+         "broaden_max": 2.5, "broaden_ratio": 1.01}
+    E0, wt = 1e-2, 0.7
+    out = O.broaden(P, np.array([E0]), np.array([wt]), np.array([]), np.array([]))
+    E = np.array([e for e, _ in out])
+    A = np.array([a for _, a in out])
+    pos = E > 0
+    Ep, Ap = E[pos], A[pos]
+    assert np.all(A[~pos] == 0.0)
+    # integrate on the log mesh: dE = E d(ln E)
+    lnE = np.log(Ep)
+    f = Ap * Ep
+    total = np.trapezoid(f, lnE)
+    assert total == pytest.approx(wt, rel=1e-6)
+    mean = np.trapezoid(f * lnE, lnE) / total
+    assert mean == pytest.approx(math.log(E0) + P["alpha"] ** 2 / 4.0, abs=1e-6)
