@@ -229,3 +229,28 @@ def test_broadening_kernel_weight_and_log_shift():
     assert total == pytest.approx(wt, rel=1e-6)
     mean = np.trapezoid(f * lnE, lnE) / total
     assert mean == pytest.approx(math.log(E0) + P["alpha"] ** 2 / 4.0, abs=1e-6)
+
+
+def test_log_bins_split_rules():
+    """Bins::add (src/bins.h): a peak between bin energies e_i and e_i+1 is
+    split linearly in log10 E, which keeps its weight and its mean bin
+    position; peaks below the grid go to the first bin and above it to the
+    last; weights below discard_immediately * E are dropped."""
+    P = {"bins": 10, "emax": 10.0, "emin": 1e-5, "discard_immediately": 1e-16}
+    b = O.Bins(P, 10)
+    assert b.n == (1 - (-5)) * 10 + 1 and b.e[0] == pytest.approx(1e-5) and b.e[-1] == pytest.approx(10.0)
+    rng = np.random.default_rng(3)
+    E = 10.0 ** rng.uniform(-4.9, 0.9, 500)
+    W = rng.uniform(0.1, 1.0, 500)
+    b.add_many(E, W)
+    pos = (np.log10(E) + 5) * 10
+    assert b.w.sum() == pytest.approx(W.sum(), rel=1e-14)
+    assert np.dot(b.w, np.arange(b.n)) == pytest.approx(np.dot(W, pos), rel=1e-12)
+    # a peak on a bin energy lands whole in that bin
+    c = O.Bins(P, 10)
+    c.add_many([c.e[17]], [2.0])
+    assert c.w[17] == pytest.approx(2.0, rel=1e-12) and abs(c.w.sum() - 2.0) < 1e-14
+    # under- and overflow, and the discard rule
+    d = O.Bins(P, 10)
+    d.add_many([1e-9, 1e3, 1e-2], [0.5, 0.25, 1e-20])
+    assert d.w[0] == 0.5 and d.w[-1] == 0.25 and d.w.sum() == 0.75
