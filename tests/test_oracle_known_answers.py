@@ -254,3 +254,25 @@ def test_log_bins_split_rules():
     d = O.Bins(P, 10)
     d.add_many([1e-9, 1e3, 1e-2], [0.5, 0.25, 1e-20])
     assert d.w[0] == 0.5 and d.w[-1] == 0.25 and d.w.sum() == 0.75
+
+
+def test_free_moment_plateaus(tmp_path):
+    """A decoupled level (V = 0) with U = 0.2, eps_d = -U/2 is a free spin
+    1/2 at T << U/2: against a run whose level is pushed far above the band,
+    the td columns differ by T chi = <Sz^2> = 1/4 and S = ln 2 (columns of
+    src/nrg.cc:454-461, src/sym-QS.cc:12-14).  The residue is truncation: with
+    the impurity doublet each band multiplet splits in two, so the same keep
+    holds fewer band states (at keep 200 the entropy gap is 0.670)."""
+    import nrg_cases as cases
+    td = {}
+    for name, U, eps in (("moment", 0.2, -0.1), ("empty", 0.0, 10.0)):
+        wd = str(tmp_path / name)
+        g.make_siam(wd, U, eps, 0.02, 2.0, 20, V=0.0, params={"keep": 700, "T": 1e-5})
+        O.Oracle(wd).run(wd + "/out")
+        td[name] = cases.read_table(wd + "/out/td")
+    low = td["moment"][:, 0] < 0.01  # T << U/2
+    assert low.sum() >= 6
+    d_tchi = td["moment"][low, 1] - td["empty"][low, 1]
+    d_s = td["moment"][low, 8] - td["empty"][low, 8]
+    assert np.all(np.abs(d_tchi - 0.25) < 2e-4)
+    assert np.all(np.abs(d_s - math.log(2.0)) < 3e-3)
