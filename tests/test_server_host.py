@@ -52,6 +52,30 @@ def test_projection_rejects_missing_input(tmp_path):
         nrgb.project_bytes(str(tmp_path / "nothing"))
 
 
+@pytest.mark.parametrize("damage", ["half", "five_lines", "empty", "garbage_line"])
+def test_damaged_data_is_refused(tmp_path, damage):
+    """A truncated or corrupted data file is refused with an error status
+    (the host reader checks every read), never a crash or a partial result."""
+    import nrgb
+    wd = _run(str(tmp_path), 100, 10)
+    lines = open(os.path.join(wd, "data")).read().splitlines(True)
+    txt = {"half": "".join(lines[:len(lines) // 2]), "five_lines": "".join(lines[:5]), "empty": "",
+           "garbage_line": "".join(lines[:3]) + "xyz abc\n" + "".join(lines[4:])}[damage]
+    open(os.path.join(wd, "data"), "w").write(txt)
+    with pytest.raises(RuntimeError, match="status 2"):
+        nrgb.project_bytes(wd)
+
+
+def test_damaged_param_is_refused(tmp_path):
+    import nrgb
+    wd = _run(str(tmp_path), 100, 10)
+    txt = open(os.path.join(wd, "param")).read()
+    assert "keep=100" in txt
+    open(os.path.join(wd, "param"), "w").write(txt.replace("keep=100", "keep=abc"))
+    with pytest.raises(RuntimeError, match="status 2"):
+        nrgb.project_bytes(wd)
+
+
 def test_server_needs_a_device():
     import torch
 
