@@ -276,3 +276,28 @@ def test_free_moment_plateaus(tmp_path):
     d_s = td["moment"][low, 8] - td["empty"][low, 8]
     assert np.all(np.abs(d_tchi - 0.25) < 2e-4)
     assert np.all(np.abs(d_s - math.log(2.0)) < 3e-3)
+
+
+@pytest.mark.parametrize("nntanh", [0.0, 3.0])
+def test_dmnrg_shell_windows_partition_unity(nntanh):
+    """N/N+2 merge of DM-NRG spectra (src/spectrumrealfreq.cc:109-185): shell
+    N covers (E_min, E_max) = goodE s (1, Lambda^2) with the crossover at
+    goodE s Lambda, and shell N+2 has s / Lambda, so on their overlap the
+    falling window of N+2 and the rising window of N sum to one, for the
+    linear ramp and for the tanh profile; the first shell keeps full weight
+    above its crossover and the last below it."""
+    P = {"NNtanh": nntanh}
+    lam, good, s = 2.0, 2.0, 1e-3
+
+    def shell(scale, first=False, last=False):
+        lo, x, hi = good * scale, good * scale * lam, good * scale * lam ** 2
+        return lambda e: O._window(P, e, lo, x, hi, first, last)
+
+    e = np.geomspace(good * s * 1.0001, good * s * lam * 0.9999, 200)
+    total = shell(s)(e) + shell(s / lam)(e)
+    assert np.max(np.abs(total - 1.0)) < 1e-12
+    # three shells: every energy strictly inside the covered range sums to 1
+    e3 = np.geomspace(good * s / lam ** 2 * 1.0001, good * s * lam ** 2 * 0.9999, 400)
+    e3 = e3[np.abs(np.log(e3 / (good * s)) / np.log(lam) - np.round(np.log(e3 / (good * s)) / np.log(lam))) > 1e-6]
+    t3 = shell(s, first=True)(e3) + shell(s / lam)(e3) + shell(s / lam ** 2, last=True)(e3)
+    assert np.max(np.abs(t3 - 1.0)) < 1e-12
