@@ -1734,9 +1734,13 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         if (grp[g].empty()) continue;
         cudaStream_t sx = aux_[used % NAUX];
         if (used < NAUX) NRGB_CUDA(cudaStreamWaitEvent(sx, fork_, 0));
-        double fl = 0;
-        for (const TrdClProb& t : grp[g]) fl += 4.0 / 3.0 * (double)t.n * t.n * t.n;
+        double fl = 0, by = 0;
+        for (const TrdClProb& t : grp[g]) {
+          fl += 4.0 / 3.0 * (double)t.n * t.n * t.n;
+          by += 8.0 * (double)t.n * t.n;  // the block, read from HBM once
+        }
         KernelStats::get().add_work("trd_cluster", fl);
+        KernelStats::get().add_work("trd_cluster_hbm", by);
         const int np = (int)grp[g].size();
         const int k = g > 3 ? g - 3 : 0;
         cudaError_t e = cudaSuccess;
