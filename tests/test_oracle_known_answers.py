@@ -301,3 +301,28 @@ def test_dmnrg_shell_windows_partition_unity(nntanh):
     e3 = e3[np.abs(np.log(e3 / (good * s)) / np.log(lam) - np.round(np.log(e3 / (good * s)) / np.log(lam))) > 1e-6]
     t3 = shell(s, first=True)(e3) + shell(s / lam)(e3) + shell(s / lam ** 2, last=True)(e3)
     assert np.max(np.abs(t3 - 1.0)) < 1e-12
+
+
+def test_fixeps_cluster_snapping_quirks():
+    """find_clusters / fix_splittings (src/splitting.cc:5-77): sorted energies
+    closer than fixeps to the first of their cluster are mapped onto it; the
+    last cluster of the list is not processed; the map persists across steps
+    and keeps its first entry for a value; fix_splittings rewrites only mapped
+    values."""
+    class Host:
+        P = {"fixeps": 1e-15}
+        cluster_map = {}
+
+    h = Host()
+    h.cluster_map = {}
+    one_b = 1.0 + 4.0 * np.finfo(float).eps
+    two_b = 2.0 + 4.0 * np.finfo(float).eps
+    E = np.array([0.0, 1e-16, 5e-16, 1.0, one_b, 1.5, 2.0, two_b])
+    O.Oracle.find_clusters(h, E)
+    assert h.cluster_map == {1e-16: 0.0, 5e-16: 0.0, one_b: 1.0}
+    # a later step: 1e-16 heads a new cluster, but its old entry stays
+    O.Oracle.find_clusters(h, np.array([1e-16, 3e-16, 7.0, 8.0]))
+    assert h.cluster_map[1e-16] == 0.0 and h.cluster_map[3e-16] == 1e-16
+    diag = {"I": O.Eig(value=np.array([5e-16, 0.7, one_b]), vec=np.eye(3), kept=3)}
+    assert O.Oracle.fix_splittings(h, diag)
+    assert list(diag["I"].value) == [0.0, 0.7, 1.0]
