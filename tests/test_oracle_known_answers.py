@@ -326,3 +326,31 @@ def test_fixeps_cluster_snapping_quirks():
     diag = {"I": O.Eig(value=np.array([5e-16, 0.7, one_b]), vec=np.eye(3), kept=3)}
     assert O.Oracle.fix_splittings(h, diag)
     assert list(diag["I"].value) == [0.0, 0.7, 1.0]
+
+
+def test_noninteracting_level_lowest_excitation_is_single_particle(tmp_path):
+    """U = 0: every many-body level is a sum of single-particle levels of the
+    tridiagonal chain Hamiltonian (impurity, hybridisation V, Wilson chain
+    zeta_n, xi_n), so at step N the lowest excitation, times SCALE(N+1), is
+    the smallest |eps_k| of the impurity plus N+2 chain sites: exactly while
+    nothing is truncated, and to the truncation error after."""
+    info = g.make_siam(str(tmp_path), 0.0, 0.0, 0.02, 2.0, 20, params={"keep": 400, "T": 1e-3})
+    o = O.Oracle(str(tmp_path))
+    o.run(str(tmp_path / "out"))
+    xi, zeta, V = info["xi"], info["zeta"], info["V"]
+    for k, rec in enumerate(o.steps):
+        N = o.Ninit + k
+        L = N + 2
+        H = np.zeros((L + 1, L + 1))
+        H[0, 1] = H[1, 0] = V
+        for i in range(L):
+            H[1 + i, 1 + i] = zeta[i]
+            if i + 1 < L:
+                H[1 + i, 2 + i] = H[2 + i, 1 + i] = xi[i]
+        eps = np.abs(np.linalg.eigvalsh(H))
+        lowest_sp = np.min(eps[eps > 1e-12])
+        vals = np.concatenate([e.value for e in rec.eig.values()])
+        lowest_mb = np.min(vals[vals > 1e-9]) * O.SCALE(o.P, N + 1)
+        truncated = any(o.steps[j].kept[I] < o.steps[j].total[I] for j in range(k) for I in o.steps[j].kept)
+        tol = 2e-5 if truncated else 1e-12
+        assert lowest_mb == pytest.approx(lowest_sp, rel=tol), (N, truncated)
