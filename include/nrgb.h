@@ -124,11 +124,13 @@ int nrgb_kernel_work(nrgb_ctx* ctx, const char* name, double* units);
  * process exits.  Limits: at most 1024 operators, and the descriptors plus all
  * n_bra*n_ket intermediates (each rounded up to 256 bytes) must fit in 32 MiB.
  * The first call on a device looks up the array's device address (set-up);
- * make that first call before any stream capture.  Calls share the array:
- * calls whose GPU work overlaps race, so order them on one stream; the call
- * returns after its work on `stream` has finished.
+ * make that first call before any stream capture.  Calls share the array, so
+ * one call runs at a time per process: a process-wide lock serialises the
+ * calls and each call blocks until its work on `stream` has finished (the
+ * call is synchronous, whatever stream it is given).  A call on a stream that
+ * is capturing returns 7 and enqueues nothing, leaving the capture intact.
  * Returns 0 on success, 1 for invalid arguments, 5 when the sizes exceed the
- * limits above, 6 on a CUDA error. */
+ * limits above, 6 on a CUDA error, 7 when `stream` is capturing. */
 int nrgb_basis_change_noalloc(int nops, const int* n_bra, const int* n_ket, const double* const* z_bra,
                               const double* const* z_ket, const double* const* op, double* const* out,
                               void* stream);

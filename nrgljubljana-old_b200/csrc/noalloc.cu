@@ -17,14 +17,19 @@
 // exits.  All calls share it:
 //   * nothing in it has to start at zero: each call writes every byte of the
 //     scratch it later reads (descriptors, then intermediates with beta = 0);
-//   * calls whose work overlaps on the GPU (different streams, or different
-//     host threads on one device without ordering) race on the array; order
-//     them on one stream or serialise them.
+//   * one call runs at a time per process: a process-wide lock serialises
+//     the calls, and each call blocks until its work on `stream` has
+//     finished, so two calls never have work on the array at the same time,
+//     whichever streams or host threads they come from.  The price is that
+//     the call is synchronous; callers that overlap streams get no
+//     asynchrony from it.
 // Host code never touches g_basis_scratch by name (on the host that name is
 // only a stand-in for the device symbol): the device address comes from
 // cudaGetSymbolAddress, once per device, with that device current, on the
 // first call on that device.  Make that first call before any stream
-// capture begins.
+// capture begins.  A call whose `stream` is capturing is refused (status 7)
+// before anything is enqueued, so the caller's capture stays intact: the
+// call's final stream synchronisation would otherwise end that capture.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -77,12 +82,18 @@ extern "C" int nrgb_basis_change_noalloc(int nops, const int* n_bra, const int* 
   }
   if (need > NOALLOC_SCRATCH_BYTES) return 5;  // larger than the static scratch
   if (nops == 0) return 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  {
+    // the call ends with a stream synchronisation, which a capture forbids
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return 6;
+    if (cs != cudaStreamCaptureStatusNone) return 7;
+  }
   std::lock_guard<std::mutex> lock(g_call_mutex);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return 6;
   unsigned char* base = scratch_address(dev);
   if (!base) return 6;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
 
   unsigned char* d_p1 = base;
   unsigned char* d_s1 = d_p1 + align256(nops * sizeof(nrgb::GemmProb));

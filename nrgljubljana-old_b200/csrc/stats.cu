@@ -108,21 +108,32 @@ void KernelStats::count_locked(const char* name, long n) {
 }
 
 void KernelStats::settle() {
-  for (auto& r : done_) {
+  // Take the finished records out of done_ first: each record is counted at
+  // most once and its events go back to the pool exactly once, even when a
+  // CUDA error ends the loop early (the failed record and the ones after it
+  // are dropped, and the error is reported once at the end).
+  std::vector<Rec> recs;
+  recs.swap(done_);
+  cudaError_t first_err = cudaSuccess;
+  for (const Rec& r : recs) {
     float ms = 0.f;
-    NRGB_CUDA(cudaEventSynchronize(r.b));
-    NRGB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
-    bool found = false;
-    for (auto& m : ms_)
-      if (m.first == r.name) {
-        m.second += ms;
-        found = true;
-      }
-    if (!found) ms_.push_back({r.name, (double)ms});
+    cudaError_t e = first_err == cudaSuccess ? cudaEventSynchronize(r.b) : first_err;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, r.a, r.b);
+    if (e == cudaSuccess) {
+      bool found = false;
+      for (auto& m : ms_)
+        if (m.first == r.name) {
+          m.second += ms;
+          found = true;
+        }
+      if (!found) ms_.push_back({r.name, (double)ms});
+    } else if (first_err == cudaSuccess) {
+      first_err = e;
+    }
     pool_.push_back(r.a);
     pool_.push_back(r.b);
   }
-  done_.clear();
+  NRGB_CUDA(first_err);
 }
 
 void KernelStats::query(const char* name, long* launches, double* ms) {

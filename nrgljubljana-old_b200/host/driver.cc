@@ -188,7 +188,12 @@ struct NrgDriver::Impl {
   double totalenergy = 0.0, GSenergy = 0.0;
   std::vector<std::vector<double>> td_rows;
   std::vector<std::pair<double, std::map<std::string, double>>> expv_rows;
-  std::vector<std::vector<std::pair<double, Invar>>> annotated;
+  // per measured step: energy scale, total energy, all (energy, subspace) pairs
+  struct Annotated {
+    double scale, total;
+    std::vector<std::pair<double, Invar>> levels;
+  };
+  std::vector<Annotated> annotated;
   // statistics
   double t_diag = 0, t_recalc = 0, t_dm = 0, t_spec = 0;
   double launches = 0, h2d = 0, d2h = 0;
@@ -525,6 +530,49 @@ struct NrgDriver::Impl {
     return row;
   }
 
+  // docalc0 (src/nrg.cc:3063-3070, called from start_run at 3183-3186):
+  // td, annotated energies and singlet expectation values of the initial
+  // cluster from `data`, at N = Ninit-1 (temperature SCALE(Ninit)/betabar,
+  // STAT::set_N at src/nrg.cc:545-553), over all states of the cluster.
+  void calc0() {
+    Step S0;
+    for (const auto& kv : D.energies) {
+      Block b;
+      b.dim = (int)kv.second.size();
+      b.value = kv.second;
+      b.kept = b.dim;
+      S0.blocks[kv.first] = std::move(b);
+    }
+    td_rows.push_back(td(S0, Ninit - 1));
+    const double sc0 = scale_of(P, Ninit);
+    if (P.dumpannotated) {
+      std::vector<std::pair<double, Invar>> l;
+      for (const auto& kv : S0.blocks)
+        for (double x : kv.second.value) l.push_back({x, kv.first});
+      std::sort(l.begin(), l.end());
+      annotated.push_back({sc0, totalenergy, std::move(l)});
+    }
+    std::map<std::string, double> row;
+    if (D.ops.count('s')) {
+      double Zs = 0;
+      for (const auto& kv : S0.blocks)
+        for (double x : kv.second.value) Zs += sym->mult(kv.first) * exp(-P.betabar * x);
+      for (const auto& op : D.ops.at('s')) {
+        double tr = 0;
+        for (const auto& kv : S0.blocks) {
+          auto it = op.second.find({kv.first, kv.first});
+          if (it == op.second.end()) throw std::runtime_error("calc0: singlet operator block missing");
+          const HostMat& M = it->second;
+          double s = 0;
+          for (int r = 0; r < kv.second.dim; ++r) s += exp(-P.betabar * kv.second.value[r]) * M.a[(size_t)r * M.cols + r];
+          tr += sym->mult(kv.first) * s;
+        }
+        row[op.first] = tr / Zs;
+      }
+    }
+    expv_rows.push_back({sc0 / P.betabar, row});
+  }
+
   // ---------------- sweep 1 ----------------
   void sweep1(Slab& persist) {
     std::map<Invar, Prev> prev;
@@ -543,6 +591,7 @@ struct NrgDriver::Impl {
     if (D.ops.count('s'))
       for (const auto& kv : D.ops.at('s')) singlets[kv.first] = upload_blocks(kv.second, *s_slab);
     totalenergy = D.gs_energy;
+    if (P.calc0) calc0();
     Slab hslab(st);
     size_t hcap = 0;
     double* H = nullptr;
@@ -674,7 +723,7 @@ struct NrgDriver::Impl {
         for (const auto& kv : S.blocks)
           for (double x : kv.second.value) l.push_back({x, kv.first});
         std::sort(l.begin(), l.end());
-        annotated.push_back(std::move(l));
+        annotated.push_back({scale1, totalenergy, std::move(l)});
       }
       sections["sweep1 truncate+td"] += secs(ts);
       // operator recalculation
@@ -1159,15 +1208,21 @@ struct NrgDriver::Impl {
     if (!P.dumpannotated) return;
     std::ofstream F(dir + "/annotated.dat");
     F << std::setprecision(P.dumpprecision);
-    for (size_t s = 0; s < annotated.size(); ++s) {
-      const auto& l = annotated[s];
-      const double sc = steps[s].scale;
+    // my_fcmp(x, y, eps) == 0 (src/numerics.h:37-53)
+    auto fcmp = [&](double x, double y) {
+      const double eps = P.grouptol;
+      if (x == 0.0 && y == 0.0) return true;
+      if (fabs(x) < eps && fabs(y) < eps) return true;
+      return fabs(x - y) / (fabs(x) + fabs(y)) < eps;
+    };
+    for (const Annotated& a : annotated) {
+      const auto& l = a.levels;
       size_t len = std::min(l.size(), (size_t)P.dumpannotated);
-      auto fcmp = [&](double a, double b) { return fabs(a - b) < P.grouptol * std::max(fabs(a), fabs(b)) || a == b; };
       for (size_t i = len; i + 1 < l.size() && i > 0; ++i) {
         if (fcmp(l[i].first, l[i - 1].first)) ++len; else break;
       }
-      auto en = [&](double e) { return e * (P.dumpscaled ? 1.0 : sc); };
+      // scaled_energy (src/nrg.cc:2052-2056)
+      auto en = [&](double e) { return e * (P.dumpscaled ? 1.0 : a.scale) + (P.dumpabs ? a.total : 0.0); };
       if (P.dumpgroups) {
         for (size_t i = 0; i < len;) {
           F << en(l[i].first);

@@ -54,6 +54,7 @@ void Params::read(const std::string& path) {
   B("dumpabs", dumpabs); B("dumpgroups", dumpgroups); D("grouptol", grouptol);
   I("width_td", width_td); I("prec_td", prec_td); I("width_custom", width_custom);
   I("prec_custom", prec_custom); I("prec_xy", prec_xy);
+  B("calc0", calc0);
   unused = kv;
   // validateparameters (src/read-input.cc:6-36) and calculate_invariants
   if (keep <= 1) throw std::runtime_error("keep must be > 1");

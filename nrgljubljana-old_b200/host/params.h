@@ -33,6 +33,7 @@ struct Params {
   bool dumpscaled = true, dumpabs = false, dumpgroups = true;
   double grouptol = 1e-6;
   int width_td = 16, prec_td = 10, width_custom = 16, prec_custom = 10, prec_xy = 10;
+  bool calc0 = true;  // td/custom/annotated rows of the initial cluster (src/param.cc:490)
   int channels = 1;  // from the data file
 
   // Parse `path`; unknown keys are kept in `unused` (the reference reports them).

@@ -136,6 +136,11 @@ void EigBatcher::run_batch(Lane& L, const std::vector<Req*>& batch) {
       batch[0]->err = e.what();
       return;
     }
+  } catch (...) {
+    // every request of the batch must be answered: its client waits for it
+    cudaGetLastError();
+    for (Req* r : batch) r->err = "eigensolver lane: unknown exception";
+    return;
   }
   // a merged call failed: solve each run's blocks alone, so that only the
   // run whose blocks fail gets the error
@@ -145,6 +150,9 @@ void EigBatcher::run_batch(Lane& L, const std::vector<Req*>& batch) {
     } catch (const std::exception& e) {
       cudaGetLastError();
       r->err = e.what();
+    } catch (...) {
+      cudaGetLastError();
+      r->err = "eigensolver lane: unknown exception";
     }
   }
 }

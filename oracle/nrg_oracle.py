@@ -63,7 +63,7 @@ DEFAULTS = {
     "dumpannotated": 0, "dumpscaled": True, "dumpabs": False, "dumpprecision": 8,
     "dumpgroups": True, "grouptol": 1e-6,
     "width_td": 16, "prec_td": 10, "width_custom": 16, "prec_custom": 10,
-    "prec_xy": 10, "diagth": 1,
+    "prec_xy": 10, "diagth": 1, "calc0": True,
 }
 
 
@@ -345,6 +345,23 @@ class Spectrum:
 
 def _g(x, prec):
     return "%.*g" % (prec, x)
+
+
+def _cpp_g(x, prec):
+    """An ostream's default float format at setprecision(prec), i.e. %g."""
+    return "%.*g" % (prec, x)
+
+
+def my_fcmp(x, y, eps):
+    """my_fcmp (src/numerics.h:37-53): 0 when x and y agree to the relative
+    tolerance eps (absolute when both are below eps), else the sign of x-y."""
+    if x == 0.0 and y == 0.0:
+        return 0
+    if abs(x) < eps and abs(y) < eps:
+        return 0
+    if abs(x - y) / (abs(x) + abs(y)) < eps:
+        return 0
+    return 1 if x > y else -1
 
 
 def broaden(P, ep, wp, en, wn):
@@ -706,6 +723,8 @@ class Oracle:
         self.annotated = []
         self.expv_rows = []
         self.stats = []
+        if P["calc0"]:
+            self.calc0(ops)
         for N in range(self.Ninit, self.Nmax):
             scale = SCALE(P, N + 1)
             subs = self.subspaces(prev)
@@ -741,7 +760,8 @@ class Oracle:
                 e.absenergy = totalenergy + e.value * scale
             self.td_rows.append(self.td(diag, N))
             if P["dumpannotated"]:
-                self.annotated.append(sorted((float(x), I) for I, e in diag.items() for x in e.value))
+                self.annotated.append((scale, totalenergy,
+                                       sorted((float(x), I) for I, e in diag.items() for x in e.value)))
             rec = StepRecord(eig={I: Eig(value=e.value.copy(), vec=e.vec, shift=e.shift,
                                          absenergy=e.absenergy.copy(), kept=e.kept)
                                   for I, e in diag.items()},
@@ -788,6 +808,30 @@ class Oracle:
         self.GSenergy = totalenergy
         self.last_prev = prev
         self.final_ops = ops
+
+    def calc0(self, ops):
+        """docalc0 (src/nrg.cc:3063-3070, called from start_run at 3183-3186
+        when calc0 is set, the default of src/param.cc:490): thermodynamics,
+        the annotated energies and the singlet expectation values of the
+        initial cluster read from `data`, at N = Ninit - 1, i.e. at the
+        temperature SCALE(Ninit)/betabar (STAT::set_N, src/nrg.cc:545-553).
+        All states of the cluster count (calc_Z, src/nrg.cc:1460-1467)."""
+        P, D = self.P, self.D
+        diag0 = {I: Eig(value=np.asarray(v, dtype=float).copy(), vec=None, kept=len(v))
+                 for I, v in D.energies.items()}
+        self.td_rows.append(self.td(diag0, self.Ninit - 1))
+        if P["dumpannotated"]:
+            self.annotated.append((SCALE(P, self.Ninit), D.gs_energy,
+                                   sorted((float(x), I) for I, e in diag0.items() for x in e.value)))
+        Zs = sum(qs.mult(I) * np.exp(-P["betabar"] * e.value).sum() for I, e in diag0.items())
+        row = {}
+        for name, blocks in ops.get("s", {}).items():
+            tr = 0.0
+            for I, e in diag0.items():
+                nI = np.asarray(blocks[(I, I)])
+                tr += qs.mult(I) * np.sum(np.exp(-P["betabar"] * e.value) * np.diag(nI))
+            row[name] = tr / Zs
+        self.expv_rows.append((SCALE(P, self.Ninit) / P["betabar"], row))
 
     def _needed_d(self, name):
         return any(name in pair.split("-") for pair in self.specd)
@@ -1066,10 +1110,55 @@ class Oracle:
                 fh.write("#" + "".join("%*s " % (wc, n) for n in ["T"] + names) + "\n")
                 for T, row in self.expv_rows:
                     fh.write(" " + "".join("%*s " % (wc, _g(v, pc)) for v in [T] + [row[n] for n in names]) + "\n")
+        if P["dumpannotated"]:
+            self.write_annotated(os.path.join(outdir, "annotated.dat"))
         res = {}
         for sp in getattr(self, "spectra", []):
             res[(sp.kind, sp.spectype, sp.name)] = sp.output(outdir)
         return res
+
+    def write_annotated(self, path):
+        """dump_annotated (src/nrg.cc:2062-2107): per step the lowest
+        `dumpannotated` levels (extended through a cluster within grouptol),
+        grouped by degeneracy with their quantum numbers and total
+        multiplicity, or every level with its quantum numbers when dumpgroups
+        is off; energies in units of omega_N (dumpscaled) and relative to the
+        ground state unless dumpabs (scaled_energy, src/nrg.cc:2052-2056).
+        Steps are separated by an empty line."""
+        P = self.P
+        prec = P["dumpprecision"]
+        gt = P["grouptol"]
+
+        def en(e, scale, total):
+            return e * (1.0 if P["dumpscaled"] else scale) + (total if P["dumpabs"] else 0.0)
+
+        with open(path, "w") as fh:
+            for scale, total, lst in self.annotated:
+                ln = min(len(lst), int(P["dumpannotated"]))
+                i = ln
+                while i < len(lst) - 1 and i > 0:
+                    if my_fcmp(lst[i][0], lst[i - 1][0], gt) == 0:
+                        ln += 1
+                        i += 1
+                    else:
+                        break
+                if P["dumpgroups"]:
+                    i = 0
+                    while i < ln:
+                        i0 = i
+                        qn = []
+                        deg = 0
+                        while i < ln and my_fcmp(lst[i][0], lst[i0][0], gt) == 0:
+                            qn.append("%d %d" % lst[i][1])
+                            deg += qs.mult(lst[i][1])
+                            i += 1
+                        qn.sort()
+                        fh.write(_cpp_g(en(lst[i0][0], scale, total), prec)
+                                 + "".join(" (%s)" % q for q in qn) + " [%d]\n" % deg)
+                else:
+                    for e, I in lst:
+                        fh.write("%s %d %d\n" % (_cpp_g(en(e, scale, total), prec), I[0], I[1]))
+                fh.write("\n")
 
     def run(self, outdir=None):
         import time

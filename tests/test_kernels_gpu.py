@@ -174,3 +174,54 @@ def test_gemm_grouped_large_tiles(ctx):
     for Cc, ref in refs:
         err = (Cc.t() - ref).abs().max().item()
         assert err <= 1e-13 * (ref.abs().max().item() + 1.0) * 50
+
+
+def _sym_torch(n, seed, kind, dev):
+    """Q diag(lam) Q^T in float64 on the device (Q from the QR of a Gaussian
+    matrix, column signs fixed by diag R), as the 40-block benchmark builds
+    its blocks; lam as in _random_sym."""
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    G = torch.randn(n, n, generator=g, dtype=torch.float64).to(dev)
+    Q, R = torch.linalg.qr(G)
+    Q = Q * torch.sign(torch.diagonal(R))
+    rng = np.random.default_rng(seed)
+    if kind == "logspaced":
+        lam = np.logspace(-12, 1, n) * rng.choice([-1.0, 1.0], n)
+    else:
+        lam = np.repeat(rng.standard_normal((n + 3) // 4), 4)[:n]
+    lam_t = torch.tensor(lam, device=dev)
+    A = (Q * lam_t) @ Q.T
+    return (A + A.T) / 2, np.sort(lam)
+
+
+# the block sizes of the workloads: up to 4096 in the 40-block benchmark,
+# about 8000 in the two-channel Kondo run at keep 3000
+@pytest.mark.parametrize("n", [2048, 4096, 8000])
+@pytest.mark.parametrize("kind", ["logspaced", "degenerate"])
+def test_syev_large_blocks(ctx, n, kind):
+    """Eigenvalues against the spectrum the block was built from (whose
+    construction error is ~1e-15 n |lam|max), residual |A Z - Z diag(w)| and
+    orthogonality |Z^T Z - 1| in FP64 on the device, at the same n-scaled
+    1e-13 bounds as the smaller sizes; the batch mixes the large block with
+    small and medium ones so the panel, cluster and warp paths run together."""
+    dev = "cuda:0"
+    A, lam = _sym_torch(n, 100 + n, kind, dev)
+    small = [torch.tensor(_random_sym(m, np.random.default_rng(m), kind), device=dev) for m in (24, 300, 700)]
+    mats = [A] + small
+    ns = [m.shape[0] for m in mats]
+    a_in = [m.t().contiguous() for m in mats]          # column-major copies, overwritten by the solver
+    ws = [torch.empty(k, dtype=torch.float64, device=dev) for k in ns]
+    zs = [torch.empty(k, k, dtype=torch.float64, device=dev) for k in ns]
+    ctx.syev_batched_dev(ns, [x.data_ptr() for x in a_in], [x.data_ptr() for x in ws], [x.data_ptr() for x in zs])
+    torch.cuda.synchronize()
+    for k, (M, w, Zc) in enumerate(zip(mats, ws, zs)):
+        m = M.shape[0]
+        Z = Zc.t()                                       # column r of Z = eigenvector r
+        nrm = max(w.abs().max().item(), 1e-300)
+        assert bool(torch.all(w[1:] >= w[:-1]))
+        ref = lam if k == 0 else np.linalg.eigvalsh(M.cpu().numpy())
+        assert np.max(np.abs(w.cpu().numpy() - ref)) <= 1e-13 * nrm * max(10, m)
+        res = (M @ Z - Z * w).abs().max().item()
+        assert res <= 1e-13 * nrm * max(10, m)
+        orth = (Z.T @ Z - torch.eye(m, dtype=torch.float64, device=dev)).abs().max().item()
+        assert orth <= 1e-13 * max(10, m)

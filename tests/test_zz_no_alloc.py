@@ -34,7 +34,9 @@ def test_noalloc_basis_change_matches_regular_entry_point():
     dev = "cuda:0"
     st = torch.cuda.current_stream().cuda_stream
     g = torch.Generator(device=dev)
-    for call, ns in enumerate(([5, 40, 33, 100, 64], [17, 129, 2, 70, 45, 8])):
+    # the third call comes close to the 32 MiB limit: two intermediates of
+    # 1400 x 1440 doubles (2 x 15.4 MiB) plus the descriptors
+    for call, ns in enumerate(([5, 40, 33, 100, 64], [17, 129, 2, 70, 45, 8], [1400, 1440])):
         g.manual_seed(100 + call)
         nblk = len(ns)
         bra = [k for k in range(nblk) for _ in range(2)]
@@ -52,9 +54,25 @@ def test_noalloc_basis_change_matches_regular_entry_point():
         ctx.eig_recalc_step_dev(ns, [a.data_ptr() for a in A], [w.data_ptr() for w in W],
                                 [z.data_ptr() for z in Z], bra, ket, [o.data_ptr() for o in O],
                                 [r.data_ptr() for r in ref], stream=st)
+        if nblk == 2:
+            bra, ket, O, ref = bra[::2], ket[::2], O[::2], ref[::2]
         new = [torch.full((ns[k], ns[b]), float("nan"), device=dev, dtype=torch.float64) for b, k in zip(bra, ket)]
-        rc = _call(lib, [ns[b] for b in bra], [ns[k] for k in ket], [Z[b].data_ptr() for b in bra],
-                   [Z[k].data_ptr() for k in ket], [o.data_ptr() for o in O], [x.data_ptr() for x in new], st)
+        nb_, nk_ = [ns[b] for b in bra], [ns[k] for k in ket]
+        zb_, zk_ = [Z[b].data_ptr() for b in bra], [Z[k].data_ptr() for k in ket]
+        op_, out_ = [o.data_ptr() for o in O], [x.data_ptr() for x in new]
+        if call == 1:
+            # empty operators (no bra or no ket states) take no GEMM work but
+            # still advance the scratch layout: the operators after them must
+            # come out unchanged
+            spare = torch.zeros(8, device=dev, dtype=torch.float64)
+            for pos, (b0, k0) in ((0, (0, 7)), (3, (6, 0))):
+                nb_.insert(pos, b0)
+                nk_.insert(pos, k0)
+                zb_.insert(pos, spare.data_ptr())
+                zk_.insert(pos, spare.data_ptr())
+                op_.insert(pos, spare.data_ptr())
+                out_.insert(pos, spare.data_ptr())
+        rc = _call(lib, nb_, nk_, zb_, zk_, op_, out_, st)
         assert rc == 0
         torch.cuda.synchronize()
         for r, x in zip(ref, new):
@@ -74,3 +92,31 @@ def test_noalloc_rejects_sizes_beyond_the_static_scratch():
     assert lib.nrgb_basis_change_noalloc(n, (ctypes.c_int * n)(*([1] * n)), (ctypes.c_int * n)(*([1] * n)),
                                          (ctypes.c_void_p * n)(), (ctypes.c_void_p * n)(),
                                          (ctypes.c_void_p * n)(), (ctypes.c_void_p * n)(), None) == 5
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """A call on a stream that is capturing returns 7 before enqueueing
+    anything, and the caller's capture stays valid (the graph still
+    instantiates and replays)."""
+    import nrgb
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+    lib = nrgb.load()
+    dev = "cuda:0"
+    Z = torch.eye(4, device=dev, dtype=torch.float64)
+    O = torch.ones(4, 4, device=dev, dtype=torch.float64)
+    out = torch.zeros(4, 4, device=dev, dtype=torch.float64)
+    x = torch.ones(16, device=dev)
+    # first call outside any capture: the per-device set-up
+    assert _call(lib, [4], [4], [Z.data_ptr()], [Z.data_ptr()], [O.data_ptr()], [out.data_ptr()],
+                 torch.cuda.current_stream().cuda_stream) == 0
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        y = x * 2
+        st = torch.cuda.current_stream().cuda_stream
+        rc = _call(lib, [4], [4], [Z.data_ptr()], [Z.data_ptr()], [O.data_ptr()], [out.data_ptr()], st)
+    assert rc == 7
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.all(y == 2)
