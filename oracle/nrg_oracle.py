@@ -63,7 +63,7 @@ DEFAULTS = {
     "dumpannotated": 0, "dumpscaled": True, "dumpabs": False, "dumpprecision": 8,
     "dumpgroups": True, "grouptol": 1e-6,
     "width_td": 16, "prec_td": 10, "width_custom": 16, "prec_custom": 10,
-    "prec_xy": 10, "diagth": 1, "calc0": True,
+    "prec_xy": 10, "diagth": 1, "calc0": True, "diag": "default", "dsyevrlimit": 100,
 }
 
 
@@ -425,11 +425,19 @@ class StepRecord:
 
 
 class Oracle:
-    def __init__(self, workdir, threads=1, eigh_driver="ev"):
+    def __init__(self, workdir, threads=1, eigh_driver=None):
+        """threads: blocks diagonalised concurrently (OpenMP over blocks,
+        src/nrg.cc:2484-2507), each with one BLAS thread; 1 leaves BLAS its
+        own threads.  eigh_driver: "ev" (dsyev), "evd" or "evr" for every
+        block; None follows the `diag` parameter as the reference does
+        (src/read-input.cc:16-33, src/diag.h:297-311): dsyev by default,
+        dsyevr for blocks of at least `dsyevrlimit` with diag=dsyevr."""
         self.dir = workdir
         self.P = read_params(os.path.join(workdir, "param"))
         self.threads = max(1, int(threads))
         self.eigh_driver = eigh_driver
+        if self.P["diag"] not in ("default", "dsyev", "dsyevr"):
+            raise ValueError("Unknown diagonalization routine: %s" % self.P["diag"])
         self.timing = {}
 
     # -- time bookkeeping (Timing sections of src/nrg.h:135-213) --
@@ -524,7 +532,10 @@ class Oracle:
     def diagonalise(self, h):
         if h.shape[0] == 0:
             return np.zeros(0), np.zeros((0, 0))
-        w, v = sla.eigh(h, driver=self.eigh_driver, check_finite=False)
+        drv = self.eigh_driver
+        if drv is None:
+            drv = "evr" if (self.P["diag"] == "dsyevr" and h.shape[0] >= self.P["dsyevrlimit"]) else "ev"
+        w, v = sla.eigh(h, driver=drv, check_finite=False)
         return w, v
 
     def find_clusters(self, energies):
