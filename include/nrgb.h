@@ -71,6 +71,18 @@ typedef struct {
 int nrgb_gemm_grouped_dev(nrgb_ctx* ctx, int nout, const nrgb_gemm_out* outs, int nterms,
                           const nrgb_gemm_term* terms, void* stream);
 
+/* Split-precision form of nrgb_gemm_grouped_dev (same descriptors): every
+ * product is computed from `slices` (2..8) signed 7-bit slices of each
+ * operand, with power-of-two scales per row of op(A) and per column of op(B),
+ * as exact INT8 tensor-core products (tcgen05 kind::i8, INT32 accumulators)
+ * recombined in FP64 with a compensated sum.  The error of an entry is about
+ * k * 2^-7S * (S + 3) * max|op(A) row| * max|op(B) column|; S = 8 is at the
+ * level of an FP64 product.  Replaces the BLAS gemm of the recalculation
+ * (src/recalc.cc:268-272) and the density matrices (src/dmnrg.h:382-387) in
+ * the split-precision form.  Returns after the work completed. */
+int nrgb_gemm_grouped_split_dev(nrgb_ctx* ctx, int slices, int nout, const nrgb_gemm_out* outs, int nterms,
+                                const nrgb_gemm_term* terms, void* stream);
+
 /* The two hot operations of one NRG step on a batch of blocks, host memory:
  * eigen-decomposition of every block h[b] (n[b] x n[b], column-major,
  * symmetric; not modified) into w[b] (ascending) and eigenvectors Z_b, then
@@ -142,6 +154,19 @@ int nrgb_basis_change_noalloc(int nops, const int* n_bra, const int* n_ket, cons
  * [3] density-matrix seconds, [4] spectral seconds, [5] kernels launched,
  * [6] host->device bytes, [7] device->host bytes. */
 int nrgb_run(nrgb_ctx* ctx, const char* workdir, const char* outdir, double* stats);
+
+/* Failure detection of the device waits.  Every wait of a kernel in this
+ * library is bounded: a grid-barrier wait of the cooperative tridiagonalisation
+ * gives up after 2^poll_log2 polls (default 23, about a second), the launch
+ * ends early, and the call returns status 2 with "grid barrier timed out"
+ * while the context stays usable.  poll_log2 in [4, 30].  No counterpart in
+ * the reference (its LAPACK calls have no waits to bound). */
+int nrgb_set_wait_limit(nrgb_ctx* ctx, int poll_log2);
+/* Host-side fault injection for tests of that path: while `on`, the panel
+ * launches' barriers expect one CTA more than is launched (a CTA that never
+ * arrives), so their waits run out and nrgb_syev_batched / nrgb_run return
+ * the timeout error.  No counterpart in the reference. */
+int nrgb_inject_barrier_shortfall(nrgb_ctx* ctx, int on);
 
 /* Eigensolver structure of nrgb_run and nrgb_eig_recalc_step(_dev) on this
  * context: 0 (default) solves all blocks of a step in one batched call; 1

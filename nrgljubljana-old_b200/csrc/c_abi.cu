@@ -9,6 +9,7 @@
 #include "../../include/nrgb.h"
 #include "common.cuh"
 #include "gemm_f64.cuh"
+#include "gemm_split.cuh"
 #include "syev.cuh"
 #include "../host/driver.h"
 
@@ -138,6 +139,39 @@ int nrgb_syev_batched(nrgb_ctx* ctx, int nblocks, const int* n, double* const* a
       NRGB_CUDA(cudaMemcpyAsync(w[b], d[b].w, n[b] * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
     NRGB_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int nrgb_gemm_grouped_split_dev(nrgb_ctx* ctx, int slices, int nout, const nrgb_gemm_out* outs, int nterms,
+                                const nrgb_gemm_term* terms, void* stream) {
+  if (slices < nrgb::SPLIT_MIN_SLICES || slices > nrgb::SPLIT_MAX_SLICES) return 1;
+  return guarded(ctx, [&] {
+    std::vector<nrgb::GemmProb> P;
+    std::vector<nrgb::GemmSeg> S(nterms);
+    for (int t = 0; t < nterms; ++t) {
+      const nrgb_gemm_term& x = terms[t];
+      S[t] = nrgb::GemmSeg{x.a, x.b, x.lda, x.ldb, x.k, x.trans_a, x.trans_b, x.alpha};
+    }
+    for (int o = 0; o < nout; ++o) {
+      const nrgb_gemm_out& y = outs[o];
+      if (y.m <= 0 || y.n <= 0) continue;
+      if (y.term0 < 0 || y.term0 + y.nterms > nterms) throw nrgb::CudaError("gemm: term range out of bounds");
+      nrgb::GemmProb p{};
+      p.C = y.c;
+      p.ldc = y.ldc;
+      p.m = y.m;
+      p.n = y.n;
+      p.beta = y.beta;
+      p.seg0 = y.term0;
+      p.nseg = y.nterms;
+      P.push_back(p);
+    }
+    if (P.empty()) return;
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->scratch.reserve(nrgb::split_gemm_workspace(P.data(), (int)P.size(), S.data(), slices));
+    ctx->scratch.reset();
+    nrgb::split_gemm_grouped(P.data(), (int)P.size(), S.data(), slices, ctx->scratch, st);
+    if (nrgb::split_gemm_take_error(st)) throw nrgb::CudaError("split gemm: a barrier wait timed out");
   });
 }
 
@@ -322,6 +356,15 @@ int nrgb_run(nrgb_ctx* ctx, const char* workdir, const char* outdir, double* sta
     if (!ctx->driver) ctx->driver.reset(new nrgb::NrgDriver(ctx->stream, solver_of(ctx)));
     ctx->driver->run(workdir, outdir, stats);
   });
+}
+
+int nrgb_set_wait_limit(nrgb_ctx* ctx, int poll_log2) {
+  if (poll_log2 < 4 || poll_log2 > 30) return 1;
+  return guarded(ctx, [&] { ctx->syev->set_wait_limit(poll_log2); });
+}
+
+int nrgb_inject_barrier_shortfall(nrgb_ctx* ctx, int on) {
+  return guarded(ctx, [&] { ctx->syev->inject_barrier_shortfall(on != 0); });
 }
 
 int nrgb_set_eig_mode(nrgb_ctx* ctx, int mode) {

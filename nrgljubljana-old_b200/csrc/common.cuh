@@ -144,13 +144,16 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 // Generation barrier for co-resident CTAs (cooperative launch).  Thread 0
 // of each CTA arrives with a release-acquire atomic and polls the
 // generation with acquire loads and exponential back-off.  Every wait is
-// bounded: after 2^23 polls (about a second) the CTA records an error and
-// continues, and a waiting CTA that sees the error leaves too; once
-// the error is set all later barriers return immediately, so a broken
-// launch ends instead of hanging the GPU.
-__device__ __forceinline__ void grid_barrier(GridBarrier* b, unsigned int nblocks) {
+// bounded: after 2^limit_log2 polls (2^23, about a second, by default) the
+// CTA records an error, and a waiting CTA that sees the error leaves too;
+// once the error is set all later barriers return immediately.  Returns
+// true (in every thread of the CTA) when the error is set, so that the
+// caller can end the launch instead of computing on unsynchronised data.
+__device__ __forceinline__ bool grid_barrier(GridBarrier* b, unsigned int nblocks, int limit_log2 = 23) {
+  __shared__ int s_failed;
   __syncthreads();
   if (threadIdx.x == 0) {
+    const long long limit = 1ll << limit_log2;
     if (*reinterpret_cast<volatile int*>(&b->error) == 0) {
       const unsigned int g = ld_acquire_u32(&b->gen);
       __threadfence();
@@ -164,7 +167,7 @@ __device__ __forceinline__ void grid_barrier(GridBarrier* b, unsigned int nblock
         long long it = 0;
         unsigned ns = 8;
         while (ld_acquire_u32(&b->gen) == g) {
-          if (++it > (1ll << 23) || *reinterpret_cast<volatile int*>(&b->error)) {
+          if (++it > limit || *reinterpret_cast<volatile int*>(&b->error)) {
             atomicExch(&b->error, 1);
             break;
           }
@@ -174,8 +177,10 @@ __device__ __forceinline__ void grid_barrier(GridBarrier* b, unsigned int nblock
       }
       __threadfence();
     }
+    s_failed = *reinterpret_cast<volatile int*>(&b->error);
   }
   __syncthreads();
+  return s_failed != 0;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

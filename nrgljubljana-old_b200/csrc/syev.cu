@@ -252,6 +252,8 @@ struct TrdProb {
   GridBarrier* bar;  // this problem's barrier: only its own CTAs synchronise
   int n;
   int cta0, ncta;
+  int wait_log2;     // a barrier wait gives up after 2^wait_log2 polls
+  int expect_extra;  // CTAs the barriers expect beyond ncta (0; 1 injects a lost CTA)
 };
 
 constexpr int RED = 2 + 2 * NB;
@@ -294,7 +296,7 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
   // Problems are independent: each synchronises only its own CTAs, so a
   // small problem does not wait for a large one inside a panel.
   GridBarrier* bar = P.bar;
-  const unsigned nblocks = (unsigned)P.ncta;
+  const unsigned nblocks = (unsigned)(P.ncta + P.expect_extra);
   const int n = P.n;
   const size_t ld = (size_t)n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -359,7 +361,11 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
       ss = block_sum(ss, scratch);
       if (tid == 0 && ss != 0.0) atomicAdd(&R[0], ss);
     }
-    grid_barrier(bar, nblocks);
+    if (grid_barrier(bar, nblocks, P.wait_log2)) {
+      // a wait gave up: end the launch and report it (the host throws)
+      if (tid == 0) atomicExch(fail, 1);
+      return;
+    }
     // ---------------- phase B ----------------
     if (act && c < n - 1) {
       const double alpha = __ldcg(&P.A[c + 1 + c * ld]);
@@ -433,7 +439,11 @@ __global__ void __launch_bounds__(TRD_NT) trd_panel_kernel(const TrdProb* __rest
       yvp = block_sum(yvp, scratch);
       if (tid == 0 && yvp != 0.0) atomicAdd(&R[1], yvp);
     }
-    grid_barrier(bar, nblocks);
+    if (grid_barrier(bar, nblocks, P.wait_log2)) {
+      // a wait gave up: end the launch and report it (the host throws)
+      if (tid == 0) atomicExch(fail, 1);
+      return;
+    }
   }
   // finish the panel's last column: W[:, NB-1] for the trailing update and v
   // below its subdiagonal
@@ -1807,6 +1817,8 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           for (size_t q = s0; q < s1; ++q) {
             TrdProb t = tp[act[q]];
             t.bar = bars + act[q];
+            t.wait_log2 = wait_log2_;
+            t.expect_extra = inject_shortfall_ ? 1 : 0;
             const double w = pow((double)(t.n - j0), 2.0) / wsum;
             int nc = 1 + (int)floor(w * extra);
             nc = std::min(nc, std::max(1, (t.n - j0) / 8));
@@ -1869,6 +1881,19 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
           }
         }
       }
+    }
+    if (inject_shortfall_) {
+      // fault injection (the barriers expected a CTA that was never
+      // launched): report the timed-out wait here, before any later stage
+      // reads the unfinished reduction, and leave no work of this call in
+      // flight on any stream
+      int f = 0;
+      NRGB_CUDA(cudaMemcpyAsync(&f, d_err_ + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NRGB_CUDA(cudaStreamSynchronize(st));
+      if (small_st_) NRGB_CUDA(cudaStreamSynchronize(small_st_));
+      for (int i = 0; i < NAUX; ++i)
+        if (aux_[i]) NRGB_CUDA(cudaStreamSynchronize(aux_[i]));
+      if (f) throw CudaError("syev: grid barrier timed out");
     }
     // the trailing blocks A[j:, j:] (j = jstop) of the larger blocks, fully
     // updated by the last trailing update, tridiagonalised in clusters

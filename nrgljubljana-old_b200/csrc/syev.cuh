@@ -63,12 +63,21 @@ class SyevBatched : public EigSolver {
   // Largest block the cluster tridiagonalisation holds (0: cluster path off);
   // larger blocks also take the cooperative panel launches.
   int cluster_nmax() const { return cl_nmax_; }
+  // Bound of the grid-barrier waits of the panel launches: 2^poll_log2 polls
+  // (default 23, about a second) before a wait gives up with an error.
+  void set_wait_limit(int poll_log2) { wait_log2_ = poll_log2; }
+  // Host-side fault injection: while on, every panel launch's barriers
+  // expect one CTA more than is launched (a lost CTA), so each wait must
+  // run out; run() then throws "grid barrier timed out".
+  void inject_barrier_shortfall(bool on) { inject_shortfall_ = on; }
 
  private:
   DeviceArena arena_;
   int* d_err_ = nullptr;
   GridBarrier* d_bar_ = nullptr;
   int launches_ = 0;
+  int wait_log2_ = 23;
+  bool inject_shortfall_ = false;
   int coop_ctas_ = 0;
   int sms_ = 0;
   int cl_max_[5] = {0, 0, 0, 0, 0};  // resident clusters of 1, 2, 4, 8, 16 CTAs (0: not usable)

@@ -37,6 +37,7 @@
 
 #include "../csrc/common.cuh"
 #include "../csrc/gemm_f64.cuh"
+#include "../csrc/gemm_split.cuh"
 #include "../csrc/nrg_kernels.cuh"
 #include "../csrc/syev.cuh"
 #include "data.h"
@@ -253,8 +254,19 @@ struct NrgDriver::Impl {
     NRGB_CUDA(cudaStreamSynchronize(st));
     desc.reset();
   }
+  DeviceArena split_ws;  // operand slices of the split-precision products
   void run_gemm(const Grouped& g) {
     if (g.probs.empty()) return;
+    if (P.gemm_slices > 0) {
+      // split precision: INT8 slices on the tensor cores (the launches of
+      // one stream run in order, so the workspace is reused call to call)
+      split_ws.reserve(split_gemm_workspace(g.probs.data(), (int)g.probs.size(), g.segs.data(), P.gemm_slices));
+      split_ws.reset();
+      split_gemm_grouped(g.probs.data(), (int)g.probs.size(), g.segs.data(), P.gemm_slices, split_ws, st,
+                         "gemm_i8_nrg");
+      launches += 3;
+      return;
+    }
     GemmProb* dp = upload(g.probs);
     GemmSeg* ds = upload(g.segs);
     KernelStats::get().add_work("gemm_f64_nrg", gemm_flops(g.probs.data(), (int)g.probs.size(), g.segs.data()));
@@ -703,6 +715,15 @@ struct NrgDriver::Impl {
       find_clusters(sorted_energies(S));
       if (fix_splittings(S)) find_clusters(sorted_energies(S));
       truncate_prepare(S, N, false);
+      if (getenv("NRGB_LOG")) {
+        // the reference's per-step log line (src/nrg.cc:3010-3013), to stderr
+        size_t nk = 0, na = 0;
+        for (const auto& kv : S.blocks) {
+          nk += kv.second.kept;
+          na += kv.second.dim;
+        }
+        fprintf(stderr, "N=%d Egs=%.17g Kept: %zu out of %zu\n", N, Egs, nk, na);
+      }
       {
         // the fixed values replace the eigenvalues on the device (one copy);
         // the staging vector lives until the copy has completed (the next
@@ -1405,6 +1426,8 @@ struct NrgDriver::Impl {
       Section x(this, "sweep2 (all)");
       sweep2(persist);
     }
+    if (P.gemm_slices > 0 && split_gemm_take_error(st))
+      throw CudaError("split-precision products: a barrier wait timed out");
     sec.reset(new Section(this, "write output"));
     write_td(od);
     write_custom(od);

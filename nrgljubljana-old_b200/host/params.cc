@@ -55,9 +55,12 @@ void Params::read(const std::string& path) {
   I("width_td", width_td); I("prec_td", prec_td); I("width_custom", width_custom);
   I("prec_custom", prec_custom); I("prec_xy", prec_xy);
   B("calc0", calc0);
+  I("gemm_slices", gemm_slices);
   unused = kv;
   // validateparameters (src/read-input.cc:6-36) and calculate_invariants
   if (keep <= 1) throw std::runtime_error("keep must be > 1");
+  if (gemm_slices != 0 && (gemm_slices < 2 || gemm_slices > 8))
+    throw std::runtime_error("gemm_slices must be 0 (FP64) or in [2, 8]");
   if (Lambda <= 1.0) throw std::runtime_error("Lambda must be > 1");
   if (dmnrg || fdm || cfs) dm = true;
   if ((fdm || cfs) && !lastalloverride) lastall = true;

@@ -34,6 +34,11 @@ struct Params {
   double grouptol = 1e-6;
   int width_td = 16, prec_td = 10, width_custom = 16, prec_custom = 10, prec_xy = 10;
   bool calc0 = true;  // td/custom/annotated rows of the initial cluster (src/param.cc:490)
+  // Products of the recalculation, density matrices and spectral weights:
+  // 0 = FP64 on the FP64 tensor pipe; 2..8 = split precision with this many
+  // INT8 slices per operand (this implementation's key; the reference has
+  // no such parameter and reports it as unknown).
+  int gemm_slices = 0;
   int channels = 1;  // from the data file
 
   // Parse `path`; unknown keys are kept in `unused` (the reference reports them).

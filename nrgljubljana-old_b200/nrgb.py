@@ -12,10 +12,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libnrgb.so")
 
 EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
-           "nrgb_syev_batched", "nrgb_syev_batched_dev", "nrgb_gemm_grouped_dev",
+           "nrgb_syev_batched", "nrgb_syev_batched_dev", "nrgb_gemm_grouped_dev", "nrgb_gemm_grouped_split_dev",
            "nrgb_eig_recalc_step", "nrgb_eig_recalc_step_dev", "nrgb_profile", "nrgb_profile_only", "nrgb_kernel_stats",
            "nrgb_kernel_work",
            "nrgb_basis_change_noalloc", "nrgb_run", "nrgb_set_eig_mode",
+           "nrgb_set_wait_limit", "nrgb_inject_barrier_shortfall",
            "nrgb_server_create", "nrgb_server_submit", "nrgb_server_wait", "nrgb_server_error",
            "nrgb_server_counters", "nrgb_server_destroy", "nrgb_project_bytes"]
 
@@ -50,8 +51,12 @@ def load(path: str = LIBPATH):
     lib.nrgb_syev_batched.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp)]
     lib.nrgb_syev_batched_dev.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp]
     lib.nrgb_gemm_grouped_dev.argtypes = [vp, C.c_int, C.POINTER(GemmOut), C.c_int, C.POINTER(GemmTerm), vp]
+    lib.nrgb_gemm_grouped_split_dev.argtypes = [vp, C.c_int, C.c_int, C.POINTER(GemmOut), C.c_int,
+                                                C.POINTER(GemmTerm), vp]
     lib.nrgb_run.argtypes = [vp, C.c_char_p, C.c_char_p, dp]
     lib.nrgb_set_eig_mode.argtypes = [vp, C.c_int]
+    lib.nrgb_set_wait_limit.argtypes = [vp, C.c_int]
+    lib.nrgb_inject_barrier_shortfall.argtypes = [vp, C.c_int]
     lib.nrgb_eig_recalc_step.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                          C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp)]
     lib.nrgb_eig_recalc_step_dev.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
@@ -125,6 +130,13 @@ class Context:
         self._check(self.lib.nrgb_gemm_grouped_dev(self.h, len(outs), o, len(terms), t, C.c_void_p(stream)),
                     "nrgb_gemm_grouped_dev")
 
+    def gemm_grouped_split_dev(self, slices, outs, terms, stream=0):
+        """Split-precision (INT8 slices, tensor cores) form of gemm_grouped_dev."""
+        o = (GemmOut * len(outs))(*outs)
+        t = (GemmTerm * len(terms))(*terms)
+        self._check(self.lib.nrgb_gemm_grouped_split_dev(self.h, slices, len(outs), o, len(terms), t,
+                                                         C.c_void_p(stream)), "nrgb_gemm_grouped_split_dev")
+
     @staticmethod
     def _ptrs(xs):
         return (C.c_void_p * len(xs))(*[int(x) if x is not None else None for x in xs])
@@ -168,6 +180,15 @@ class Context:
     def set_eig_mode(self, mode: int):
         """0: one batched eigensolver call per step; 1: one call per block."""
         self._check(self.lib.nrgb_set_eig_mode(self.h, mode), "nrgb_set_eig_mode")
+
+    def set_wait_limit(self, poll_log2: int):
+        """Device barrier waits give up after 2**poll_log2 polls (default 23)."""
+        self._check(self.lib.nrgb_set_wait_limit(self.h, poll_log2), "nrgb_set_wait_limit")
+
+    def inject_barrier_shortfall(self, on: bool):
+        """Fault injection: panel launches wait for a CTA that never arrives."""
+        self._check(self.lib.nrgb_inject_barrier_shortfall(self.h, 1 if on else 0),
+                    "nrgb_inject_barrier_shortfall")
 
     def run(self, workdir: str, outdir: str):
         stats = (C.c_double * 8)()

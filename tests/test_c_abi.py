@@ -35,3 +35,11 @@ def test_create_without_device_fails_cleanly():
     lib = nrgb.load()
     h = ctypes.c_void_p()
     assert lib.nrgb_create(0, ctypes.byref(h)) != 0
+
+
+def test_wait_limit_arguments_are_checked_without_a_device():
+    lib = nrgb.load()
+    assert lib.nrgb_set_wait_limit(None, 3) == 1      # below the allowed range
+    assert lib.nrgb_set_wait_limit(None, 31) == 1     # above it
+    assert lib.nrgb_set_wait_limit(None, 16) == 1     # null context
+    assert lib.nrgb_inject_barrier_shortfall(None, 1) == 1
