@@ -155,6 +155,26 @@ int nrgb_basis_change_noalloc(int nops, const int* n_bra, const int* n_ket, cons
  * [6] host->device bytes, [7] device->host bytes. */
 int nrgb_run(nrgb_ctx* ctx, const char* workdir, const char* outdir, double* stats);
 
+/* Size-bucketed schedule of the batched step, one table per device shared
+ * by every context of the process (no counterpart in the reference, whose
+ * only schedule is a sort of the blocks by size, src/nrg.cc:2785-2803):
+ *   cluster_limit    blocks up to this size are tridiagonalised whole in one
+ *                    thread-block cluster, larger ones take cooperative
+ *                    panel launches until their trailing block is this small
+ *                    (0 = the cluster kernel's capacity);
+ *   gemm_large_from  grouped FP64 GEMM launches whose problems average at
+ *                    least this output edge use 128 x 128 tiles (0 = never).
+ * nrgb_autotune measures both choices on the device (a few seconds of
+ * synthetic work: square GEMMs of edge 128..2048 with both tile sizes, one
+ * batched eigensolve of a mix of block sizes under several limits), sets the
+ * table and writes a JSON report of the timings and choices into `report`
+ * (report_len bytes, NUL-terminated, may be NULL).  nrgb_set_schedule sets
+ * the table directly (e.g. to replay a tuned schedule); nrgb_get_schedule
+ * reads it and the cluster kernel's capacity. */
+int nrgb_autotune(nrgb_ctx* ctx, char* report, int report_len);
+int nrgb_set_schedule(nrgb_ctx* ctx, int cluster_limit, int gemm_large_from);
+int nrgb_get_schedule(nrgb_ctx* ctx, int* cluster_limit, int* gemm_large_from, int* cluster_capacity);
+
 /* Failure detection of the device waits.  Every wait of a kernel in this
  * library is bounded: a grid-barrier wait of the cooperative tridiagonalisation
  * gives up after 2^poll_log2 polls (default 23, about a second), the launch

@@ -1,7 +1,9 @@
 // C ABI of libnrgb.so (declarations and the reference seams they replace are
 // in include/nrgb.h).
 #include <cuda_runtime.h>
+#include <string.h>
 
+#include <algorithm>
 #include <memory>
 #include <string>
 #include <vector>
@@ -9,7 +11,9 @@
 #include "../../include/nrgb.h"
 #include "common.cuh"
 #include "gemm_f64.cuh"
+#include "autotune.cuh"
 #include "gemm_split.cuh"
+#include "schedule.cuh"
 #include "syev.cuh"
 #include "../host/driver.h"
 
@@ -355,6 +359,35 @@ int nrgb_run(nrgb_ctx* ctx, const char* workdir, const char* outdir, double* sta
   return guarded(ctx, [&] {
     if (!ctx->driver) ctx->driver.reset(new nrgb::NrgDriver(ctx->stream, solver_of(ctx)));
     ctx->driver->run(workdir, outdir, stats);
+  });
+}
+
+int nrgb_autotune(nrgb_ctx* ctx, char* report, int report_len) {
+  return guarded(ctx, [&] {
+    const std::string r = nrgb::autotune(*ctx->syev, ctx->syev->cluster_capacity(), ctx->stream);
+    if (report && report_len > 0) {
+      const size_t n = std::min((size_t)report_len - 1, r.size());
+      memcpy(report, r.data(), n);
+      report[n] = 0;
+    }
+  });
+}
+
+int nrgb_set_schedule(nrgb_ctx* ctx, int cluster_limit, int gemm_large_from) {
+  if (cluster_limit < 0 || gemm_large_from < 0) return 1;
+  return guarded(ctx, [&] {
+    nrgb::Schedule& s = nrgb::schedule_of(ctx->device);
+    s.cluster_limit.store(cluster_limit);
+    s.gemm_large_from.store(gemm_large_from);
+  });
+}
+
+int nrgb_get_schedule(nrgb_ctx* ctx, int* cluster_limit, int* gemm_large_from, int* cluster_capacity) {
+  return guarded(ctx, [&] {
+    const nrgb::Schedule& s = nrgb::schedule_of(ctx->device);
+    if (cluster_limit) *cluster_limit = s.cluster_limit.load();
+    if (gemm_large_from) *gemm_large_from = s.gemm_large_from.load();
+    if (cluster_capacity) *cluster_capacity = ctx->syev->cluster_capacity();
   });
 }
 

@@ -8,6 +8,7 @@
 #include <atomic>
 #include "common.cuh"
 #include "gemm_f64.cuh"
+#include "schedule.cuh"
 
 namespace nrgb {
 
@@ -378,10 +379,10 @@ __global__ void __launch_bounds__(LNT) gemm_grouped_large_kernel(const GemmProb*
 }
 
 constexpr size_t LSMEM = 2 * (size_t)LSTAGES * BK * LLDS * sizeof(double);
-// Measured on B200: the 128x128 cp.async variant reaches 21-25 TF/s against
-// 25-28 TF/s for the 64x64 register-staged kernel on the same shapes, so it
-// is not selected.
-constexpr bool kUseLargeTiles = false;
+// The 128x128 cp.async variant is used only where the device's schedule
+// (schedule.cuh, set by the autotuner's measurements) says it wins: by
+// default never (measured on B200 at first: 21-25 TF/s against 25-28 TF/s
+// for the 64x64 register-staged kernel on the same shapes).
 
 }  // namespace
 
@@ -406,9 +407,13 @@ double gemm_flops(const GemmProb* probs, int nprob, const GemmSeg* segs) {
 cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs,
                                 int total_tiles, cudaStream_t stream, const char* tag, int total_stiles) {
   if (total_tiles <= 0 || nprob <= 0) return cudaSuccess;
-  // 128x128 tiles when they cover at most 30% more area than the 64x64 ones
-  // and still give enough CTAs to fill the GPU
-  if (kUseLargeTiles && total_stiles > 0 && 4.0 * total_stiles <= 1.3 * total_tiles && total_stiles >= 120) {
+  // 128x128 tiles when the schedule selects them for this problem size,
+  // they cover at most 30% more area than the 64x64 ones and they still give
+  // enough CTAs to fill the GPU
+  const int large_from = schedule_here().gemm_large_from.load(std::memory_order_relaxed);
+  const double edge = GEMM_BM * sqrt((double)total_tiles / nprob);  // mean output edge per problem
+  if (large_from > 0 && edge >= large_from && total_stiles > 0 && 4.0 * total_stiles <= 1.3 * total_tiles &&
+      total_stiles >= 120) {
     // once per device (function attributes belong to the device's context);
     // every caller sets the same value, so threads that race here agree
     static std::atomic<bool> attr[64];

@@ -25,6 +25,7 @@
 
 #include "gemm_f64.cuh"
 #include "syev.cuh"
+#include "schedule.cuh"
 
 namespace nrgb {
 
@@ -1587,6 +1588,11 @@ size_t SyevBatched::workspace_bytes(const std::vector<int>& ns) {
   return pl.bytes + (size_t)ns.size() * 4096 + (1 << 20);
 }
 
+int SyevBatched::cl_use() const {
+  const int lim = schedule_here().cluster_limit.load(std::memory_order_relaxed);
+  return (lim > 0 && lim < cl_nmax_) ? lim : cl_nmax_;
+}
+
 void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
   launches_ = 0;
   NRGB_CUDA(cudaMemsetAsync(d_err_, 0, 4 * sizeof(int), st));
@@ -1772,16 +1778,17 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     // Larger blocks: panel launches for their leading columns until the
     // trailing block fits a cluster, whose tridiagonalisation finishes it.
     std::vector<int> jstop(nbig);
+    const int clim = cl_use();
     {
       std::vector<TrdClProb> whole;
       for (int b = 0; b < nbig; ++b) {
         const int n = tp[b].n;
         jstop[b] = n;
-        if (cl_nmax_ > 0 && n <= cl_nmax_) {
+        if (clim > 0 && n <= clim) {
           whole.push_back(TrdClProb{tp[b].A, tp[b].d, tp[b].e, tp[b].tau, n, n});
           via_cluster[b] = 1;
-        } else if (cl_nmax_ > 0) {
-          jstop[b] = ((n - cl_nmax_ + NB - 1) / NB) * NB;
+        } else if (clim > 0) {
+          jstop[b] = ((n - clim + NB - 1) / NB) * NB;
         }
       }
       launch_clusters(whole);

@@ -62,7 +62,9 @@ class SyevBatched : public EigSolver {
   int last_launches() const { return launches_; }
   // Largest block the cluster tridiagonalisation holds (0: cluster path off);
   // larger blocks also take the cooperative panel launches.
-  int cluster_nmax() const { return cl_nmax_; }
+  int cluster_nmax() const { return cl_use(); }
+  // The cluster kernel's capacity, before the schedule's limit.
+  int cluster_capacity() const { return cl_nmax_; }
   // Bound of the grid-barrier waits of the panel launches: 2^poll_log2 polls
   // (default 23, about a second) before a wait gives up with an error.
   void set_wait_limit(int poll_log2) { wait_log2_ = poll_log2; }
@@ -83,6 +85,9 @@ class SyevBatched : public EigSolver {
   int cl_max_[5] = {0, 0, 0, 0, 0};  // resident clusters of 1, 2, 4, 8, 16 CTAs (0: not usable)
   size_t cl_smem_ = 0;                // shared memory per CTA of the cluster kernel
   int cl_nmax_ = 0;                   // largest block it holds (0: cluster path off)
+  // blocks up to this size go to the cluster kernel whole: the capacity, or
+  // the schedule's limit when it is lower (schedule.cuh)
+  int cl_use() const;
   // side streams on which the cluster launches of different sizes overlap
   static constexpr int NAUX = 6;
   cudaStream_t aux_[NAUX] = {};

@@ -40,6 +40,7 @@
 #include "../csrc/gemm_split.cuh"
 #include "../csrc/nrg_kernels.cuh"
 #include "../csrc/syev.cuh"
+#include "../csrc/truncate.cuh"
 #include "data.h"
 #include "params.h"
 #include "symmetry.h"
@@ -127,7 +128,20 @@ struct Block {
 struct Step {
   std::map<Invar, Block> blocks;
   double Egs = 0.0, scale = 0.0;
+  double total = 0.0;       // total energy after this step
+  double* wall = nullptr;   // the blocks' eigenvalues back to back (device)
+  int wtot = 0;
   std::unique_ptr<Slab> slab;
+};
+
+// Singlet expectation values of one step, gathered on the device and
+// evaluated once the step's eigenvalues are on the host.
+struct ExpvDeferred {
+  size_t step;
+  double T;
+  const double* diag = nullptr;  // gathered diagonals (device)
+  std::vector<std::pair<std::string, Invar>> order;
+  std::vector<int> len;
 };
 
 struct Prev {
@@ -185,7 +199,6 @@ struct NrgDriver::Impl {
   std::unique_ptr<Symmetry> sym;
   int Nmax = 0, Ninit = 0;
   std::vector<Step> steps;
-  std::map<double, double> cluster_map;  // persists across steps and sweeps (src/splitting.cc)
   double totalenergy = 0.0, GSenergy = 0.0;
   std::vector<std::vector<double>> td_rows;
   std::vector<std::pair<double, std::map<std::string, double>>> expv_rows;
@@ -212,16 +225,69 @@ struct NrgDriver::Impl {
   DeviceArena desc;
   size_t desc_off = 0;
 
+  // device truncation: splitting map, step workspace, the per-step record
+  TruncState tstate;
+  void* twork = nullptr;
+  size_t twork_bytes = 0;
+  void* tail_dev = nullptr;
+  size_t tail_dev_bytes = 0;
+  char* tail_pin = nullptr;
+  size_t tail_pin_bytes = 0;
+  std::vector<ExpvDeferred> expv_def;
+  std::unique_ptr<Slab> expv_slab;
+  void free_trunc() {
+    for (int i = 0; i < 2; ++i) {
+      if (tstate.map_k[i]) cudaFreeAsync(tstate.map_k[i], st);
+      if (tstate.map_v[i]) cudaFreeAsync(tstate.map_v[i], st);
+      tstate.map_k[i] = tstate.map_v[i] = nullptr;
+    }
+    if (tstate.d_count) cudaFreeAsync(tstate.d_count, st);
+    tstate = TruncState();
+    if (twork) cudaFreeAsync(twork, st);
+    twork = nullptr;
+    twork_bytes = 0;
+    if (tail_dev) cudaFreeAsync(tail_dev, st);
+    tail_dev = nullptr;
+    tail_dev_bytes = 0;
+  }
+  // Map buffers that hold `need` entries (the current map is copied over).
+  void ensure_map(int need) {
+    if (need <= tstate.map_cap) return;
+    int cap = std::max(4096, tstate.map_cap);
+    while (cap < need) cap *= 2;
+    double *nk[2], *nv[2];
+    for (int i = 0; i < 2; ++i) {
+      NRGB_CUDA(cudaMallocAsync((void**)&nk[i], sizeof(double) * cap, st));
+      NRGB_CUDA(cudaMallocAsync((void**)&nv[i], sizeof(double) * cap, st));
+    }
+    if (!tstate.d_count) {
+      NRGB_CUDA(cudaMallocAsync((void**)&tstate.d_count, sizeof(int), st));
+      NRGB_CUDA(cudaMemsetAsync(tstate.d_count, 0, sizeof(int), st));
+    }
+    const int c = tstate.cur;
+    if (tstate.map_count > 0) {
+      NRGB_CUDA(cudaMemcpyAsync(nk[c], tstate.map_k[c], sizeof(double) * tstate.map_count, cudaMemcpyDeviceToDevice, st));
+      NRGB_CUDA(cudaMemcpyAsync(nv[c], tstate.map_v[c], sizeof(double) * tstate.map_count, cudaMemcpyDeviceToDevice, st));
+    }
+    for (int i = 0; i < 2; ++i) {
+      if (tstate.map_k[i]) cudaFreeAsync(tstate.map_k[i], st);
+      if (tstate.map_v[i]) cudaFreeAsync(tstate.map_v[i], st);
+      tstate.map_k[i] = nk[i];
+      tstate.map_v[i] = nv[i];
+    }
+    tstate.map_cap = cap;
+  }
+
   MemCount mem;
   double eig_calls = 0;
   std::vector<double> wstage;  // host staging of per-step eigenvalue uploads
 
   Impl(cudaStream_t s, EigSolver* e) : st(s), syev(e) {}
   ~Impl() {
-    if (desc_pin) {
-      cudaStreamSynchronize(st);
-      cudaFreeHost(desc_pin);
-    }
+    free_trunc();
+    cudaStreamSynchronize(st);
+    if (desc_pin) cudaFreeHost(desc_pin);
+    if (tail_pin) cudaFreeHost(tail_pin);
   }
   Impl(const Impl&) = delete;
   Impl& operator=(const Impl&) = delete;
@@ -440,81 +506,6 @@ struct NrgDriver::Impl {
     return compute_targets(tg, slab);
   }
 
-  // ---------------- truncation bookkeeping (host) ----------------
-  void find_clusters(const std::vector<double>& e) {
-    // src/splitting.cc:45-77, with its conventions: the last cluster is not
-    // processed and the mapping persists for the rest of the run.
-    if (e.empty()) return;
-    double e0 = e[0];
-    size_t i0 = 0;
-    int csize = 1;
-    for (size_t i = 0; i < e.size(); ++i) {
-      if (e[i] - e0 < P.fixeps) {
-        ++csize;
-      } else {
-        if (csize > 1) {
-          bool split = false;
-          for (size_t k = i0 + 1; k < i && !split; ++k) split = e[k] != e[i0];
-          if (split)
-            for (size_t k = i0 + 1; k < i; ++k)
-              if (e[k] != e[i0]) cluster_map.emplace(e[k], e[i0]);
-        }
-        e0 = e[i];
-        i0 = i;
-        csize = 1;
-      }
-    }
-  }
-  bool fix_splittings(Step& S) {
-    bool changed = false;
-    if (cluster_map.empty()) return false;
-    for (auto& kv : S.blocks)
-      for (double& x : kv.second.value) {
-        auto it = cluster_map.find(x);
-        if (it != cluster_map.end()) {
-          x = it->second;
-          changed = true;
-        }
-      }
-    return changed;
-  }
-  std::vector<double> sorted_energies(const Step& S) {
-    std::vector<double> e;
-    for (const auto& kv : S.blocks) e.insert(e.end(), kv.second.value.begin(), kv.second.value.end());
-    std::sort(e.begin(), e.end());
-    return e;
-  }
-  double highest_retained_energy(const std::vector<double>& e) {
-    if (e.front() != 0.0) throw std::runtime_error("truncation: ground state not at zero");
-    const size_t total = e.size();
-    size_t nrkeep;
-    if (P.keepenergy <= 0.0) {
-      nrkeep = P.keep;
-    } else {
-      nrkeep = 1 + std::count_if(e.begin(), e.end(), [&](double x) { return x <= P.keepenergy; });
-      nrkeep = std::min(std::max(nrkeep, (size_t)P.keepmin), (size_t)P.keep);
-    }
-    if (P.safeguard > 0.0) {
-      int extra = 0;
-      while (nrkeep < total && e[nrkeep] - e[nrkeep - 1] <= P.safeguard && extra < P.safeguardmax) {
-        ++nrkeep;
-        ++extra;
-      }
-    }
-    nrkeep = std::min(std::max(nrkeep, (size_t)1), total);
-    return e[nrkeep - 1];
-  }
-  void truncate_prepare(Step& S, int N, bool dmnrg_run) {
-    const double Emax = highest_retained_energy(sorted_energies(S));
-    for (auto& kv : S.blocks) {
-      Block& b = kv.second;
-      int cnt = (int)std::count_if(b.value.begin(), b.value.end(), [&](double x) { return x <= Emax; });
-      if (cfs_flags() && last(N) && !P.lastalloverride) cnt = (int)b.value.size();
-      if (dmnrg_run && last(N) && P.lastall) cnt = (int)b.value.size();
-      b.kept = cnt;
-    }
-  }
-
   std::vector<double> td(const Step& S, int N) {
     const double f = P.betabar;
     double Z = 0, E = 0, E2 = 0;
@@ -583,6 +574,90 @@ struct NrgDriver::Impl {
       }
     }
     expv_rows.push_back({sc0 / P.betabar, row});
+  }
+
+  // nrg_calculate_TD (src/nrg.cc:2333-2369) from the per-block sums of
+  // e^-bE, bE e^-bE and (bE)^2 e^-bE computed on the device
+  std::vector<double> td_sums(const Step& S, int N, const double* sums) {
+    double Z = 0, E = 0, E2 = 0;
+    std::vector<std::pair<Invar, double>> zs;
+    size_t b = 0;
+    for (const auto& kv : S.blocks) {
+      const int m = sym->mult(kv.first);
+      Z += m * sums[3 * b];
+      E += m * sums[3 * b + 1];
+      E2 += m * sums[3 * b + 2];
+      zs.push_back({kv.first, sums[3 * b]});
+      ++b;
+    }
+    E /= Z;
+    E2 /= Z;
+    const double C = E2 - E * E, F = -log(Z), Sent = E - F;
+    std::vector<double> row = {scale_of(P, N + 1) / P.betabar};
+    for (double v : sym->td_values_sums(zs, Z)) row.push_back(v);
+    for (double v : {E, E2, C, F, Sent}) row.push_back(v);
+    return row;
+  }
+
+  // The eigenvalues of every step of sweep 1 to the host, once the sweep
+  // is done (one copy per step, one synchronisation): absolute energies,
+  // the energy flow and the deferred expectation values.
+  void finish_sweep1() {
+    std::vector<std::vector<double>> hv(steps.size());
+    for (size_t k = 0; k < steps.size(); ++k) {
+      hv[k].resize(steps[k].wtot);
+      NRGB_CUDA(cudaMemcpyAsync(hv[k].data(), steps[k].wall, steps[k].wtot * sizeof(double), cudaMemcpyDeviceToHost, st));
+      d2h += steps[k].wtot * sizeof(double);
+    }
+    std::vector<std::vector<double>> hd(expv_def.size());
+    for (size_t k = 0; k < expv_def.size(); ++k) {
+      size_t n = 0;
+      for (int l : expv_def[k].len) n += l;
+      hd[k].resize(n);
+      if (n) {
+        NRGB_CUDA(cudaMemcpyAsync(hd[k].data(), expv_def[k].diag, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        d2h += n * sizeof(double);
+      }
+    }
+    NRGB_CUDA(cudaStreamSynchronize(st));
+    for (size_t k = 0; k < steps.size(); ++k) {
+      Step& S = steps[k];
+      size_t o = 0;
+      for (auto& kv : S.blocks) {
+        Block& b = kv.second;
+        b.value.assign(hv[k].begin() + o, hv[k].begin() + o + b.dim);
+        o += b.dim;
+        b.absE.resize(b.dim);
+        for (int r = 0; r < b.dim; ++r) b.absE[r] = S.total + b.value[r] * S.scale;
+      }
+      if (P.dumpannotated) {
+        std::vector<std::pair<double, Invar>> l;
+        for (const auto& kv : S.blocks)
+          for (double x : kv.second.value) l.push_back({x, kv.first});
+        std::sort(l.begin(), l.end());
+        annotated.push_back({S.scale, S.total, std::move(l)});
+      }
+    }
+    // expectation values of singlet operators (nrg_measure_singlet, src/nrg.cc:2226-2236)
+    for (size_t k = 0; k < expv_def.size(); ++k) {
+      const ExpvDeferred& x = expv_def[k];
+      const Step& S = steps[x.step];
+      std::map<std::string, double> row;
+      double Zs = 0;
+      for (const auto& kv : S.blocks)
+        for (int r = 0; r < kv.second.kept; ++r) Zs += sym->mult(kv.first) * exp(-P.betabar * kv.second.value[r]);
+      size_t p = 0;
+      for (size_t j = 0; j < x.order.size(); ++j) {
+        const Block& b = S.blocks.at(x.order[j].second);
+        double sv = 0;
+        for (int r = 0; r < x.len[j]; ++r) sv += exp(-P.betabar * b.value[r]) * hd[k][p + r];
+        row[x.order[j].first] += sym->mult(x.order[j].second) * sv;
+        p += x.len[j];
+      }
+      for (auto& kv : row) kv.second /= Zs;
+      expv_rows.push_back({x.T, row});
+    }
+    expv_def.clear();
   }
 
   // ---------------- sweep 1 ----------------
@@ -696,55 +771,69 @@ struct NrgDriver::Impl {
       t_diag += secs(t0);
       sections["sweep1 diag"] += secs(t0);
       ts = Clock::now();
-      // eigenvalues to the host: ground state, clusters, truncation
+      // truncation on the device: ground state, splitting correction,
+      // retained states, thermodynamics sums; one small record comes back
       {
-        const std::vector<double> wh = download(wall, wtot);
-        size_t o = 0;
-        for (auto& kv : S.blocks) {
-          kv.second.value.assign(wh.begin() + o, wh.begin() + o + kv.second.dim);
+        const int nb = (int)S.blocks.size();
+        std::vector<TruncBlock> tb;
+        int o = 0;
+        for (const auto& kv : S.blocks) {
+          tb.push_back(TruncBlock{kv.second.w, kv.second.dim, o});
           o += kv.second.dim;
         }
-      }
-      double Egs = 1e300;
-      for (const auto& kv : S.blocks) Egs = std::min(Egs, kv.second.value[0] + kv.second.shift);
-      for (auto& kv : S.blocks) {
-        for (double& x : kv.second.value) x -= Egs;
-        kv.second.shift = Egs;
-      }
-      S.Egs = Egs;
-      find_clusters(sorted_energies(S));
-      if (fix_splittings(S)) find_clusters(sorted_energies(S));
-      truncate_prepare(S, N, false);
-      if (getenv("NRGB_LOG")) {
-        // the reference's per-step log line (src/nrg.cc:3010-3013), to stderr
-        size_t nk = 0, na = 0;
-        for (const auto& kv : S.blocks) {
-          nk += kv.second.kept;
-          na += kv.second.dim;
+        ensure_map(tstate.map_count + 2 * (int)wtot + 16);
+        const size_t wb = trunc_work_bytes((int)wtot, nb);
+        if (wb > twork_bytes) {
+          if (twork) NRGB_CUDA(cudaFreeAsync(twork, st));
+          twork_bytes = wb + wb / 2;
+          NRGB_CUDA(cudaMallocAsync(&twork, twork_bytes, st));
         }
-        fprintf(stderr, "N=%d Egs=%.17g Kept: %zu out of %zu\n", N, Egs, nk, na);
-      }
-      {
-        // the fixed values replace the eigenvalues on the device (one copy);
-        // the staging vector lives until the copy has completed (the next
-        // download synchronises the stream)
-        wstage.clear();
-        for (const auto& kv : S.blocks) wstage.insert(wstage.end(), kv.second.value.begin(), kv.second.value.end());
-        NRGB_CUDA(cudaMemcpyAsync(wall, wstage.data(), wstage.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-        h2d += wstage.size() * sizeof(double);
-      }
-      totalenergy += Egs * scale1;
-      for (auto& kv : S.blocks) {
-        kv.second.absE.resize(kv.second.dim);
-        for (int r = 0; r < kv.second.dim; ++r) kv.second.absE[r] = totalenergy + kv.second.value[r] * scale1;
-      }
-      td_rows.push_back(td(S, N));
-      if (P.dumpannotated) {
-        std::vector<std::pair<double, Invar>> l;
-        for (const auto& kv : S.blocks)
-          for (double x : kv.second.value) l.push_back({x, kv.first});
-        std::sort(l.begin(), l.end());
-        annotated.push_back({scale1, totalenergy, std::move(l)});
+        const size_t tbytes = trunc_tail_bytes(nb);
+        if (tbytes > tail_dev_bytes) {
+          if (tail_dev) NRGB_CUDA(cudaFreeAsync(tail_dev, st));
+          tail_dev_bytes = tbytes + tbytes / 2;
+          NRGB_CUDA(cudaMallocAsync(&tail_dev, tail_dev_bytes, st));
+        }
+        if (tbytes > tail_pin_bytes) {
+          NRGB_CUDA(cudaStreamSynchronize(st));
+          if (tail_pin) NRGB_CUDA(cudaFreeHost(tail_pin));
+          tail_pin_bytes = tbytes + tbytes / 2;
+          NRGB_CUDA(cudaMallocHost(&tail_pin, tail_pin_bytes));
+        }
+        TruncRules R{P.fixeps, P.keepenergy, P.keep, P.keepmin, P.safeguard, P.safeguardmax,
+                     (cfs_flags() && last(N) && !P.lastalloverride) ? 1 : 0, P.betabar};
+        NRGB_CUDA(truncate_step(upload(tb), nb, wall, (int)wtot, R, tstate, twork, tail_dev, st));
+        launches += 17;
+        NRGB_CUDA(cudaMemcpyAsync(tail_pin, tail_dev, tbytes, cudaMemcpyDeviceToHost, st));
+        NRGB_CUDA(cudaStreamSynchronize(st));
+        d2h += tbytes;
+        const TruncTail& T = *reinterpret_cast<const TruncTail*>(tail_pin);
+        if (T.flags & 1) throw std::runtime_error("truncation: ground state not at zero");
+        if (T.flags & 2)
+          throw std::runtime_error("truncation: eigenvalues of a block not ascending after the splitting correction");
+        tstate.map_count = T.map_count;
+        const int* kept = trunc_tail_kept(tail_pin);
+        const double Egs = T.Egs;
+        S.Egs = Egs;
+        size_t b = 0;
+        for (auto& kv : S.blocks) {
+          kv.second.kept = kept[b++];
+          kv.second.shift = Egs;
+        }
+        if (getenv("NRGB_LOG")) {
+          // the reference's per-step log line (src/nrg.cc:3010-3013), to stderr
+          size_t nk = 0, na = 0;
+          for (const auto& kv : S.blocks) {
+            nk += kv.second.kept;
+            na += kv.second.dim;
+          }
+          fprintf(stderr, "N=%d Egs=%.17g Kept: %zu out of %zu\n", N, Egs, nk, na);
+        }
+        totalenergy += Egs * scale1;
+        S.total = totalenergy;
+        S.wall = wall;
+        S.wtot = (int)wtot;
+        td_rows.push_back(td_sums(S, N, trunc_tail_sums(tail_pin, nb)));
       }
       sections["sweep1 truncate+td"] += secs(ts);
       // operator recalculation
@@ -755,39 +844,32 @@ struct NrgDriver::Impl {
       auto s_new = std::make_unique<Slab>(st);
       std::map<std::string, DevBlocks> singlets_new;
       for (const auto& kv : singlets) singlets_new[kv.first] = recalc_op('s', S, kv.second, false, *s_new);
-      // expectation values of singlet operators (nrg_measure_singlet, src/nrg.cc:2226-2236)
-      std::map<std::string, double> row;
-      if (!singlets_new.empty()) {
-        std::vector<DiagGather> dg;
-        int off = 0, maxl = 0;
-        std::vector<std::pair<std::string, Invar>> order;
-        for (const auto& op : singlets_new)
-          for (const auto& kv : S.blocks) {
-            const DevMat& M = op.second.at({kv.first, kv.first});
-            dg.push_back(DiagGather{M.p, M.ld, M.rows, off});
-            order.push_back({op.first, kv.first});
-            off += M.rows;
-            maxl = std::max(maxl, M.rows);
-          }
-        double* buf = f_new->alloc(off + 1);
-        NRGB_CUDA(gather_diag_launch(upload(dg), (int)dg.size(), maxl, buf, st));
-        launches += 1;
-        const std::vector<double> diagv = download(buf, off);
-        double Zs = 0;
-        for (const auto& kv : S.blocks)
-          for (int r = 0; r < kv.second.kept; ++r) Zs += sym->mult(kv.first) * exp(-P.betabar * kv.second.value[r]);
-        size_t p = 0;
-        for (size_t k = 0; k < dg.size(); ++k) {
-          const Block& b = S.blocks.at(order[k].second);
-          double s = 0;
-          for (int r = 0; r < dg[k].len; ++r) s += exp(-P.betabar * b.value[r]) * diagv[p + r];
-          row[order[k].first] += sym->mult(order[k].second) * s;
-          p += dg[k].len;
+      // expectation values of singlet operators (nrg_measure_singlet,
+      // src/nrg.cc:2226-2236): the diagonals are gathered now, the sums
+      // are taken when the eigenvalues come to the host after the sweep
+      {
+        ExpvDeferred x;
+        x.step = steps.size() - 1;
+        x.T = scale1 / P.betabar;
+        if (!singlets_new.empty()) {
+          std::vector<DiagGather> dg;
+          int off = 0, maxl = 0;
+          for (const auto& op : singlets_new)
+            for (const auto& kv : S.blocks) {
+              const DevMat& M = op.second.at({kv.first, kv.first});
+              dg.push_back(DiagGather{M.p, M.ld, M.rows, off});
+              x.order.push_back({op.first, kv.first});
+              x.len.push_back(M.rows);
+              off += M.rows;
+              maxl = std::max(maxl, M.rows);
+            }
+          double* buf = expv_slab->alloc(off + 1);
+          NRGB_CUDA(gather_diag_launch(upload(dg), (int)dg.size(), maxl, buf, st));
+          launches += 1;
+          x.diag = buf;
         }
-        for (auto& kv : row) kv.second /= Zs;
+        expv_def.push_back(std::move(x));
       }
-      expv_rows.push_back({scale1 / P.betabar, row});
-      NRGB_CUDA(cudaStreamSynchronize(st));
       t_recalc += secs(t0);
       sections["sweep1 recalc"] += secs(t0);
       // the new <f> and singlets replace the old ones; truncated values become prev
@@ -798,7 +880,7 @@ struct NrgDriver::Impl {
       prev.clear();
       for (const auto& kv : S.blocks) prev[kv.first] = Prev{kv.second.w, kv.second.kept};
     }
-    NRGB_CUDA(cudaStreamSynchronize(st));
+    finish_sweep1();
     GSenergy = totalenergy;
   }
 
@@ -1378,7 +1460,9 @@ struct NrgDriver::Impl {
     const auto t0 = Clock::now();
     t_diag = t_recalc = t_dm = t_spec = 0;
     launches = h2d = d2h = 0;
-    cluster_map.clear();
+    free_trunc();
+    expv_def.clear();
+    expv_slab.reset(new Slab(st));
     td_rows.clear();
     expv_rows.clear();
     annotated.clear();

@@ -50,6 +50,8 @@ class Symmetry {
   virtual std::vector<std::string> td_names() const = 0;
   virtual std::vector<double> td_values(const std::vector<std::pair<Invar, const std::vector<double>*>>& blocks,
                                         double factor, double Z) const = 0;
+  // Same from the Boltzmann sums sum_r e^(-factor E_r) of each block.
+  virtual std::vector<double> td_values_sums(const std::vector<std::pair<Invar, double>>& zsum, double Z) const = 0;
   static Invar combine(const Invar& a, const Invar& b) { return {a.first + b.first, a.second + b.second}; }
   static Invar inverse(const Invar& a) { return {-a.first, -a.second}; }
 };
@@ -151,6 +153,17 @@ class SymmetryQS : public Symmetry {
       double sumZ = 0;
       for (double x : *b.second) sumZ += exp(-factor * x);
       sumZ *= mult(b.first);
+      const double q = b.first.first, ss = b.first.second;
+      trQ += sumZ * q;
+      trQ2 += sumZ * q * q;
+      trSZ += sumZ * (ss * ss - 1) / 12.0;
+    }
+    return {trSZ / Z, trQ / Z, trQ2 / Z};
+  }
+  std::vector<double> td_values_sums(const std::vector<std::pair<Invar, double>>& zsum, double Z) const override {
+    double trSZ = 0, trQ = 0, trQ2 = 0;
+    for (const auto& b : zsum) {
+      const double sumZ = b.second * mult(b.first);
       const double q = b.first.first, ss = b.first.second;
       trQ += sumZ * q;
       trQ2 += sumZ * q * q;

@@ -17,6 +17,7 @@ EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
            "nrgb_kernel_work",
            "nrgb_basis_change_noalloc", "nrgb_run", "nrgb_set_eig_mode",
            "nrgb_set_wait_limit", "nrgb_inject_barrier_shortfall",
+           "nrgb_autotune", "nrgb_set_schedule", "nrgb_get_schedule",
            "nrgb_server_create", "nrgb_server_submit", "nrgb_server_wait", "nrgb_server_error",
            "nrgb_server_counters", "nrgb_server_destroy", "nrgb_project_bytes"]
 
@@ -56,6 +57,9 @@ def load(path: str = LIBPATH):
     lib.nrgb_run.argtypes = [vp, C.c_char_p, C.c_char_p, dp]
     lib.nrgb_set_eig_mode.argtypes = [vp, C.c_int]
     lib.nrgb_set_wait_limit.argtypes = [vp, C.c_int]
+    lib.nrgb_autotune.argtypes = [vp, C.c_char_p, C.c_int]
+    lib.nrgb_set_schedule.argtypes = [vp, C.c_int, C.c_int]
+    lib.nrgb_get_schedule.argtypes = [vp, ip, ip, ip]
     lib.nrgb_inject_barrier_shortfall.argtypes = [vp, C.c_int]
     lib.nrgb_eig_recalc_step.argtypes = [vp, C.c_int, ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                          C.c_int, ip, ip, C.POINTER(vp), C.POINTER(vp)]
@@ -180,6 +184,21 @@ class Context:
     def set_eig_mode(self, mode: int):
         """0: one batched eigensolver call per step; 1: one call per block."""
         self._check(self.lib.nrgb_set_eig_mode(self.h, mode), "nrgb_set_eig_mode")
+
+    def autotune(self):
+        """Measure and set the device's schedule; returns the report (dict)."""
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        self._check(self.lib.nrgb_autotune(self.h, buf, len(buf)), "nrgb_autotune")
+        return json.loads(buf.value.decode())
+
+    def set_schedule(self, cluster_limit: int = 0, gemm_large_from: int = 0):
+        self._check(self.lib.nrgb_set_schedule(self.h, cluster_limit, gemm_large_from), "nrgb_set_schedule")
+
+    def get_schedule(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.lib.nrgb_get_schedule(self.h, C.byref(a), C.byref(b), C.byref(c)), "nrgb_get_schedule")
+        return {"cluster_limit": a.value, "gemm_large_from": b.value, "cluster_capacity": c.value}
 
     def set_wait_limit(self, poll_log2: int):
         """Device barrier waits give up after 2**poll_log2 polls (default 23)."""

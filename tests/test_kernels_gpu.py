@@ -144,8 +144,18 @@ def test_profile_only_times_one_kernel(ctx):
 
 
 def test_gemm_grouped_large_tiles(ctx):
-    """Problems large enough that the launch uses the 128x128-tile kernel."""
+    """Problems large enough for the 128x128-tile kernel, with the schedule
+    forcing it (gemm_large_from = 1) so that this kernel is the one that runs."""
     import nrgb
+    saved = ctx.get_schedule()
+    ctx.set_schedule(saved["cluster_limit"], 1)
+    try:
+        _large_tiles_case(ctx, nrgb)
+    finally:
+        ctx.set_schedule(saved["cluster_limit"], saved["gemm_large_from"])
+
+
+def _large_tiles_case(ctx, nrgb):
     rng = np.random.default_rng(5)
     dev = "cuda:0"
     outs, terms, refs, keep = [], [], [], []
