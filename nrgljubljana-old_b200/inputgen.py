@@ -6,10 +6,14 @@ maketable at initial.m:4309-4392), which is not available here.  This module
 restates the parts of that front end that the QS (charge U(1) x spin SU(2))
 workloads need:
 
-* the Wilson chain of a flat band in the Yoshida-Whitaker-Oliveira (Y)
-  discretization, by Lanczos tridiagonalisation of the star Hamiltonian in
-  arbitrary precision (initial.m:2902-2908 band, 3538-3545 Y energies,
-  3055-3164 Lanczos recursion, 4040-4044 table output);
+* the Wilson chain of a flat band in the Yoshida-Whitaker-Oliveira (Y),
+  Campo-Oliveira (C) or Zitko-Pruschke (Z) discretization, by Lanczos
+  tridiagonalisation of the star Hamiltonian in arbitrary precision
+  (initial.m:2902-2908 band, 3538-3598 representative energies, 3055-3164
+  Lanczos recursion, 4040-4044 table output);
+* the Wilson chain of a tabulated hybridisation function on the adaptive
+  logarithmic mesh (the tools/adapt nrgchain program), checked against the
+  reference's own fixtures;
 * the initial cluster (impurity + site f_0 of every channel): Fock-space
   Hamiltonian, its eigenstates per invariant subspace (Q, SS) with the
   representative member at S_z = S (initial.m:1664-1668), energies shifted by
@@ -55,21 +59,56 @@ def scale_factor(N: int, Lambda: float, z: float = 1.0, discretization: str = "Y
     return s * Lambda ** (-(N - 1) / 2.0 + 1.0 - z) * bandrescale
 
 
-def wilson_chain_flat(Lambda: float, z: float, Nmax: int, mMAX: int | None = None,
-                      dps: int = 200) -> Tuple[np.ndarray, np.ndarray]:
-    """Chain coefficients xi[0..Nmax], zeta[0..Nmax] of a flat band (D=1) in the
-    Y discretization.
+def _lanczos_star(de_pos, de_neg, u_pos, u_neg, Nmax):
+    """Tridiagonalise the star Hamiltonian diag(+de_pos, -de_neg) from the
+    start vector (u_pos, u_neg) (normalised here) at the current mpmath
+    precision; returns the raw chain coefficients xi[0..Nmax], zeta[0..Nmax]
+    as mpf (initial.m:3055-3164; tools/adapt/nrgchain.cc tridiag)."""
+    diagA = list(de_pos) + [-x for x in de_neg]
+    u = list(u_pos) + list(u_neg)
+    norm = mpmath.fsum(x * x for x in u)
+    u = [x / mpmath.sqrt(norm) for x in u]  # rescale exactly to one
+    xi, zeta = [], []
+    uprev = [mpmath.mpf(0)] * len(u)
+    xiprev = mpmath.mpf(0)
+    for n in range(Nmax + 1):
+        Au = [a * x for a, x in zip(diagA, u)]
+        zn = mpmath.fsum(a * x for a, x in zip(Au, u))
+        r = [a - zn * x - xiprev * p for a, x, p in zip(Au, u, uprev)]
+        # at this precision no reorthogonalisation is needed; renormalise
+        # as initial.m:3450-3458
+        xn = mpmath.sqrt(mpmath.fsum(x * x for x in r))
+        zeta.append(zn)
+        xi.append(xn)
+        uprev, u = u, [x / xn for x in r]
+        xiprev = xn
+    return xi, zeta
 
-    Star levels (initial.m:2902-2908, 3538-3545): interval edges eps_0 = 1,
+
+def wilson_chain_flat(Lambda: float, z: float, Nmax: int, mMAX: int | None = None,
+                      dps: int = 200, discretization: str = "Y") -> Tuple[np.ndarray, np.ndarray]:
+    """Chain coefficients xi[0..Nmax], zeta[0..Nmax] of a flat band (D=1).
+
+    Star levels (initial.m:2902-2908): interval edges eps_0 = 1,
     eps_m = Lambda^(1-z-m); hybridisation weights df_m = eps_m - eps_{m+1}
-    (theta = 2, symmetric); representative energies de_0 = (1+Lambda^-z)/2,
-    de_m = (1+1/Lambda)/2 * Lambda^(1-z-m).  mMAX defaults to
-    max(80, 2*Nmax) as in initial.m:2877.  The Lanczos recursion runs at `dps`
-    decimal digits, since double precision loses orthogonality along the
-    chain (the reference uses 1000 digits, initial.m:2790-2793).
+    (theta = 2, symmetric).  Representative energies by discretization
+    scheme:
+      Y (Yoshida-Whitaker-Oliveira, initial.m:3538-3545):
+          de_0 = (1+Lambda^-z)/2,  de_m = (1+1/Lambda)/2 * Lambda^(1-z-m);
+      C (Campo-Oliveira, initial.m:3568-3572):
+          de_m = (eps_m - eps_{m+1}) / ln(eps_m / eps_{m+1});
+      Z (Zitko-Pruschke, initial.m:3592-3598):
+          de_0 = (1 - Lambda^-z + ln Lambda - z ln Lambda) / ln Lambda,
+          de_m as for C (m >= 1).
+    mMAX defaults to max(80, 2*Nmax) as in initial.m:2877.  The Lanczos
+    recursion runs at `dps` decimal digits, since double precision loses
+    orthogonality along the chain (the reference uses 1000 digits,
+    initial.m:2790-2793).
     """
     if mpmath is None:
         raise RuntimeError("mpmath is required for the Wilson chain")
+    if discretization not in ("Y", "C", "Z"):
+        raise ValueError("unknown discretization " + discretization)
     if mMAX is None:
         mMAX = max(80, 2 * Nmax)
     mp = mpmath.mp
@@ -78,30 +117,141 @@ def wilson_chain_flat(Lambda: float, z: float, Nmax: int, mMAX: int | None = Non
     try:
         L = mpmath.mpf(Lambda)
         Z = mpmath.mpf(z)
+        lnL = mpmath.log(L)
         eps = [mpmath.mpf(1)] + [L ** (1 - Z - m) for m in range(1, mMAX + 2)]
         df = [eps[m] - eps[m + 1] for m in range(mMAX + 1)]
-        de = [(1 + L ** (-Z)) / 2] + [(1 + 1 / L) / 2 * L ** (1 - Z - m) for m in range(1, mMAX + 1)]
+        if discretization == "Y":
+            de = [(1 + L ** (-Z)) / 2] + [(1 + 1 / L) / 2 * L ** (1 - Z - m) for m in range(1, mMAX + 1)]
+        else:
+            de = [(eps[m] - eps[m + 1]) / mpmath.log(eps[m] / eps[m + 1]) for m in range(mMAX + 1)]
+            if discretization == "Z":
+                de[0] = (1 - L ** (-Z) + lnL - Z * lnL) / lnL
         theta = mpmath.mpf(2)
-        # Diagonal star Hamiltonian A = diag(+de, -de) with start vector u0.
-        diagA = de + [-x for x in de]
-        u = [mpmath.sqrt(x / theta) for x in df] * 2
-        norm = mpmath.fsum(x * x for x in u)
-        u = [x / mpmath.sqrt(norm) for x in u]  # rescale exactly to one
-        xi, zeta = [], []
-        uprev = [mpmath.mpf(0)] * len(u)
-        xiprev = mpmath.mpf(0)
-        for n in range(Nmax + 1):
-            Au = [a * x for a, x in zip(diagA, u)]
-            zn = mpmath.fsum(a * x for a, x in zip(Au, u))
-            r = [a - zn * x - xiprev * p for a, x, p in zip(Au, u, uprev)]
-            # one step of reorthogonalisation against the previous vectors is
-            # unnecessary at this precision; renormalise as initial.m:3450-3458.
-            xn = mpmath.sqrt(mpmath.fsum(x * x for x in r))
-            zeta.append(zn)
-            xi.append(xn)
-            uprev, u = u, [x / xn for x in r]
-            xiprev = xn
+        u = [mpmath.sqrt(x / theta) for x in df]
+        xi, zeta = _lanczos_star(de, de, u, u, Nmax)
         return (np.array([float(x) for x in xi]), np.array([float(x) for x in zeta]))
+    finally:
+        mp.dps = old
+
+
+# ---------------------------------------------------------------------------
+# Wilson chain of a tabulated density of states with the adaptive mesh
+# ---------------------------------------------------------------------------
+
+class _LinInt:
+    """Linear interpolation of a table, constant beyond its ends (the
+    tabulated functions of tools/adapt: linint.h LinInt)."""
+
+    def __init__(self, xy):
+        xy = sorted(xy)
+        self.x = np.array([p[0] for p in xy])
+        self.y = np.array([p[1] for p in xy])
+
+    def __call__(self, x):
+        if x <= self.x[0]:
+            return float(self.y[0])
+        if x >= self.x[-1]:
+            return float(self.y[-1])
+        i = int(np.searchsorted(self.x, x, side="right")) - 1
+        x0, x1, f0, f1 = self.x[i], self.x[i + 1], self.y[i], self.y[i + 1]
+        return float(f0 + (f1 - f0) / (x1 - x0) * (x - x0))
+
+
+class _IntLinInt(_LinInt):
+    """Running integral of the linearly interpolated table from its first
+    point: trapezoid sums at the nodes, exact quadratic inside an interval,
+    linear continuation beyond the ends (linint.h IntLinInt, calc.h
+    integrate)."""
+
+    def __init__(self, xy):
+        super().__init__(xy)
+        dx = np.diff(self.x)
+        self.I = np.concatenate([[0.0], np.cumsum(dx * (self.y[1:] + self.y[:-1]) / 2.0)])
+
+    def __call__(self, x):
+        if x <= self.x[0]:
+            return float(self.I[0] + self.y[0] * (x - self.x[0]))
+        if x >= self.x[-1]:
+            return float(self.I[-1] + self.y[-1] * (x - self.x[-1]))
+        i = int(np.searchsorted(self.x, x, side="right")) - 1
+        x0, x1, f0, f1 = self.x[i], self.x[i + 1], self.y[i], self.y[i + 1]
+        d = x - x0
+        return float(self.I[i] + d * f0 + d * d * ((f1 - f0) / (x1 - x0)) / 2.0)
+
+
+def _trapezoid_to(xy, b):
+    """Integral of the table from its first point up to b (calc.h integrate_ab)."""
+    xy = sorted(xy)
+    s = 0.0
+    for (x0, y0), (x1, y1) in zip(xy[:-1], xy[1:]):
+        if x0 < b and x1 <= b:
+            dx = x1 - x0
+        elif x0 < b < x1:
+            dx = b - x0
+        else:
+            dx = 0.0
+        s += dx * (y0 + y1) / 2.0
+    return s
+
+
+def read_two_columns(path):
+    out = []
+    with open(path) as fh:
+        for line in fh:
+            t = line.split()
+            if not t or t[0].startswith("#"):
+                continue
+            out.append((float(t[0]), float(t[1])))
+    return out
+
+
+def wilson_chain_tabulated(dos, g_pos, g_neg, f_pos, f_neg, Lambda: float, z: float, Nmax: int,
+                           mMAX: int | None = None, adapt: bool = True, bandrescale: float = 1.0,
+                           dps: int = 600) -> Tuple[np.ndarray, np.ndarray, float]:
+    """Wilson chain of a tabulated hybridisation function with the adaptive
+    logarithmic mesh (Zitko, Comput. Phys. Commun. 180, 1271 (2009)): the
+    restatement of tools/adapt/nrgchain.cc (tables, tridiag).
+
+    dos: (omega, rho) pairs on both sides of zero; g_*/f_*: (x, g(x)) and
+    (x, f(x)) tables of the mesh ODE solutions (GSOL*.dat, FSOL*.dat).
+    Mesh eps(x) = g(x) Lambda^(2-x) for x > 2 (1 below), representative
+    energies E(x) = f(x) Lambda^(2-x); interval m (x = z+m+1) carries weight
+    int_{eps(x+1)}^{eps(x)} rho and energy E(x), m = 0..mMAX.  Returns the raw
+    xi[0..Nmax] (divide by SCALE(n+1) of the Z scheme for nrgchain's xi.dat)
+    and zeta[0..Nmax], and theta (total weight up to |omega| = 1)."""
+    if mMAX is None:
+        mMAX = 2 * Nmax
+    pos = [(abs(x), y * bandrescale) for x, y in dos if x > 0]
+    neg = [(abs(x), y * bandrescale) for x, y in dos if x < 0]
+    pos = [(x / bandrescale, y) for x, y in pos]
+    neg = [(x / bandrescale, y) for x, y in neg]
+    ip, ineg = _IntLinInt(pos), _IntLinInt(neg)
+    gp, gn, fp, fn = _LinInt(g_pos), _LinInt(g_neg), _LinInt(f_pos), _LinInt(f_neg)
+
+    def eps(g, x):
+        return 1.0 if x <= 2.0 else (g(x) if adapt else 1.0) * Lambda ** (2.0 - x)
+
+    theta = _trapezoid_to(pos, 1.0) + _trapezoid_to(neg, 1.0)
+    du_p, du_n, de_p, de_n = [], [], [], []
+    for m in range(mMAX + 1):
+        x1, x2 = z + m + 1, z + m + 2
+        du_p.append(math.sqrt(ip(eps(gp, x1)) - ip(eps(gp, x2))) / math.sqrt(theta))
+        du_n.append(math.sqrt(ineg(eps(gn, x1)) - ineg(eps(gn, x2))) / math.sqrt(theta))
+        de_p.append(fp(x1) * Lambda ** (2.0 - x1))
+        de_n.append(fn(x1) * Lambda ** (2.0 - x1))
+    check = sum(a * a for a in du_p) + sum(a * a for a in du_n)
+    if abs(1.0 - check) > 1e-10:
+        raise ValueError("weights of the discretization do not sum to theta (1 - sum = %g)" % (1.0 - check))
+    du_p = [a / math.sqrt(check) for a in du_p]
+    du_n = [a / math.sqrt(check) for a in du_n]
+    mp = mpmath.mp
+    old = mp.dps
+    mp.dps = dps
+    try:
+        M = mpmath.mpf
+        xi, zeta = _lanczos_star([M(x) for x in de_p], [M(x) for x in de_n], [M(x) for x in du_p],
+                                 [M(x) for x in du_n], Nmax)
+        return np.array([float(x) for x in xi]), np.array([float(x) for x in zeta]), theta
     finally:
         mp.dps = old
 
@@ -434,16 +584,17 @@ def write_param(path: str, params: Dict[str, object]) -> None:
 
 def make_siam(dirpath: str, U: float, eps_d: float, Gamma: float, Lambda: float,
               Nmax: int, z: float = 1.0, params: Dict[str, object] | None = None,
-              V: float | None = None, dps: int = 200) -> dict:
+              V: float | None = None, dps: int = 200, discretization: str = "Y") -> dict:
     """Generate `data` and `param` for a QS single-impurity Anderson model on a
-    flat band (D=1) in directory `dirpath`.  V defaults to sqrt(2 Gamma/pi)."""
+    flat band (D=1) in directory `dirpath`.  V defaults to sqrt(2 Gamma/pi);
+    discretization Y, C or Z (wilson_chain_flat)."""
     os.makedirs(dirpath, exist_ok=True)
     if V is None:
         V = math.sqrt(2.0 * Gamma / math.pi)
-    xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps)
+    xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps, discretization=discretization)
     m = siam_cluster(U, eps_d, V, zeta0=zeta[0])
-    info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, 1)
-    p = {"Lambda": Lambda, "z": z, "discretization": "Y"}
+    info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, 1, discretization)
+    p = {"Lambda": Lambda, "z": z, "discretization": discretization}
     if params:
         p.update(params)
     write_param(os.path.join(dirpath, "param"), p)
@@ -452,12 +603,12 @@ def make_siam(dirpath: str, U: float, eps_d: float, Gamma: float, Lambda: float,
 
 
 def make_kondo(dirpath: str, J: List[float], Lambda: float, Nmax: int, z: float = 1.0,
-               params: Dict[str, object] | None = None, dps: int = 200) -> dict:
+               params: Dict[str, object] | None = None, dps: int = 200, discretization: str = "Y") -> dict:
     os.makedirs(dirpath, exist_ok=True)
-    xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps)
+    xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps, discretization=discretization)
     m = kondo_cluster(J)
-    info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, len(J))
-    p = {"Lambda": Lambda, "z": z, "discretization": "Y"}
+    info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, len(J), discretization)
+    p = {"Lambda": Lambda, "z": z, "discretization": discretization}
     if params:
         p.update(params)
     write_param(os.path.join(dirpath, "param"), p)
