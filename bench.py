@@ -686,6 +686,52 @@ def run_micro_only(args):
     return 0
 
 
+def run_split_micro(edge, slices, nprob):
+    """Split-precision grouped GEMM (INT8 slices on tcgen05) against the FP64
+    DMMA grouped GEMM on `nprob` problems of edge^3, device-resident inputs;
+    CUDA events on the launch stream; the split result is checked against
+    the FP64 one."""
+    import torch
+
+    import nrgb
+    dev = torch.device("cuda", 0)
+    ctx = nrgb.Context(0)
+    g = torch.Generator(device=dev).manual_seed(SEED)
+    A = [torch.randn(edge, edge, generator=g, device=dev, dtype=torch.float64) for _ in range(nprob)]
+    B = [torch.randn(edge, edge, generator=g, device=dev, dtype=torch.float64) for _ in range(nprob)]
+    C1 = [torch.empty(edge, edge, device=dev, dtype=torch.float64) for _ in range(nprob)]
+    C2 = [torch.empty(edge, edge, device=dev, dtype=torch.float64) for _ in range(nprob)]
+    terms = [nrgb.GemmTerm(a.data_ptr(), b.data_ptr(), edge, edge, edge, 0, 0, 1.0) for a, b in zip(A, B)]
+    o1 = [nrgb.GemmOut(c.data_ptr(), edge, edge, edge, 0.0, i, 1) for i, c in enumerate(C1)]
+    o2 = [nrgb.GemmOut(c.data_ptr(), edge, edge, edge, 0.0, i, 1) for i, c in enumerate(C2)]
+    st = torch.cuda.current_stream(dev)
+    out = {"edge": edge, "problems": nprob, "slices": slices}
+    fl = 2.0 * edge ** 3 * nprob
+    for key, fn in (("fp64", lambda: ctx.gemm_grouped_dev(o1, terms, stream=st.cuda_stream)),
+                    ("split", lambda: ctx.gemm_grouped_split_dev(slices, o2, terms, stream=st.cuda_stream))):
+        fn()
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(st)
+            fn()
+            t1.record(st)
+            torch.cuda.synchronize()
+            best = min(best, t0.elapsed_time(t1))
+        out[key + "_ms"] = best
+        out[key + "_tflops"] = fl / best / 1e9
+    # the split call includes slicing the operands; its INT8 work is
+    # S(S+1)/2 products of the same shape
+    out["int8_tops"] = fl * slices * (slices + 1) / 2 / out["split_ms"] / 1e9
+    err = max(((x - y).abs().max() / (y.abs().max() + 1.0)).item() for x, y in zip(C2, C1))
+    out["max_rel_diff_vs_fp64"] = err
+    ctx.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_ncu_small(nmax):
     """Small profiling case (no torch on the GPU): 12 blocks with sizes up to
     `nmax` and their 72 operators through the host-buffer C ABI, twice."""
@@ -726,6 +772,10 @@ def main():
     ap.add_argument("--detail", default="", help="also write the line and its details to this JSON file")
     ap.add_argument("--micro", action="store_true", help="run only the 40-block microbenchmark")
     ap.add_argument("--nmax", type=int, default=4096, help="cap on block sizes of the microbenchmark")
+    ap.add_argument("--split-micro", type=int, default=0,
+                    help="time the split-precision grouped GEMM against FP64 on problems of this edge")
+    ap.add_argument("--slices", type=int, default=8)
+    ap.add_argument("--nprob", type=int, default=4)
     ap.add_argument("--ncu-small", type=int, default=0,
                     help="run only the small profiling case with blocks up to this size (no torch GPU work)")
     args = ap.parse_args()
@@ -735,6 +785,8 @@ def main():
     NMAX = args.nmax
     if args.ncu_small:
         return run_ncu_small(args.ncu_small)
+    if args.split_micro:
+        return run_split_micro(args.split_micro, args.slices, args.nprob)
     if args.micro:
         return run_micro_only(args)
     rank = int(os.environ.get("RANK", "0"))

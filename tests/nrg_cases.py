@@ -167,7 +167,10 @@ def _parse_annotated_text(text):
 
 
 # Accuracy targets of the plain FP64 path against the oracle.
-RTOL_TD = 1e-8      # td (chi(T) = <Sz^2>, S(T), ...) and custom, relative
+RTOL_TD = 1e-8      # td (chi(T) = <Sz^2>, S(T), ...) and custom, relative, ...
+ATOL_TD = 1e-12     # ... plus 1e-12 absolute: every column is a ratio of sums of O(1) terms, and a
+                    # column that vanishes by symmetry (<Q> at particle-hole symmetry) keeps
+                    # their FP64 cancellation noise (up to ~2e-13 here), which differs run to run
 RTOL_E = 1e-10      # energy flow (annotated.dat), relative
 ATOL_E = 1e-12      # floor for levels at or near the ground state (E = 0)
 RTOL_W = 1e-8       # spectral weight per bin, relative, where |w| >= WFLOOR max|w|, ...
@@ -181,21 +184,21 @@ def compare_outputs(got, ref, what=""):
     the FP64 targets: td and custom within 1e-8 relative (columns that vanish
     by symmetry against 1e-13 of the column scale), energies of the energy
     flow within 1e-10 relative (1e-12 absolute at E ~ 0) with identical
-    quantum numbers and degeneracies, spectral bins within 1e-8 relative per
+    quantum numbers and degeneracies (td/custom also 1e-12 absolute, the
+    cancellation noise of columns that vanish by symmetry), spectral bins
+    within 1e-8 relative per
     bin wherever |w| >= 1e-6 of the largest bin and within 1e-8 of the largest
     bin everywhere (the per-bin check allows an absolute 1e-13 of the
     largest bin, the FP64 rounding level of the sums behind a small bin),
     broadened spectra within 1e-8 of their maximum."""
     to, tg = ref["td"], got["td"]
     assert to.shape == tg.shape, (what, to.shape, tg.shape)
-    colmax = np.max(np.abs(to), axis=0)
-    tol = RTOL_TD * np.abs(to) + 1e-13 * (1.0 + colmax)
+    tol = RTOL_TD * np.abs(to) + ATOL_TD
     assert np.all(np.abs(tg - to) <= tol), (what, "td", float(np.max((np.abs(tg - to) - tol) / (np.abs(to) + 1e-300))))
     if "custom" in ref:
         co, cg = ref["custom"], got["custom"]
         assert co.shape == cg.shape, (what, "custom shape")
-        colmax = np.max(np.abs(co), axis=0)
-        assert np.all(np.abs(cg - co) <= RTOL_TD * np.abs(co) + 1e-13 * (1.0 + colmax)), (what, "custom")
+        assert np.all(np.abs(cg - co) <= RTOL_TD * np.abs(co) + ATOL_TD), (what, "custom")
     if "annotated" in ref:
         assert "annotated" in got, (what, "annotated.dat missing")
         ao, ag = _parse_annotated_text(ref["annotated"]), _parse_annotated_text(got["annotated"])
@@ -269,12 +272,14 @@ def error_report(got, ref):
     the spectral weights per bin (bins above 1e-6 of the largest)."""
     out = {}
     ao, ag = _parse_annotated_text(ref["annotated"]), _parse_annotated_text(got["annotated"])
-    e = 0.0
+    e, ea = 0.0, 0.0
     for so, sg in zip(ao, ag):
         for x, y in zip(so, sg):
-            if x[0] != 0.0:
+            ea = max(ea, abs(y[0] - x[0]))
+            if abs(x[0]) >= 1e-2:  # relative error of levels above 1e-2 omega_N
                 e = max(e, abs(y[0] - x[0]) / abs(x[0]))
     out["energies"] = e
+    out["energies_abs"] = ea
     to, tg = ref["td"], got["td"]
     out["chi_T"] = float(np.max(np.abs(tg[:, 1] - to[:, 1]) / np.abs(to[:, 1])))
     out["S_T"] = float(np.max(np.abs(tg[:, 8] - to[:, 8]) / np.maximum(np.abs(to[:, 8]), 1e-300)))
