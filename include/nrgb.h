@@ -71,6 +71,86 @@ typedef struct {
 int nrgb_gemm_grouped_dev(nrgb_ctx* ctx, int nout, const nrgb_gemm_out* outs, int nterms,
                           const nrgb_gemm_term* terms, void* stream);
 
+/* ---- Step-level plan: the reference's own driver and Symmetry plug-ins
+ * call the device one NRG step at a time.  nrg_iterate (src/nrg.cc:3043-3051)
+ * and the Symmetry class (src/symmetry.cc:64-221, sym-<SYM>.cc,
+ * nrg-recalc-<SYM>.cc) stay on the host; they expand their tables into the
+ * flat task lists below, so a new symmetry needs host tables only.  Energies,
+ * eigenvectors and operator blocks stay in device memory under integer
+ * handles owned by the context. */
+
+/* Device matrices (column-major).  nrgb_mat_upload copies rows x cols
+ * doubles from host memory; nrgb_mat_download copies back; nrgb_run_begin
+ * frees every handle of the context and resets the splitting-correction map
+ * (the reference keeps it for a whole run, src/splitting.cc). */
+int nrgb_mat_upload(nrgb_ctx* ctx, int rows, int cols, const double* host, int* handle);
+int nrgb_mat_download(nrgb_ctx* ctx, int handle, double* host);
+int nrgb_mat_shape(nrgb_ctx* ctx, int handle, int* rows, int* cols);
+int nrgb_mat_free(nrgb_ctx* ctx, int handle);
+int nrgb_run_begin(nrgb_ctx* ctx);
+
+/* Diagonal term of block blk (diag_function, src/matrix.cc:172-192 and the
+ * sqrt(Lambda) E_prev diagonal of src/nrg.cc:2456-2478):
+ *   H[off + r, off + r] += scale * src[r] + shift,  r < len
+ * (src: handle of a vector of at least len values, or -1 for shift only). */
+typedef struct {
+  int blk, off, len, src;
+  double scale, shift;
+} nrgb_diag_term;
+/* Off-diagonal term (offdiag_build, src/matrix.cc:86-137):
+ *   H[offi + r, offj + c] = factor * src(r, c)  and the mirror entry,
+ * src: handle of a rows x cols matrix (an <I||f||J> block). */
+typedef struct {
+  int blk, offi, offj, rows, cols, src;
+  double factor;
+} nrgb_offdiag_term;
+typedef struct {
+  int nblocks;
+  const int* dim;  /* block dimensions */
+  int ndiag;
+  const nrgb_diag_term* diag;
+  int noff;
+  const nrgb_offdiag_term* off;
+  /* truncation (src/nrg.cc:1919-1998, src/splitting.cc) */
+  double fixeps, keepenergy;
+  int keep, keepmin;
+  double safeguard;
+  int safeguardmax;
+  int keep_all; /* keep every state (the last step of a CFS/FDM run) */
+  double betabar;
+} nrgb_step_plan;
+/* One NRG step on the device: assemble every block, diagonalise all of them
+ * (dsyev per block, src/diag.h:54-89), subtract the ground-state energy,
+ * apply the splitting correction and choose the retained states.  Outputs
+ * per block b: z_handles[b] (dim x dim eigenvectors, eigenvector r in column
+ * r), w_handles[b] (dim eigenvalues, ascending, ground state subtracted,
+ * corrected), kept[b]; egs (the subtracted ground-state energy) and, if not
+ * NULL, zsums[3b .. 3b+2] = sum_r e^(-betabar E_r), sum_r betabar E_r
+ * e^(-betabar E_r), sum_r (betabar E_r)^2 e^(-betabar E_r) over all states of
+ * block b (nrg_calculate_TD, src/nrg.cc:2333-2369). */
+int nrgb_step(nrgb_ctx* ctx, const nrgb_step_plan* plan, int* z_handles, int* w_handles, int* kept,
+              double* egs, double* zsums);
+
+/* Recalculation (recalc_general / recalc_f, src/recalc.cc:12-97, 164-281):
+ * output o (k1 x kp) = sum over its terms of
+ *   factor * Z1[off1 : off1+r1, 0 : k1]^T * op[0 : r1, 0 : rp] * Zp[offp : offp+rp, 0 : kp]
+ * with op = -1 meaning the identity (recalc_f, r1 == rp).  Z1, Zp: the
+ * eigenvector handles of nrgb_step (the reference's U blocks of
+ * split_in_blocks are these sub-blocks, transposed).  out_handles[o]
+ * receives a new handle per output. */
+typedef struct {
+  int z1, off1, r1;
+  int zp, offp, rp;
+  int op;
+  double factor;
+} nrgb_recalc_term;
+typedef struct {
+  int k1, kp;
+  int term0, nterms;
+} nrgb_recalc_out;
+int nrgb_recalc(nrgb_ctx* ctx, int nout, const nrgb_recalc_out* outs, int nterms, const nrgb_recalc_term* terms,
+                int* out_handles);
+
 /* Split-precision form of nrgb_gemm_grouped_dev (same descriptors): every
  * product is computed from `slices` (2..8) signed 7-bit slices of each
  * operand, with power-of-two scales per row of op(A) and per column of op(B),

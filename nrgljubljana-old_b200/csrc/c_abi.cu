@@ -17,57 +17,10 @@
 #include "syev.cuh"
 #include "../host/driver.h"
 
-namespace {
-// The reference's structure on the GPU: one solver call per block
-// (dsyev per invariant subspace, src/nrg.cc:2484-2507), for comparisons.
-struct PerBlockSolver : nrgb::EigSolver {
-  nrgb::SyevBatched* s = nullptr;
-  int solve(const std::vector<nrgb::SyevDesc>& probs, cudaStream_t st) override {
-    int l = 0;
-    for (const auto& p : probs) l += s->solve(std::vector<nrgb::SyevDesc>{p}, st);
-    return l;
-  }
-};
-}  // namespace
+#include "ctx.h"
 
-struct nrgb_ctx {
-  int device = 0;
-  std::string err;
-  cudaStream_t stream = nullptr;
-  std::unique_ptr<nrgb::SyevBatched> syev;
-  PerBlockSolver per_block;
-  int eig_mode = 0;
-  nrgb::DeviceArena scratch;
-  nrgb::DeviceArena io;
-  std::unique_ptr<nrgb::NrgDriver> driver;
-};
-
-namespace {
-
-// The solver nrgb_set_eig_mode selected for this context.
-nrgb::EigSolver* solver_of(nrgb_ctx* ctx) {
-  if (ctx->eig_mode == 1) {
-    ctx->per_block.s = ctx->syev.get();
-    return &ctx->per_block;
-  }
-  return ctx->syev.get();
-}
-
-template <class F>
-int guarded(nrgb_ctx* ctx, F&& f) {
-  if (!ctx) return 1;
-  try {
-    NRGB_CUDA(cudaSetDevice(ctx->device));
-    f();
-    ctx->err.clear();
-    return 0;
-  } catch (const std::exception& e) {
-    ctx->err = e.what();
-    return 2;
-  }
-}
-
-}  // namespace
+using nrgb::guarded;
+using nrgb::solver_of;
 
 extern "C" {
 
@@ -97,6 +50,7 @@ int nrgb_destroy(nrgb_ctx* ctx) {
   if (!ctx) return 0;
   cudaSetDevice(ctx->device);
   ctx->driver.reset();
+  nrgb::plan_release(ctx);
   ctx->syev.reset();
   ctx->scratch.release();
   ctx->io.release();

@@ -18,6 +18,8 @@ EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
            "nrgb_basis_change_noalloc", "nrgb_run", "nrgb_set_eig_mode",
            "nrgb_set_wait_limit", "nrgb_inject_barrier_shortfall",
            "nrgb_autotune", "nrgb_set_schedule", "nrgb_get_schedule",
+           "nrgb_mat_upload", "nrgb_mat_download", "nrgb_mat_shape", "nrgb_mat_free", "nrgb_run_begin",
+           "nrgb_step", "nrgb_recalc",
            "nrgb_server_create", "nrgb_server_submit", "nrgb_server_wait", "nrgb_server_error",
            "nrgb_server_counters", "nrgb_server_destroy", "nrgb_project_bytes"]
 
@@ -25,6 +27,33 @@ EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
 class GemmTerm(C.Structure):
     _fields_ = [("a", C.c_void_p), ("b", C.c_void_p), ("lda", C.c_int), ("ldb", C.c_int),
                 ("k", C.c_int), ("trans_a", C.c_int), ("trans_b", C.c_int), ("alpha", C.c_double)]
+
+
+class DiagTerm(C.Structure):
+    _fields_ = [("blk", C.c_int), ("off", C.c_int), ("len", C.c_int), ("src", C.c_int),
+                ("scale", C.c_double), ("shift", C.c_double)]
+
+
+class OffdiagTerm(C.Structure):
+    _fields_ = [("blk", C.c_int), ("offi", C.c_int), ("offj", C.c_int), ("rows", C.c_int), ("cols", C.c_int),
+                ("src", C.c_int), ("factor", C.c_double)]
+
+
+class StepPlan(C.Structure):
+    _fields_ = [("nblocks", C.c_int), ("dim", C.POINTER(C.c_int)), ("ndiag", C.c_int),
+                ("diag", C.POINTER(DiagTerm)), ("noff", C.c_int), ("off", C.POINTER(OffdiagTerm)),
+                ("fixeps", C.c_double), ("keepenergy", C.c_double), ("keep", C.c_int), ("keepmin", C.c_int),
+                ("safeguard", C.c_double), ("safeguardmax", C.c_int), ("keep_all", C.c_int),
+                ("betabar", C.c_double)]
+
+
+class RecalcTerm(C.Structure):
+    _fields_ = [("z1", C.c_int), ("off1", C.c_int), ("r1", C.c_int), ("zp", C.c_int), ("offp", C.c_int),
+                ("rp", C.c_int), ("op", C.c_int), ("factor", C.c_double)]
+
+
+class RecalcOut(C.Structure):
+    _fields_ = [("k1", C.c_int), ("kp", C.c_int), ("term0", C.c_int), ("nterms", C.c_int)]
 
 
 class GemmOut(C.Structure):
@@ -58,6 +87,13 @@ def load(path: str = LIBPATH):
     lib.nrgb_set_eig_mode.argtypes = [vp, C.c_int]
     lib.nrgb_set_wait_limit.argtypes = [vp, C.c_int]
     lib.nrgb_autotune.argtypes = [vp, C.c_char_p, C.c_int]
+    lib.nrgb_mat_upload.argtypes = [vp, C.c_int, C.c_int, vp, ip]
+    lib.nrgb_mat_download.argtypes = [vp, C.c_int, vp]
+    lib.nrgb_mat_shape.argtypes = [vp, C.c_int, ip, ip]
+    lib.nrgb_mat_free.argtypes = [vp, C.c_int]
+    lib.nrgb_run_begin.argtypes = [vp]
+    lib.nrgb_step.argtypes = [vp, C.POINTER(StepPlan), ip, ip, ip, dp, dp]
+    lib.nrgb_recalc.argtypes = [vp, C.c_int, C.POINTER(RecalcOut), C.c_int, C.POINTER(RecalcTerm), ip]
     lib.nrgb_set_schedule.argtypes = [vp, C.c_int, C.c_int]
     lib.nrgb_get_schedule.argtypes = [vp, ip, ip, ip]
     lib.nrgb_inject_barrier_shortfall.argtypes = [vp, C.c_int]
@@ -199,6 +235,54 @@ class Context:
         a, b, c = C.c_int(), C.c_int(), C.c_int()
         self._check(self.lib.nrgb_get_schedule(self.h, C.byref(a), C.byref(b), C.byref(c)), "nrgb_get_schedule")
         return {"cluster_limit": a.value, "gemm_large_from": b.value, "cluster_capacity": c.value}
+
+    # -- step-level plan --
+    def mat_upload(self, M):
+        import numpy as np
+        M = np.asfortranarray(np.atleast_2d(np.asarray(M, dtype=np.float64)))
+        h = C.c_int()
+        self._check(self.lib.nrgb_mat_upload(self.h, M.shape[0], M.shape[1], M.ctypes.data, C.byref(h)),
+                    "nrgb_mat_upload")
+        return h.value
+
+    def mat_download(self, handle):
+        import numpy as np
+        r, c = C.c_int(), C.c_int()
+        self._check(self.lib.nrgb_mat_shape(self.h, handle, C.byref(r), C.byref(c)), "nrgb_mat_shape")
+        out = np.empty((r.value, c.value), order="F")
+        self._check(self.lib.nrgb_mat_download(self.h, handle, out.ctypes.data), "nrgb_mat_download")
+        return out
+
+    def mat_free(self, handle):
+        self._check(self.lib.nrgb_mat_free(self.h, handle), "nrgb_mat_free")
+
+    def run_begin(self):
+        self._check(self.lib.nrgb_run_begin(self.h), "nrgb_run_begin")
+
+    def step(self, dims, diag_terms, off_terms, rules):
+        """One NRG step (nrgb_step); rules: dict of the truncation fields.
+        Returns (z_handles, w_handles, kept, egs, zsums)."""
+        import numpy as np
+        nb = len(dims)
+        dim = (C.c_int * nb)(*dims)
+        dt = (DiagTerm * max(1, len(diag_terms)))(*diag_terms)
+        ot = (OffdiagTerm * max(1, len(off_terms)))(*off_terms)
+        plan = StepPlan(nb, dim, len(diag_terms), dt, len(off_terms), ot, rules["fixeps"], rules["keepenergy"],
+                        rules["keep"], rules["keepmin"], rules["safeguard"], rules["safeguardmax"],
+                        rules.get("keep_all", 0), rules["betabar"])
+        zh, wh, kept = (C.c_int * nb)(), (C.c_int * nb)(), (C.c_int * nb)()
+        egs = C.c_double()
+        zs = (C.c_double * (3 * nb))()
+        self._check(self.lib.nrgb_step(self.h, C.byref(plan), zh, wh, kept, C.byref(egs), zs), "nrgb_step")
+        return list(zh), list(wh), list(kept), egs.value, np.array(list(zs)).reshape(nb, 3)
+
+    def recalc(self, outs, terms):
+        n = len(outs)
+        o = (RecalcOut * max(1, n))(*outs)
+        t = (RecalcTerm * max(1, len(terms)))(*terms)
+        hs = (C.c_int * max(1, n))()
+        self._check(self.lib.nrgb_recalc(self.h, n, o, len(terms), t, hs), "nrgb_recalc")
+        return list(hs)[:n]
 
     def set_wait_limit(self, poll_log2: int):
         """Device barrier waits give up after 2**poll_log2 polls (default 23)."""

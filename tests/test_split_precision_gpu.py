@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "nrg", "siam_c4.npz")
 
 
-@pytest.mark.parametrize("slices", [8, 6])
+@pytest.mark.parametrize("slices", [8, 7])
 def test_split_precision_run_against_the_fp64_oracle(tmp_path, slices):
     import nrgb
     if not os.path.exists(GOLDEN):
