@@ -660,6 +660,74 @@ struct NrgDriver::Impl {
     expv_def.clear();
   }
 
+  // ---------------- transformation files ----------------
+  // unitary<N>: "NRGBU001", int32 N, int32 nblocks, then per block int32 Q,
+  // int32 SS, int32 dim, int32 0, the dim eigenvalues as returned by the
+  // eigensolver (before the ground-state shift) and the dim x dim
+  // eigenvectors (column-major, eigenvector r in column r); little endian.
+  std::string workdir;
+  int laststored = -1;
+  std::string unitary_fn(int N) const { return workdir + "/unitary" + std::to_string(N); }
+  void find_laststored() {
+    // init_laststored (src/nrg.cc:3512-3524)
+    laststored = -1;
+    if (!P.resume) return;
+    for (int N = Ninit; N < Nmax; ++N) {
+      std::ifstream f(unitary_fn(N), std::ios::binary);
+      if (f.good()) laststored = N;
+    }
+  }
+  void store_transformations(int N, const Step& S) {
+    std::vector<double> w, z;
+    std::ofstream f(unitary_fn(N), std::ios::binary);
+    if (!f) throw std::runtime_error("cannot open " + unitary_fn(N) + " for writing");
+    const int32_t hdr[2] = {N, (int32_t)S.blocks.size()};
+    f.write("NRGBU001", 8);
+    f.write(reinterpret_cast<const char*>(hdr), sizeof(hdr));
+    for (const auto& kv : S.blocks) {
+      const Block& b = kv.second;
+      w.resize(b.dim);
+      z.resize((size_t)b.dim * b.dim);
+      NRGB_CUDA(cudaMemcpyAsync(w.data(), b.w, b.dim * sizeof(double), cudaMemcpyDeviceToHost, st));
+      NRGB_CUDA(cudaMemcpyAsync(z.data(), b.Z, z.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+      NRGB_CUDA(cudaStreamSynchronize(st));
+      d2h += (w.size() + z.size()) * sizeof(double);
+      const int32_t bh[4] = {kv.first.first, kv.first.second, b.dim, 0};
+      f.write(reinterpret_cast<const char*>(bh), sizeof(bh));
+      f.write(reinterpret_cast<const char*>(w.data()), w.size() * sizeof(double));
+      f.write(reinterpret_cast<const char*>(z.data()), z.size() * sizeof(double));
+    }
+    if (!f) throw std::runtime_error("error writing " + unitary_fn(N));
+  }
+  void load_transformations(int N, Step& S) {
+    std::ifstream f(unitary_fn(N), std::ios::binary);
+    char magic[8];
+    int32_t hdr[2];
+    f.read(magic, 8);
+    f.read(reinterpret_cast<char*>(hdr), sizeof(hdr));
+    if (!f || memcmp(magic, "NRGBU001", 8) != 0 || hdr[0] != N)
+      throw std::runtime_error("not a transformation file of step " + std::to_string(N) + ": " + unitary_fn(N));
+    if (hdr[1] != (int32_t)S.blocks.size())
+      throw std::runtime_error(unitary_fn(N) + ": subspaces differ from this run's");
+    std::vector<double> w, z;
+    for (auto& kv : S.blocks) {
+      Block& b = kv.second;
+      int32_t bh[4];
+      f.read(reinterpret_cast<char*>(bh), sizeof(bh));
+      if (!f || bh[0] != kv.first.first || bh[1] != kv.first.second || bh[2] != b.dim)
+        throw std::runtime_error(unitary_fn(N) + ": subspaces differ from this run's");
+      w.resize(b.dim);
+      z.resize((size_t)b.dim * b.dim);
+      f.read(reinterpret_cast<char*>(w.data()), w.size() * sizeof(double));
+      f.read(reinterpret_cast<char*>(z.data()), z.size() * sizeof(double));
+      if (!f) throw std::runtime_error("error reading " + unitary_fn(N));
+      // pageable sources: the copies complete before the calls return
+      NRGB_CUDA(cudaMemcpy(b.w, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice));
+      NRGB_CUDA(cudaMemcpy(b.Z, z.data(), z.size() * sizeof(double), cudaMemcpyHostToDevice));
+      h2d += (w.size() + z.size()) * sizeof(double);
+    }
+  }
+
   // ---------------- sweep 1 ----------------
   void sweep1(Slab& persist) {
     std::map<Invar, Prev> prev;
@@ -764,10 +832,18 @@ struct NrgDriver::Impl {
       }
       sections["sweep1 setup"] += secs(ts);
       auto t0 = Clock::now();
-      NRGB_CUDA(assemble_launch(upload(ad), (int)ad.size(), upload(ao), (int)ao.size(), maxlen, maxrc, st));
-      launches += 2;
-      launches += syev->solve(sd, st);
-      eig_calls += 1;
+      if (P.resume && N <= laststored) {
+        // the step's eigen-decompositions from the previous run's file
+        // (nrg_do_diag, src/nrg.cc:2891-2895)
+        NRGB_CUDA(cudaStreamSynchronize(st));
+        load_transformations(N, S);
+      } else {
+        NRGB_CUDA(assemble_launch(upload(ad), (int)ad.size(), upload(ao), (int)ao.size(), maxlen, maxrc, st));
+        launches += 2;
+        launches += syev->solve(sd, st);
+        eig_calls += 1;
+        if (!P.removefiles) store_transformations(N, S);
+      }
       t_diag += secs(t0);
       sections["sweep1 diag"] += secs(t0);
       ts = Clock::now();
@@ -1482,6 +1558,8 @@ struct NrgDriver::Impl {
     if ((int)D.xi[0].size() - 1 != P.Nmax) throw std::runtime_error("length of coefficient table != Nmax");
     Nmax = P.Nmax;
     Ninit = P.Ninit;
+    workdir = wd;
+    find_laststored();
     if (Nmax <= Ninit) throw std::runtime_error("zero-bandwidth runs (Nmax == Ninit) are not supported");
     if (P.dm && P.T <= 0) throw std::runtime_error("density-matrix runs need T > 0");
     Slab persist(st);

@@ -56,6 +56,8 @@ void Params::read(const std::string& path) {
   I("prec_custom", prec_custom); I("prec_xy", prec_xy);
   B("calc0", calc0);
   I("gemm_slices", gemm_slices);
+  B("removefiles", removefiles);
+  B("resume", resume);
   unused = kv;
   // validateparameters (src/read-input.cc:6-36) and calculate_invariants
   if (keep <= 1) throw std::runtime_error("keep must be > 1");

@@ -39,6 +39,12 @@ struct Params {
   // INT8 slices per operand (this implementation's key; the reference has
   // no such parameter and reports it as unknown).
   int gemm_slices = 0;
+  // Transformation files (src/dmnrg.h:183-304, src/nrg.cc:3512-3524): with
+  // removefiles=false every step's eigen-decompositions are written to
+  // <workdir>/unitary<N>; with resume=true the steps that have such a file
+  // load it instead of diagonalising.  The file layout is this
+  // implementation's own (the reference writes boost archives).
+  bool removefiles = true, resume = false;
   int channels = 1;  // from the data file
 
   // Parse `path`; unknown keys are kept in `unused` (the reference reports them).
