@@ -1551,9 +1551,17 @@ struct NrgDriver::Impl {
     P.read(wd + "/param");
     D = DataFile();
     D.read(wd + "/data");
-    if (D.symtype != "QS") throw std::runtime_error("symmetry type " + D.symtype + " is not built (QS only)");
     P.channels = D.channels;
-    sym.reset(new SymmetryQS(D.channels));
+    if (D.symtype == "QS") {
+      sym.reset(new SymmetryQS(D.channels));
+    } else if (D.symtype == "QSZ") {
+      if (D.channels != 1) throw std::runtime_error("symmetry type QSZ: one channel is built");
+      if (!P.specd.empty() || !P.spect.empty() || !P.specs.empty())
+        throw std::runtime_error("symmetry type QSZ: spectral functions are not built");
+      sym.reset(new SymmetryQSZ());
+    } else {
+      throw std::runtime_error("symmetry type " + D.symtype + " is not built (QS, QSZ)");
+    }
     if (P.Nmax == 0) P.Nmax = D.Nmax;
     if ((int)D.xi[0].size() - 1 != P.Nmax) throw std::runtime_error("length of coefficient table != Nmax");
     Nmax = P.Nmax;

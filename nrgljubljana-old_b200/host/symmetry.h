@@ -178,4 +178,91 @@ class SymmetryQS : public Symmetry {
   std::vector<Invar> in_, qn_;
 };
 
+// QSZ plug-in: charge U(1) x spin-projection U(1), invariant subspaces
+// (Q, SSZ) with SSZ = 2 S_z (src/sym-QSZ.cc), one channel.  Every state is
+// its own multiplet (mult 1); both spin components of f^dag share one list of
+// matrix elements <I1|f^dag_sigma|I2>, I1 = I2 + (1, +-1) (the reference's
+// perchannel = 1 for QSZ, src/read-input.cc:67-74).
+//
+// Tables (coefnew/qsz/qsz-1ch-*.dat): combination i of a subspace I has the
+// ancestor I + In[i] and the new site in state i: empty, down, up, doubly
+// occupied (QN).  With the new site's operators to the left of the chain's,
+// |s_i, a> = c_i |a>, c = (1, f^dag_dn, f^dag_up, f^dag_up f^dag_dn):
+//  * hopping f^dag_N,s f_N+1,s (+ h.c.) between combinations i < j: the
+//    site's f_s takes c_j to c_i with sign +-1 and f^dag_N,s passes the n_i
+//    site electrons of c_i: (1,2) +1, (1,3) +1, (2,4) -1, (3,4) +1
+//    (qsz-1ch-offdiag.dat);
+//  * <f^dag_s> of the new site: up (I1 = Ip + (1, 1)): (3 <- 1) +1,
+//    (4 <- 2) +1 (qsz-1ch-spinupa.dat); down (I1 = Ip + (1, -1)): (2 <- 1)
+//    +1, (4 <- 3) -1 (qsz-1ch-spindowna.dat);
+//  * electrons of the new site per combination 0, 1, 1, 2 (qsz-1ch-diag.dat).
+// Thermodynamics columns <Sz^2>, <Sz>, <Q>, <Q^2> (calculate_TD,
+// src/sym-QSZ.cc:73-94).  Doublet and triplet operators (and with them the
+// spectral functions) are not provided for QSZ.
+class SymmetryQSZ : public Symmetry {
+ public:
+  SymmetryQSZ() {
+    in_ = {{1, 0}, {0, 1}, {0, -1}, {-1, 0}};
+    qn_ = {{-1, 0}, {0, -1}, {0, 1}, {1, 0}};
+  }
+  std::string name() const override { return "QSZ"; }
+  int combs() const override { return 4; }
+  const std::vector<Invar>& In() const override { return in_; }
+  const std::vector<Invar>& QN() const override { return qn_; }
+  int mult(const Invar&) const override { return 1; }
+  bool allowed(const Invar&) const override { return true; }
+  bool triangle(const Invar& a, const Invar& b, const Invar& c) const override {
+    return a.first == b.first + c.first && a.second == b.second + c.second;
+  }
+  Invar singlet() const override { return {0, 0}; }
+  Invar doublet() const override { return {1, 1}; }
+  Invar triplet() const override { return {0, 2}; }
+  std::vector<OffdiagTerm> offdiag(const Invar&) const override {
+    return {{1, 2, 0, 1.0}, {1, 3, 0, 1.0}, {2, 4, 0, -1.0}, {3, 4, 0, 1.0}};
+  }
+  std::vector<DiagTerm> diag() const override { return {{1, 0, 0.0}, {2, 0, 1.0}, {3, 0, 1.0}, {4, 0, 2.0}}; }
+  std::vector<RecalcTable> recalc_f(const Invar& Ip) const override {
+    const int qp = Ip.first, zp = Ip.second;
+    return {{{qp + 1, zp + 1}, 0, {{3, 1, 1.0}, {4, 2, 1.0}}},
+            {{qp + 1, zp - 1}, 0, {{2, 1, 1.0}, {4, 3, -1.0}}}};
+  }
+  std::vector<RecalcTable> recalc_doublet(const Invar&) const override {
+    throw std::runtime_error("QSZ: doublet operators are not built");
+  }
+  std::vector<RecalcTable> recalc_triplet(const Invar&) const override {
+    throw std::runtime_error("QSZ: triplet operators are not built");
+  }
+  double specdens_factor(const Invar&, const Invar&) const override {
+    throw std::runtime_error("QSZ: spectral functions are not built");
+  }
+  double dynsusc_factor(const Invar&, const Invar&) const override {
+    throw std::runtime_error("QSZ: spectral functions are not built");
+  }
+  std::vector<std::string> td_names() const override { return {"<Sz^2>", "<Sz>", "<Q>", "<Q^2>"}; }
+  std::vector<double> td_values(const std::vector<std::pair<Invar, const std::vector<double>*>>& blocks,
+                                double factor, double Z) const override {
+    std::vector<std::pair<Invar, double>> zs;
+    for (const auto& b : blocks) {
+      double sumZ = 0;
+      for (double x : *b.second) sumZ += exp(-factor * x);
+      zs.push_back({b.first, sumZ});
+    }
+    return td_values_sums(zs, Z);
+  }
+  std::vector<double> td_values_sums(const std::vector<std::pair<Invar, double>>& zsum, double Z) const override {
+    double trSZ = 0, trSZ2 = 0, trQ = 0, trQ2 = 0;
+    for (const auto& b : zsum) {
+      const double sz = 0.5 * b.first.second, q = b.first.first;
+      trSZ += b.second * sz;
+      trSZ2 += b.second * sz * sz;
+      trQ += b.second * q;
+      trQ2 += b.second * q * q;
+    }
+    return {trSZ2 / Z, trSZ / Z, trQ / Z, trQ2 / Z};
+  }
+
+ private:
+  std::vector<Invar> in_, qn_;
+};
+
 }  // namespace nrgb

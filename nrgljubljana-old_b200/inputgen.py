@@ -573,6 +573,89 @@ def write_data(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: int,
     return {"subspaces": len(subs), "gs_energy": gs, "scale0": sc0}
 
 
+def decompose_qsz(m: ClusterModel) -> List[Subspace]:
+    """Eigenstates per invariant subspace (Q, SSZ = 2 S_z) of the QSZ symmetry
+    (charge U(1) x spin-projection U(1), src/sym-QSZ.cc): every state of a
+    sector, no spin multiplets.  The Subspace field SS holds SSZ here."""
+    F = m.fock
+    _, Sz = _total_spin_ops(m)
+    ncharge = F.occ[:, [2 * o for o in m.charge_orbitals]].sum(1) + \
+        F.occ[:, [2 * o + 1 for o in m.charge_orbitals]].sum(1)
+    Q = ncharge - len(m.charge_orbitals)
+    ssz = np.round(np.diag(Sz) * 2).astype(int)
+    subs = []
+    for q in sorted(set(Q[m.basis_mask])):
+        for z2 in sorted(set(ssz[(Q == q) & m.basis_mask])):
+            idx = np.where((Q == q) & (ssz == z2) & m.basis_mask)[0]
+            Hs = m.H[np.ix_(idx, idx)]
+            Hs = 0.5 * (Hs + Hs.T)
+            e, w = np.linalg.eigh(Hs)
+            vec = np.zeros((F.dim, len(idx)))
+            vec[idx] = w
+            subs.append(Subspace(int(q), int(z2), e, vec))
+    return subs
+
+
+def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: int,
+                   xi: np.ndarray, zeta: np.ndarray, discretization: str = "Y") -> dict:
+    """Write a version-9 `data` file of the QSZ symmetry (one channel): the
+    sector energies, the matrix elements <I1|f^dag_sigma|I2> of the first chain
+    site for both spins in one list (I1 = I2 + (1, +-1); the reference keeps
+    one f list per channel for QSZ, src/read-input.cc:67-74, 131-145) and the
+    singlet operators.  Doublet and triplet operators are not written."""
+    if len(m.f_orbitals) != 1:
+        raise ValueError("QSZ data: one channel")
+    F = m.fock
+    subs = decompose_qsz(m)
+    smap = {(s.Q, s.SS): s for s in subs}
+    gs = min(s.energies[0] for s in subs)
+    sc0 = scale_factor(0, Lambda, z, discretization)
+    lines = ["# Input file for NRG Ljubljana (generated by inputgen.py)",
+             "# symtype QSZ",
+             "#!9",
+             "# Number of channels, chain sites, subspaces: ",
+             "%d %d %d" % (1, Nmax, len(subs)),
+             "# SCALE " + _fmt(sc0),
+             "# Energies (GS energy subtracted, multiplied by 1/SCALE):"]
+    for s in subs:
+        lines.append("%d %d" % (s.Q, s.SS))
+        lines.append("%d" % len(s.energies))
+        lines.append(" ".join(_fmt((e - gs) / sc0) for e in s.energies))
+    lines.append("# Irreducible matrix elements for Wilson chains:")
+    orb = m.f_orbitals[0]
+    f = {}
+    for (q2, z2), s2 in smap.items():
+        for spin, dz in ((0, +1), (1, -1)):
+            key1 = (q2 + 1, z2 + dz)
+            if key1 in smap:
+                f[(key1, (q2, z2))] = smap[key1].vectors.T @ F.cd(orb, spin) @ s2.vectors
+    lines.append("f 0 0")
+    lines.append("%d" % len(f))
+    for (k1, k2), M in f.items():
+        lines.append("%d %d %d %d" % (k1[0], k1[1], k2[0], k2[1]))
+        _write_matrix(lines, M)
+    lines.append("# GS energy in absolute units:")
+    lines.append("e")
+    lines.append(_fmt(gs))
+    lines.append("# Irreducible matrix elements for other operators:")
+    for name, op in m.singlet_ops.items():
+        lines.append("s" + name)
+        lines.append("%d" % len(smap))
+        for key, sub in smap.items():
+            lines.append("%d %d %d %d" % (key[0], key[1], key[0], key[1]))
+            _write_matrix(lines, sub.vectors.T @ op @ sub.vectors)
+    lines.append("# Discretization tables:")
+    lines.append("z")
+    lines.append("%d" % (len(xi) - 1))
+    lines.extend(_fmt(x) for x in xi)
+    lines.append("%d" % (len(zeta) - 1))
+    lines.extend(_fmt(x) for x in zeta)
+    lines.append("")
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines))
+    return {"subspaces": len(subs), "gs_energy": gs, "scale0": sc0}
+
+
 def write_param(path: str, params: Dict[str, object]) -> None:
     with open(path, "w") as fh:
         fh.write("[param]\n")
@@ -584,16 +667,22 @@ def write_param(path: str, params: Dict[str, object]) -> None:
 
 def make_siam(dirpath: str, U: float, eps_d: float, Gamma: float, Lambda: float,
               Nmax: int, z: float = 1.0, params: Dict[str, object] | None = None,
-              V: float | None = None, dps: int = 200, discretization: str = "Y") -> dict:
-    """Generate `data` and `param` for a QS single-impurity Anderson model on a
-    flat band (D=1) in directory `dirpath`.  V defaults to sqrt(2 Gamma/pi);
-    discretization Y, C or Z (wilson_chain_flat)."""
+              V: float | None = None, dps: int = 200, discretization: str = "Y",
+              symtype: str = "QS") -> dict:
+    """Generate `data` and `param` for a single-impurity Anderson model on a
+    flat band (D=1) in directory `dirpath`, symmetry QS or QSZ.  V defaults
+    to sqrt(2 Gamma/pi); discretization Y, C or Z (wilson_chain_flat)."""
     os.makedirs(dirpath, exist_ok=True)
     if V is None:
         V = math.sqrt(2.0 * Gamma / math.pi)
     xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps, discretization=discretization)
     m = siam_cluster(U, eps_d, V, zeta0=zeta[0])
-    info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, 1, discretization)
+    if symtype == "QSZ":
+        info = write_data_qsz(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, discretization)
+    elif symtype == "QS":
+        info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, 1, discretization)
+    else:
+        raise ValueError("symtype QS or QSZ")
     p = {"Lambda": Lambda, "z": z, "discretization": discretization}
     if params:
         p.update(params)

@@ -425,7 +425,7 @@ class StepRecord:
 
 
 class Oracle:
-    def __init__(self, workdir, threads=1, eigh_driver=None):
+    def __init__(self, workdir, threads=1, eigh_driver=None, spill_dir=None, progress=False):
         """threads: blocks diagonalised concurrently (OpenMP over blocks,
         src/nrg.cc:2484-2507), each with one BLAS thread; 1 leaves BLAS its
         own threads.  eigh_driver: "ev" (dsyev), "evd" or "evr" for every
@@ -436,6 +436,11 @@ class Oracle:
         self.P = read_params(os.path.join(workdir, "param"))
         self.threads = max(1, int(threads))
         self.eigh_driver = eigh_driver
+        # spill_dir: keep each step's eigenvectors in .npy files there,
+        # memory-mapped (the reference's unitary<N> files, src/dmnrg.h:183-304),
+        # for runs whose eigenvectors exceed the host memory
+        self.spill_dir = spill_dir
+        self.progress = progress
         if self.P["diag"] not in ("default", "dsyev", "dsyevr"):
             raise ValueError("Unknown diagonalization routine: %s" % self.P["diag"])
         self.timing = {}
@@ -773,6 +778,15 @@ class Oracle:
             if P["dumpannotated"]:
                 self.annotated.append((scale, totalenergy,
                                        sorted((float(x), I) for I, e in diag.items() for x in e.value)))
+            if self.spill_dir:
+                for I, e in diag.items():
+                    fn = os.path.join(self.spill_dir, "u%d_%d_%d.npy" % (N, I[0], I[1]))
+                    np.save(fn, e.vec)
+                    e.vec = np.load(fn, mmap_mode="r")
+            if self.progress:
+                print("oracle step %d: %d blocks, kept %d of %d" % (N, len(diag), sum(e.kept for e in diag.values()),
+                                                                   sum(len(e.value) for e in diag.values())),
+                      flush=True)
             rec = StepRecord(eig={I: Eig(value=e.value.copy(), vec=e.vec, shift=e.shift,
                                          absenergy=e.absenergy.copy(), kept=e.kept)
                                   for I, e in diag.items()},

@@ -2,7 +2,7 @@
 store their outputs as tests/golden/nrg/<case>.npz, with the sha256 of the
 generated `param`/`data` they were made from.
 
-    python tests/golden/make_nrg_goldens.py [case ...] [--threads N] [--driver ev|evd]
+    python tests/golden/make_nrg_goldens.py [case ...] [--threads N] [--driver ev|evd] [--spill]
 
 The oracle diagonalises with LAPACK dsyev by default (the reference's
 routine, src/diag.h:54-89); `--driver evd` uses dsyevd, which gives the same
@@ -30,15 +30,21 @@ def main():
     ap.add_argument("cases", nargs="*")
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     ap.add_argument("--driver", default="ev", choices=("ev", "evd"))
+    ap.add_argument("--spill", action="store_true", help="keep eigenvectors on disk (memory-mapped)")
+    ap.add_argument("--tmp", default=None, help="directory for the inputs and spilled eigenvectors")
     a = ap.parse_args()
     names = a.cases or sorted(cases.GOLDEN_CASES)
     os.makedirs(os.path.join(HERE, "nrg"), exist_ok=True)
     for name in names:
-        with tempfile.TemporaryDirectory() as tmp:
+        with tempfile.TemporaryDirectory(dir=a.tmp) as tmp:
             wd = cases.make_case(name, os.path.join(tmp, "in"))
             out = os.path.join(tmp, "out")
             t0 = time.time()
-            o = O.Oracle(wd, threads=a.threads, eigh_driver=a.driver)
+            spill = None
+            if a.spill:
+                spill = os.path.join(tmp, "spill")
+                os.makedirs(spill)
+            o = O.Oracle(wd, threads=a.threads, eigh_driver=a.driver, spill_dir=spill, progress=True)
             o.run(out)
             dt = time.time() - t0
             meta = {"case": name, "driver": a.driver, "threads": a.threads, "seconds": round(dt, 1)}
