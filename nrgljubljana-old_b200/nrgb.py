@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBPATH = os.path.join(HERE, "libnrgb.so")
+# NRGB_LIB overrides the library's path (for example to compare two builds)
+LIBPATH = os.environ.get("NRGB_LIB") or os.path.join(HERE, "libnrgb.so")
 
 EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
            "nrgb_syev_batched", "nrgb_syev_batched_dev", "nrgb_gemm_grouped_dev", "nrgb_gemm_grouped_split_dev",
