@@ -496,7 +496,7 @@ __host__ __device__ inline int trdc_ld(int n) { return n | 1; }
 // v and y (n each), one partial column dot per thread, one partial sum of
 // y^T v per warp of every CTA, 2 x 4 scalars.
 __host__ __device__ inline size_t trdc_smem_doubles(int n, int cl) {
-  return (size_t)((n + cl - 1) / cl) * trdc_ld(n) + 3 * (size_t)n + TRDC_NT + (size_t)cl * (TRDC_NT / 32) + 8;
+  return (size_t)((n + cl - 1) / cl) * trdc_ld(n) + 2 * (size_t)n + TRDC_NT + (size_t)cl * (TRDC_NT / 32) + 8;
 }
 
 // Active held columns up to this count take the warp-per-column-group
@@ -552,17 +552,6 @@ __device__ __forceinline__ void trdc_reflector(const TrdClProb& P, const double*
   }
 }
 
-// v of column cc (v[cc+1] = 1, v[i] = scal * col[i] below) into the buffer
-// `vbuf` of every CTA of the cluster, by the threads of the column's owner.
-template <int CL>
-__device__ __forceinline__ void trdc_push_v(const double* col, int cc, int n, double scal, double* vbuf, int tid) {
-  for (int i = cc + 1 + tid; i < n; i += TRDC_NT) {
-    const double x = (i == cc + 1) ? 1.0 : col[i] * scal;
-#pragma unroll 4
-    for (int q = 0; q < CL; ++q) trdc_at<CL>(vbuf, q)[i] = x;
-  }
-}
-
 // Unblocked Householder tridiagonalisation (the dsytd2 recurrence, lower)
 // of one block per cluster of CL CTAs.  The matrix lives in the CTAs'
 // shared memory, distributed by columns (CTA r holds the columns j with
@@ -596,10 +585,9 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
   constexpr int nwarps = TRDC_NT / 32;
   const int ncol = r < n ? (n - r + CL - 1) / CL : 0;
   extern __shared__ double sm[];
-  double* Acol = sm;                                      // ncol columns, ld lds
-  double* vb = Acol + (size_t)((n + CL - 1) / CL) * lds;  // 2 x n: v of even / odd columns,
-                                                          // written by the column's owner
-  double* y = vb + 2 * (size_t)n;                         // n (written by every CTA)
+  double* Acol = sm;                                     // ncol columns, ld lds
+  double* v = Acol + (size_t)((n + CL - 1) / CL) * lds;  // n
+  double* y = v + n;                                     // n (written by every CTA)
   double* ypart = y + n;                                 // TRDC_NT partial column dots
   double* part = ypart + TRDC_NT;                        // CL x nwarps parts of y^T v
   double* misc = part + CL * nwarps;                     // 2 x 4 reflector scalars
@@ -611,20 +599,19 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
   // every CTA of the cluster has started (and loaded) before any of them
   // touches another's shared memory
   trdc_sync<CL>();
-  if (n > 1 && r == 0) {
-    if (warp == 0) trdc_reflector<CL>(P, Acol, 0, n, misc, lane);
-    __syncthreads();
-    trdc_push_v<CL>(Acol, 0, n, misc[1], vb, tid);
-  }
+  if (n > 1 && r == 0 && warp == 0) trdc_reflector<CL>(P, Acol, 0, n, misc, lane);
   trdc_sync<CL>();
 
   for (int c = 0; c < n - 1; ++c) {
     const int o = c % CL;
     const double* mc = misc + (c & 1) * 4;
-    // ---- a: y_j for the columns held here, parts of y^T v (v of column c
-    // was pushed into every CTA by its owner before the last cluster barrier) ----
-    const double tc = mc[0];
-    double* v = vb + (size_t)(c & 1) * n;
+    // ---- a: v, y_j for the columns held here, parts of y^T v ----
+    const double tc = mc[0], scal = mc[1];
+    {
+      const double* ocol = trdc_at<CL>(Acol, o) + (size_t)(c / CL) * lds;
+      for (int i = c + 1 + tid; i < n; i += TRDC_NT) v[i] = (i == c + 1) ? 1.0 : ocol[i] * scal;
+    }
+    __syncthreads();
     // held columns after c: local indices l0 .. ncol-1
     const int l0 = (c + 1 - r + CL - 1) / CL > 0 ? (c + 1 - r + CL - 1) / CL : 0;
     const int nact = ncol > l0 ? ncol - l0 : 0;
@@ -754,20 +741,14 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
         }
       }
     }
-    if (own_next) {
+    if (own_next && warp == 0) {
       double* col = Acol + (size_t)l0 * lds;
-      if (warp == 0) {
-        if (tc != 0.0) {
-          const double vj = v[cn], wj = tc * y[cn] + a2 * v[cn];
-          for (int i = c + 1 + lane; i < n; i += 32) col[i] -= v[i] * wj + (tc * y[i] + a2 * v[i]) * vj;
-          __syncwarp();
-        }
-        trdc_reflector<CL>(P, col, cn, n, misc + (cn & 1) * 4, lane);
+      if (tc != 0.0) {
+        const double vj = v[cn], wj = tc * y[cn] + a2 * v[cn];
+        for (int i = c + 1 + lane; i < n; i += 32) col[i] -= v[i] * wj + (tc * y[i] + a2 * v[i]) * vj;
+        __syncwarp();
       }
-      // the whole owner CTA pushes v of column cn into every CTA (the other
-      // buffer: the CTAs may still be using this column's v)
-      __syncthreads();
-      trdc_push_v<CL>(col, cn, n, misc[(cn & 1) * 4 + 1], vb + (size_t)(cn & 1) * n, tid);
+      trdc_reflector<CL>(P, col, cn, n, misc + (cn & 1) * 4, lane);
     }
     trdc_sync<CL>();
   }
