@@ -482,7 +482,7 @@ struct NrgDriver::Impl {
         auto it = S.blocks.find(Ip);
         if (it == S.blocks.end()) continue;
         const Block& Bp = it->second;
-        if (!sym->triangle(I1, Ip, Iop)) continue;
+        if (!sym->connects(I1, Ip, Iop)) continue;
         Target t{{I1, Ip}, nst(B1), nst(Bp), {}};
         if (t.k1 > 0 && t.kp > 0) {
           for (const RecalcRow& r : tab.rows) {
@@ -493,7 +493,7 @@ struct NrgDriver::Impl {
             if (r1 == 0 || rp == 0) continue;
             auto ot = cold.find({IN1, INp});
             const bool cnt = ot != cold.end();
-            if (!sym->triangle(IN1, Iop, INp) && !cnt) continue;
+            if (!sym->connects(IN1, INp, Iop) && !cnt) continue;
             if (!cnt) throw std::runtime_error("recalc: cold.count(ININ) != 1");
             if (!std::isfinite(r.factor)) throw std::runtime_error("recalc: factor not finite");
             if (ot->second.rows < r1 || ot->second.cols < rp) throw std::runtime_error("recalc: operator too small");
@@ -1168,6 +1168,7 @@ struct NrgDriver::Impl {
     std::string name, prefix, type;  // type DMNRG or FDM
     char kind;                       // 'd' doublet (fermionic) or 't' triplet (bosonic)
     std::string op1, op2;
+    int spin = 0;                    // +1 / -1: spin-resolved (symmetries with a field), 0: all pairs
     double* full = nullptr;          // device [pos | neg]
     double* chain = nullptr;
   };
@@ -1198,15 +1199,21 @@ struct NrgDriver::Impl {
         if (dash == std::string::npos) continue;
         const std::string a = pair.substr(0, dash), b = pair.substr(dash + 1);
         if (!D.ops.count(kind) || !D.ops.at(kind).count(a) || !D.ops.at(kind).count(b)) continue;
-        for (const char* type : {"DMNRG", "FDM"}) {
-          if (std::string(type) == "DMNRG" && !P.dmnrg) continue;
-          if (std::string(type) == "FDM" && !P.fdm) continue;
-          Spec s{pair, prefix, type, kind, a, b};
-          s.full = persist.alloc(2 * grid.nbins);
-          s.chain = persist.alloc(2 * grid.nbins);
-          NRGB_CUDA(cudaMemsetAsync(s.full, 0, 2 * grid.nbins * sizeof(double), st));
-          spectra.push_back(s);
-        }
+        // spin-resolved spectra for the symmetries with a field: names get
+        // "-u" / "-d" (SDNAME, src/nrg.cc:1498-1505)
+        std::vector<int> spins = {0};
+        if (kind == 'd' && sym->isfield()) spins = {-1, 1};
+        for (int spin : spins)
+          for (const char* type : {"DMNRG", "FDM"}) {
+            if (std::string(type) == "DMNRG" && !P.dmnrg) continue;
+            if (std::string(type) == "FDM" && !P.fdm) continue;
+            Spec s{pair + (spin == 1 ? "-u" : spin == -1 ? "-d" : ""), prefix, type, kind, a, b};
+            s.spin = spin;
+            s.full = persist.alloc(2 * grid.nbins);
+            s.chain = persist.alloc(2 * grid.nbins);
+            NRGB_CUDA(cudaMemsetAsync(s.full, 0, 2 * grid.nbins * sizeof(double), st));
+            spectra.push_back(s);
+          }
       }
     };
     bin_e_dev = persist.alloc(grid.nbins);
@@ -1269,6 +1276,7 @@ struct NrgDriver::Impl {
               const Twoinvar II{bj.first, bi.first};
               auto a1 = o1.find(II), a2 = o2.find(II);
               if (a1 == o1.end() || a2 == o2.end()) continue;
+              if (sp.spin != 0 && !sym->check_spin(bj.first, bi.first, sp.spin)) continue;
               const double sf = sp.kind == 'd' ? sym->specdens_factor(bi.first, bj.first)
                                                : sym->dynsusc_factor(bi.first, bj.first);
               auto rp = R.find({bi.first, bi.first}), r1 = R.find({bj.first, bj.first});
@@ -1305,6 +1313,7 @@ struct NrgDriver::Impl {
               const Twoinvar II{bj.first, bi.first};
               auto a1 = o1.find(II), a2 = o2.find(II);
               if (a1 == o1.end() || a2 == o2.end()) continue;
+              if (sp.spin != 0 && !sym->check_spin(bj.first, bi.first, sp.spin)) continue;
               const double sf = sp.kind == 'd' ? sym->specdens_factor(bi.first, bj.first)
                                                : sym->dynsusc_factor(bi.first, bj.first);
               auto ri = R.find({bi.first, bi.first}), rj = R.find({bj.first, bj.first});
@@ -1556,8 +1565,8 @@ struct NrgDriver::Impl {
       sym.reset(new SymmetryQS(D.channels));
     } else if (D.symtype == "QSZ") {
       if (D.channels != 1) throw std::runtime_error("symmetry type QSZ: one channel is built");
-      if (!P.specd.empty() || !P.spect.empty() || !P.specs.empty())
-        throw std::runtime_error("symmetry type QSZ: spectral functions are not built");
+      if (!P.spect.empty() || !P.specs.empty())
+        throw std::runtime_error("symmetry type QSZ: only the spectral functions of doublet operators are built");
       sym.reset(new SymmetryQSZ());
     } else {
       throw std::runtime_error("symmetry type " + D.symtype + " is not built (QS, QSZ)");

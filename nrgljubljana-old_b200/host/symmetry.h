@@ -52,6 +52,16 @@ class Symmetry {
                                         double factor, double Z) const = 0;
   // Same from the Boltzmann sums sum_r e^(-factor E_r) of each block.
   virtual std::vector<double> td_values_sums(const std::vector<std::pair<Invar, double>>& zsum, double Z) const = 0;
+  // Symmetries with a spin-projection quantum number (a magnetic field is
+  // allowed) resolve fermionic spectral functions by spin: SPIN = +1 / -1
+  // pairs with SSZ(I1) - SSZ(Ip) = SPIN (isfield, check_SPIN, src/sym-QSZ.cc:26-33,
+  // src/nrg.cc:1770-1787).
+  virtual bool isfield() const { return false; }
+  virtual bool check_spin(const Invar&, const Invar&, int) const { return true; }
+  // Whether an operator of kind Iop can connect Ip to I1 (the triangle
+  // inequality for SU(2) symmetries; both spin components of a doublet for
+  // the spin-projection symmetries).
+  virtual bool connects(const Invar& I1, const Invar& Ip, const Invar& Iop) const { return triangle(I1, Ip, Iop); }
   static Invar combine(const Invar& a, const Invar& b) { return {a.first + b.first, a.second + b.second}; }
   static Invar inverse(const Invar& a) { return {-a.first, -a.second}; }
 };
@@ -197,8 +207,8 @@ class SymmetryQS : public Symmetry {
 //    +1, (4 <- 3) -1 (qsz-1ch-spindowna.dat);
 //  * electrons of the new site per combination 0, 1, 1, 2 (qsz-1ch-diag.dat).
 // Thermodynamics columns <Sz^2>, <Sz>, <Q>, <Q^2> (calculate_TD,
-// src/sym-QSZ.cc:73-94).  Doublet and triplet operators (and with them the
-// spectral functions) are not provided for QSZ.
+// src/sym-QSZ.cc:73-94).  Doublet operators and their spin-resolved
+// spectral functions are provided; triplet operators are not.
 class SymmetryQSZ : public Symmetry {
  public:
   SymmetryQSZ() {
@@ -226,15 +236,29 @@ class SymmetryQSZ : public Symmetry {
     return {{{qp + 1, zp + 1}, 0, {{3, 1, 1.0}, {4, 2, 1.0}}},
             {{qp + 1, zp - 1}, 0, {{2, 1, 1.0}, {4, 3, -1.0}}}};
   }
-  std::vector<RecalcTable> recalc_doublet(const Invar&) const override {
-    throw std::runtime_error("QSZ: doublet operators are not built");
+  // Doublet operators (d^dag_s of the impurity) recalculated through the new
+  // site: d^dag passes the n_i electrons of the site, rows (i, i) with sign
+  // (-1)^n_i, for the spin-up component (Ip = I1 - (1, 1)) and the spin-down
+  // one (Ip = I1 - (1, -1)) (qsz-1ch-doubletp.dat, qsz-1ch-doubletm.dat).
+  std::vector<RecalcTable> recalc_doublet(const Invar& I1) const override {
+    const int q1 = I1.first, z1 = I1.second;
+    const std::vector<RecalcRow> rows = {{1, 1, 1.0}, {2, 2, -1.0}, {3, 3, -1.0}, {4, 4, 1.0}};
+    return {{{q1 - 1, z1 - 1}, 0, rows}, {{q1 - 1, z1 + 1}, 0, rows}};
   }
   std::vector<RecalcTable> recalc_triplet(const Invar&) const override {
     throw std::runtime_error("QSZ: triplet operators are not built");
   }
-  double specdens_factor(const Invar&, const Invar&) const override {
-    throw std::runtime_error("QSZ: spectral functions are not built");
+  bool isfield() const override { return true; }
+  bool check_spin(const Invar& I1, const Invar& Ip, int spin) const override {
+    return I1.second - Ip.second == spin;
   }
+  bool connects(const Invar& I1, const Invar& Ip, const Invar& Iop) const override {
+    if (Iop == doublet()) return I1.first == Ip.first + 1 && abs(I1.second - Ip.second) == 1;
+    return triangle(I1, Ip, Iop);
+  }
+  // every state is its own multiplet: no degeneracy factor (the default of
+  // Symmetry::specdens_factor, src/symmetry.cc:170-173)
+  double specdens_factor(const Invar&, const Invar&) const override { return 1.0; }
   double dynsusc_factor(const Invar&, const Invar&) const override {
     throw std::runtime_error("QSZ: spectral functions are not built");
   }

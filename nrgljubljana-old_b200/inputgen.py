@@ -601,8 +601,9 @@ def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: in
     """Write a version-9 `data` file of the QSZ symmetry (one channel): the
     sector energies, the matrix elements <I1|f^dag_sigma|I2> of the first chain
     site for both spins in one list (I1 = I2 + (1, +-1); the reference keeps
-    one f list per channel for QSZ, src/read-input.cc:67-74, 131-145) and the
-    singlet operators.  Doublet and triplet operators are not written."""
+    one f list per channel for QSZ, src/read-input.cc:67-74, 131-145), the
+    singlet operators and the doublet operators (both spins in one list, like
+    f).  Triplet operators are not written."""
     if len(m.f_orbitals) != 1:
         raise ValueError("QSZ data: one channel")
     F = m.fock
@@ -644,6 +645,19 @@ def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: in
         for key, sub in smap.items():
             lines.append("%d %d %d %d" % (key[0], key[1], key[0], key[1]))
             _write_matrix(lines, sub.vectors.T @ op @ sub.vectors)
+    # doublet operators: <I1|a^dag_s|I2> for both spins in one list, as f
+    for name, orb2 in m.doublet_ops.items():
+        blocks = {}
+        for (q2, z2), s2 in smap.items():
+            for spin, dz in ((0, +1), (1, -1)):
+                key1 = (q2 + 1, z2 + dz)
+                if key1 in smap:
+                    blocks[(key1, (q2, z2))] = smap[key1].vectors.T @ F.cd(orb2, spin) @ s2.vectors
+        lines.append("d" + name)
+        lines.append("%d" % len(blocks))
+        for (k1, k2), M in blocks.items():
+            lines.append("%d %d %d %d" % (k1[0], k1[1], k2[0], k2[1]))
+            _write_matrix(lines, M)
     lines.append("# Discretization tables:")
     lines.append("z")
     lines.append("%d" % (len(xi) - 1))

@@ -4,8 +4,9 @@ Anderson model truncated by an energy cutoff (keepenergy, with the safeguard
 completing split multiplets) keeps the same states in both, so every
 thermodynamic column they share (<Sz^2>, <Q>, <Q^2>, <E>, <E^2>, C, F, S)
 must agree, <Sz> must vanish, the singlet expectation values must agree,
-and the QSZ energy flow must be the QS one with each level repeated over its
-spin projections."""
+the QSZ energy flow must be the QS one with each level repeated over its
+spin projections, and each spin component of the QSZ spectral function
+(spec_*_dens_A_d-A_d-u / -d, DM-NRG and FDM) must equal the QS one."""
 import collections
 import os
 
@@ -18,7 +19,8 @@ import nrg_cases as cases
 pytestmark = pytest.mark.gpu
 
 PARAMS = {"keep": 100000, "keepenergy": 6.0, "keepmin": 1, "T": 1e-4, "dumpannotated": 1, "dumpgroups": False,
-          "prec_td": 16, "prec_custom": 16, "dumpprecision": 16}
+          "prec_td": 16, "prec_custom": 16, "dumpprecision": 16, "fdm": True, "dmnrg": True,
+          "specd": "A_d-A_d", "bins": 40, "savebins": True, "broaden": False}
 
 
 @pytest.mark.parametrize("U,eps", [(0.1, -0.05), (0.3, -0.05)])
@@ -62,3 +64,14 @@ def test_qsz_matches_qs(tmp_path, U, eps):
             qq[q] += ss
         qz = collections.Counter(int(lab[0].split()[0]) for _, lab, _ in sz)
         assert qq == qz
+
+    for typ in ("DMNRG", "FDM"):
+        q = cases.read_bins(os.path.join(out["QS"], "spec_%s_dens_A_d-A_d.bin" % typ))
+        dq = dict(zip(q[:, 0], q[:, 1]))
+        wmax = max(abs(v) for v in dq.values())
+        for spin in ("u", "d"):
+            z = cases.read_bins(os.path.join(out["QSZ"], "spec_%s_dens_A_d-A_d-%s.bin" % (typ, spin)))
+            dz = dict(zip(z[:, 0], z[:, 1]))
+            keys = set(dq) | set(dz)
+            err = max(abs(dq.get(k, 0.0) - dz.get(k, 0.0)) for k in keys)
+            assert err <= 1e-8 * wmax, (typ, spin, err / wmax)
