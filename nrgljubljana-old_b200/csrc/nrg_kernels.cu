@@ -52,26 +52,65 @@ __global__ void gather_diag_kernel(const DiagGather* __restrict__ g, double* __r
     dst[G.dst_off + r] = G.src[(size_t)r * (G.ld + 1)];
 }
 
-__device__ __forceinline__ void bin_add(double* sbins, const BinGrid& g, double E, double w) {
-  // Bins::add / add_std (src/bins.h:102-131) with the positive/negative split
-  // of ChainSpectrumBinning::add.
-  double* b = sbins;
+// Bins::add / add_std (src/bins.h:102-131) with the positive/negative split
+// of ChainSpectrumBinning::add: the (up to two) bins of one peak and the
+// weights they receive; bins < 0 take nothing.
+__device__ __forceinline__ void bin_targets(const BinGrid& g, double E, double w, int& k0, double& v0, int& k1,
+                                            double& v1) {
+  k0 = k1 = -1;
+  v0 = v1 = 0.0;
+  int base = 0;
   if (E < 0.0) {
     E = -E;
-    b = sbins + g.nbins;
+    base = g.nbins;
   }
   if (fabs(w) < g.discard * E) return;
   const double pos = (log10(E) - g.l0) * g.bpd;
   const long idx = (long)pos;  // truncation toward zero, as the reference's long(pos)
   if (idx < 0) {
-    atomicAdd(&b[0], w);
+    k0 = base;
+    v0 = w;
   } else if (idx >= g.nbins - 1) {
-    atomicAdd(&b[g.nbins - 1], w);
+    k0 = base + g.nbins - 1;
+    v0 = w;
   } else {
     const double rem = pos - (double)idx;
-    atomicAdd(&b[idx], (1.0 - rem) * w);
-    atomicAdd(&b[idx + 1], rem * w);
+    k0 = base + (int)idx;
+    v0 = (1.0 - rem) * w;
+    k1 = k0 + 1;
+    v1 = rem * w;
   }
+}
+
+// Warp-level reduction of one contribution per lane into shared-memory bins:
+// lanes that hit the same bin are found with __match_any_sync, their values
+// summed by the group's lowest lane (shuffles over the group), and one atomic
+// add per distinct bin remains.  Every lane of the warp calls it.
+__device__ __forceinline__ void bin_add_warp(double* sbins, int k, double v) {
+  const unsigned peers = __match_any_sync(0xffffffffu, k);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  double sum = 0.0;
+  for (unsigned m = peers; m; m &= m - 1) {
+    const double x = __shfl_sync(peers, v, __ffs(m) - 1);
+    sum += x;
+  }
+  if (lane == leader && k >= 0 && sum != 0.0) atomicAdd(&sbins[k], sum);
+}
+
+// One peak per lane (active lanes only) into the shared-memory bins, with
+// the warp-level reduction.  Every lane of the warp calls it.
+__device__ __forceinline__ void bin_add(double* sbins, const BinGrid& g, double E, double w, bool active) {
+  int k0, k1;
+  double v0, v1;
+  if (active) {
+    bin_targets(g, E, w, k0, v0, k1, v1);
+  } else {
+    k0 = k1 = -1;
+    v0 = v1 = 0.0;
+  }
+  bin_add_warp(sbins, k0, v0);
+  bin_add_warp(sbins, k1, v1);
 }
 
 __device__ __forceinline__ void flush_bins(const double* sbins, double* bins, int nb2) {
@@ -97,15 +136,24 @@ __global__ void __launch_bounds__(SPEC_NT) spec_dmnrg_kernel(const SpecDmnrgPair
   const long total = (long)P.dim1 * P.dimp;
   const long e0 = (long)blockIdx.x * SPEC_PER_CTA;
   const long e1 = min(total, e0 + SPEC_PER_CTA);
-  for (long e = e0 + threadIdx.x; e < e1; e += SPEC_NT) {
-    const int rj = (int)(e % P.dim1), rm = (int)(e / P.dim1);
-    const double dE = P.E1[rj] - P.Ep[rm];
-    const double a = fabs(dE);
-    if (a < Emin || a > Emax) continue;
-    const size_t io = (size_t)rj + (size_t)rm * P.ldo;
-    const size_t is = (size_t)rj + (size_t)rm * P.dim1;
-    const double w = P.sf * (P.SA[is] * P.op1[io] + msign * P.SB[is] * P.op2[io]);
-    bin_add(sbins, g, scale * dE, w);
+  // the loop runs the same number of rounds in every lane of a warp, so the
+  // warp-level binning sees whole warps
+  for (long e00 = e0; e00 < e1; e00 += SPEC_NT) {
+    const long e = e00 + threadIdx.x;
+    bool on = e < e1;
+    double dE = 0.0, w = 0.0;
+    if (on) {
+      const int rj = (int)(e % P.dim1), rm = (int)(e / P.dim1);
+      dE = P.E1[rj] - P.Ep[rm];
+      const double a = fabs(dE);
+      on = !(a < Emin || a > Emax);
+      if (on) {
+        const size_t io = (size_t)rj + (size_t)rm * P.ldo;
+        const size_t is = (size_t)rj + (size_t)rm * P.dim1;
+        w = P.sf * (P.SA[is] * P.op1[io] + msign * P.SB[is] * P.op2[io]);
+      }
+    }
+    bin_add(sbins, g, scale * dE, w, on);
   }
   flush_bins(sbins, bins, nb2);
 }
@@ -121,27 +169,39 @@ __global__ void __launch_bounds__(SPEC_NT) spec_fdm_kernel(const SpecFdmPair* __
   const long total = (long)P.allj * P.alli;
   const long e0 = (long)blockIdx.x * SPEC_PER_CTA;
   const long e1 = min(total, e0 + SPEC_PER_CTA);
-  for (long e = e0 + threadIdx.x; e < e1; e += SPEC_NT) {
-    const int j = (int)(e % P.allj), i = (int)(e / P.allj);
-    const size_t io = (size_t)j + (size_t)i * P.ldo;
-    const double o1 = P.op1[io];
-    const double Ej = P.Ej[j], Ei = P.Ei[i];
-    const double dE = Ej - Ei;
-    const bool idisc = i >= P.reti, jdisc = j >= P.retj;
-    // greater correlation function
-    if (idisc) {
-      bin_add(sbins, g, dE, P.sf * o1 * P.op2[io] * wnf * exp(-Ei / T));          // A3, A2
-    } else if (jdisc) {
-      bin_add(sbins, g, dE, P.sf * o1 * P.O2R[(size_t)j + (size_t)i * P.allj]);  // A1
+  for (long e00 = e0; e00 < e1; e00 += SPEC_NT) {
+    const long e = e00 + threadIdx.x;
+    double dE = 0.0, wg = 0.0, wl = 0.0;
+    bool ong = false, onl = false;
+    if (e < e1) {
+      const int j = (int)(e % P.allj), i = (int)(e / P.allj);
+      const size_t io = (size_t)j + (size_t)i * P.ldo;
+      const double o1 = P.op1[io];
+      const double Ej = P.Ej[j], Ei = P.Ei[i];
+      dE = Ej - Ei;
+      const bool idisc = i >= P.reti, jdisc = j >= P.retj;
+      // greater correlation function
+      if (idisc) {
+        wg = P.sf * o1 * P.op2[io] * wnf * exp(-Ei / T);  // A3, A2
+        ong = true;
+      } else if (jdisc) {
+        wg = P.sf * o1 * P.O2R[(size_t)j + (size_t)i * P.allj];  // A1
+        ong = true;
+      }
+      // lesser correlation function
+      if (idisc && jdisc) {
+        wl = P.sf * o1 * P.op2[io] * msign * wnf * exp(-Ej / T);  // B3
+        onl = true;
+      } else if (idisc && !jdisc) {
+        wl = P.sf * o1 * P.RO2[(size_t)j + (size_t)i * P.retj] * msign;  // B2
+        onl = true;
+      } else if (!idisc && jdisc) {
+        wl = P.sf * o1 * P.op2[io] * msign * wnf * exp(-Ej / T);  // B1
+        onl = true;
+      }
     }
-    // lesser correlation function
-    if (idisc && jdisc) {
-      bin_add(sbins, g, dE, P.sf * o1 * P.op2[io] * msign * wnf * exp(-Ej / T));  // B3
-    } else if (idisc && !jdisc) {
-      bin_add(sbins, g, dE, P.sf * o1 * P.RO2[(size_t)j + (size_t)i * P.retj] * msign);  // B2
-    } else if (!idisc && jdisc) {
-      bin_add(sbins, g, dE, P.sf * o1 * P.op2[io] * msign * wnf * exp(-Ej / T));  // B1
-    }
+    bin_add(sbins, g, dE, wg, ong);
+    bin_add(sbins, g, dE, wl, onl);
   }
   flush_bins(sbins, bins, nb2);
 }
