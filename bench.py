@@ -732,6 +732,57 @@ def run_split_micro(edge, slices, nprob):
     return 0
 
 
+def run_configs(args):
+    """Wall time of one run of each workload through nrgb_run on the GPU
+    (batched eigensolves per step; one eigensolver call per block; split
+    precision where it applies) and of the CPU oracle on the host cores
+    (faster of the two settings, diag=dsyevr) where that fits in minutes.
+    Prints one JSON object."""
+    import nrgb
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import nrg_cases as cases
+    cores = os.cpu_count() or 1
+    out = {"cores": cores}
+    tmp = tempfile.mkdtemp(prefix="nrgb_cfg_")
+    try:
+        for name, cpu in (("siam_nmax30", True), ("siam_c4", True), ("kondo2ch_full", False)):
+            wd = cases.make_case(name, os.path.join(tmp, name))
+            rec = {}
+            for mode, key in ((0, "gpu_batched_s"), (1, "gpu_per_block_s")):
+                ctx = nrgb.Context(0)
+                ctx.set_eig_mode(mode)
+                od = os.path.join(tmp, name + "_out%d" % mode)
+                os.makedirs(od, exist_ok=True)
+                t0 = time.perf_counter()
+                ctx.run(wd, od)
+                rec[key] = time.perf_counter() - t0
+                ctx.close()
+            if name == "siam_c4":
+                import shutil as _sh
+                wd2 = os.path.join(tmp, name + "_split")
+                _sh.copytree(wd, wd2)
+                with open(os.path.join(wd2, "param"), "a") as fh:
+                    fh.write("gemm_slices=8\n")
+                ctx = nrgb.Context(0)
+                od = os.path.join(tmp, name + "_outsplit")
+                os.makedirs(od, exist_ok=True)
+                t0 = time.perf_counter()
+                ctx.run(wd2, od)
+                rec["gpu_batched_split8_s"] = time.perf_counter() - t0
+                ctx.close()
+            if cpu and not args.no_cpu_baseline:
+                import serve
+                req = serve.Request(z=1.0, eps_d=0.0, keep=0, workdir=wd, outdir=os.path.join(tmp, name + "_cpu"))
+                with open(os.path.join(wd, "param"), "a") as fh:
+                    fh.write("diag=dsyevr\n")
+                rec["cpu_oracle_s"] = oracle_run(req, "omp_blocks", cores)
+            out[name] = rec
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_ncu_small(nmax):
     """Small profiling case (no torch on the GPU): 12 blocks with sizes up to
     `nmax` and their 72 operators through the host-buffer C ABI, twice."""
@@ -775,6 +826,8 @@ def main():
     ap.add_argument("--split-micro", type=int, default=0,
                     help="time the split-precision grouped GEMM against FP64 on problems of this edge")
     ap.add_argument("--slices", type=int, default=8)
+    ap.add_argument("--configs", action="store_true",
+                    help="time one run of each workload on the GPU and (where it fits) on the CPU oracle")
     ap.add_argument("--nprob", type=int, default=4)
     ap.add_argument("--ncu-small", type=int, default=0,
                     help="run only the small profiling case with blocks up to this size (no torch GPU work)")
@@ -787,6 +840,8 @@ def main():
         return run_ncu_small(args.ncu_small)
     if args.split_micro:
         return run_split_micro(args.split_micro, args.slices, args.nprob)
+    if args.configs:
+        return run_configs(args)
     if args.micro:
         return run_micro_only(args)
     rank = int(os.environ.get("RANK", "0"))
