@@ -56,7 +56,7 @@ WAVE = 32           # requests per step (one z value x 32 eps_d)
 LOAD = 0.85         # Poisson rate for the latency pass, as a fraction of capacity
 LOAD_LOW = 0.5      # second latency pass, well below capacity
 LAT_RUNS = 64       # requests in the latency pass
-MAX_RUNS = 16       # worker slots of the server (12 / 16 / 20 on one box: 27.3k / 33.0k / 35.7k runs/hour, p50 1.13 / 1.13 / 1.52 s)
+MAX_RUNS = 16       # worker slots of the server: 12..32 measured 16.7k-35.7k runs/hour on shared boxes, host load dominating
 
 # microbenchmark: 40 dense blocks per step, 6 operators per block pair
 NBLOCKS = 40
