@@ -783,6 +783,27 @@ def run_configs(args):
     return 0
 
 
+def run_one_case(name):
+    """One NRG run of a test workload (tests/nrg_cases.py) through nrgb_run,
+    for profiling the whole step (assembly, eigensolver, truncation,
+    recalculation, density matrices, spectra)."""
+    import nrgb
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import nrg_cases as cases
+    tmp = tempfile.mkdtemp(prefix="nrgb_one_")
+    try:
+        wd = cases.make_case(name, os.path.join(tmp, "in"))
+        od = os.path.join(tmp, "out")
+        os.makedirs(od)
+        ctx = nrgb.Context(0)
+        st = ctx.run(wd, od)
+        ctx.close()
+        print(json.dumps({"case": name, "wall_s": st["wall_s"], "launches": st["launches"]}), flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
 def run_ncu_small(nmax):
     """Small profiling case (no torch on the GPU): 12 blocks with sizes up to
     `nmax` and their 72 operators through the host-buffer C ABI, twice."""
@@ -826,6 +847,7 @@ def main():
     ap.add_argument("--split-micro", type=int, default=0,
                     help="time the split-precision grouped GEMM against FP64 on problems of this edge")
     ap.add_argument("--slices", type=int, default=8)
+    ap.add_argument("--one-run", default="", help="one nrgb_run of a test workload (profiling)")
     ap.add_argument("--configs", action="store_true",
                     help="time one run of each workload on the GPU and (where it fits) on the CPU oracle")
     ap.add_argument("--nprob", type=int, default=4)
@@ -842,6 +864,8 @@ def main():
         return run_split_micro(args.split_micro, args.slices, args.nprob)
     if args.configs:
         return run_configs(args)
+    if args.one_run:
+        return run_one_case(args.one_run)
     if args.micro:
         return run_micro_only(args)
     rank = int(os.environ.get("RANK", "0"))
