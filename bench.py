@@ -20,6 +20,11 @@ steps serve the first 128 requests of the 256-run stream.
   plain      the same requests one after another through nrgb_run, with one
              batched eigensolver call per step and with one call per block
              (the reference's per-subspace dsyev structure), sampled per Nkeep
+  split8     the same stream again with the products of the recalculations
+             and density matrices in split precision (gemm_slices=8: INT8
+             slices on the tensor cores), all queued at t = 0, with the
+             largest per-bin relative difference of its spectra from the
+             FP64 pass (bins above 1e-6 of each spectrum's largest)
   microbench the batched eigensolve + recalc step of 40 dense blocks of size
              16..4096 (log-uniform), batched against per-block solver calls,
              with the panel kernel's roofline
@@ -240,6 +245,25 @@ def one_per_keep(reqs):
     return sorted(out, key=lambda r: r.keep)
 
 
+def spectra_rel_err(ref_reqs, reqs):
+    """Largest relative difference per bin (bins above 1e-6 of each
+    spectrum's largest) between the .bin spectra of two passes of the same
+    requests."""
+    worst = 0.0
+    for a, b in zip(ref_reqs, reqs):
+        for name in os.listdir(a.outdir):
+            if not name.endswith(".bin"):
+                continue
+            x = np.fromfile(os.path.join(a.outdir, name), dtype="<f8").reshape(-1, 2)
+            y = np.fromfile(os.path.join(b.outdir, name), dtype="<f8").reshape(-1, 2)
+            dx, dy = dict(zip(x[:, 0], x[:, 1])), dict(zip(y[:, 0], y[:, 1]))
+            wmax = max(abs(v) for v in dx.values()) if dx else 0.0
+            for k, v in dx.items():
+                if abs(v) >= 1e-6 * wmax and v != 0.0:
+                    worst = max(worst, abs(dy.get(k, 0.0) - v) / abs(v))
+    return worst
+
+
 def bench_config(reqs):
     """The workload description both arms print (identical, so that the two
     lines describe the same configuration)."""
@@ -335,6 +359,20 @@ def run_ours(args, rank, world):
         # (near capacity a busy host can leave the server short of the
         # arrival rate, and p99 then measures the growing queue)
         latlow = serve.serve(srv, lat_low, LOAD_LOW * len(reqs) / res["span_s"])
+        # ---- the same stream in split precision (INT8-slice products, 8
+        # slices), all queued at t = 0, and its spectra against the FP64 pass ----
+        split = None
+        if not args.no_split:
+            sreqs = serve.prepare(copy.deepcopy(reqs), os.path.join(tmp, "split"))
+            for r in sreqs:
+                with open(os.path.join(r.workdir, "param"), "a") as fh:
+                    fh.write("gemm_slices=8\n")
+            sres = serve.serve(srv, sreqs, 0.0)
+            sspan = sres["span_s"]
+            if dist:
+                sspan = max_over_ranks(dist, [sspan], dev)[0]
+            split = {"value": replica_value(world, len(sreqs), sspan),
+                     "max_spectra_rel_err": spectra_rel_err(reqs, sreqs)}
         cnt = srv.counters()
         srv.close()
         # ---- plain: one run at a time (batched per step, and per block) ----
@@ -386,6 +424,9 @@ def run_ours(args, rank, world):
                     "plain_batched_runs_per_hour": plain_rate,
                     "served_over_per_block": value / world / per_block_rate,
                     "served_over_plain_batched": value / world / plain_rate,
+                    **({"served_split8_runs_per_hour": split["value"],
+                        "served_split8_over_per_block": split["value"] / world / per_block_rate,
+                        "split8_max_spectra_rel_err": split["max_spectra_rel_err"]} if split else {}),
                     "server_slots": args.max_runs},
             "gpu_launches": int(launches),
             "roofline": roof,
@@ -840,6 +881,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=40.0, help="seconds of oracle work per reference step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-micro", action="store_true", help="skip the 40-block microbenchmark")
+    ap.add_argument("--no-split", action="store_true", help="skip the split-precision pass of the stream")
     ap.add_argument("--micro-steps", type=int, default=20, help="steps of the 40-block microbenchmark")
     ap.add_argument("--detail", default="", help="also write the line and its details to this JSON file")
     ap.add_argument("--micro", action="store_true", help="run only the 40-block microbenchmark")

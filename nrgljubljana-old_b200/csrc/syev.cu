@@ -757,17 +757,281 @@ __global__ void __launch_bounds__(TRDC_NT) trd_cluster_kernel(const TrdClProb* _
   trdc_sync<CL>();
 }
 
+// Threads of a CTA of the one-barrier kernel (8 warps; 16 measured slower,
+// and so did splitting the rank-2 update into column x row-segment tasks).
+constexpr int TRDC1_NT = 256;
+// Rows of the next column each thread of the one-barrier kernel reads from
+// its owner before the rank-2 update and finishes after it.
+constexpr int TRDC1_ROWS = 4;
+
+// Doubles of dynamic shared memory of the one-barrier kernel: the held
+// columns, v, the running copy of the next column, y twice (alternating by
+// column parity), one partial column dot per thread, the parts of y^T v
+// twice, one partial norm per warp, scalars.
+__host__ __device__ inline size_t trdc1_smem_doubles(int n, int cl) {
+  return (size_t)((n + cl - 1) / cl) * trdc_ld(n) + 4 * (size_t)n + TRDC1_NT + 2 * (size_t)cl * (TRDC1_NT / 32) +
+         (TRDC1_NT / 32) + 8;
+}
+
+
+
+// The same recurrence with one cluster barrier per column.  Every CTA keeps
+// its own copy of the column being reduced and forms each reflector itself
+// (all CTAs run the same arithmetic on the same values, so they agree to the
+// bit); the owner of a column therefore never broadcasts it, and the second
+// cluster barrier of trd_cluster_kernel is gone.  Per column c:
+//   a. beta, tau and v of column c from the local copy (the norm's partial
+//      sums were left by step c-1); y_j of the held columns j > c into
+//      every CTA's y buffer of this parity, parts of y^T v likewise; cluster
+//      barrier;
+//   b. every CTA reads column c+1 from its owner's shared memory (which the
+//      owner no longer updates from this step on), applies this step's
+//      rank-2 correction to it and leaves the partial norms for step c+1;
+//      the held columns j > c+1 take the rank-2 update; CTA barrier.
+// y and the parts alternate by parity: a CTA writes step c+1's values only
+// after the cluster barrier of step c+1, which every CTA reaches after it has
+// read step c-1's.  Output as trd_cluster_kernel.
+template <int CL>
+__global__ void __launch_bounds__(TRDC1_NT) trd_cluster1_kernel(const TrdClProb* __restrict__ probs) {
+  int r = 0;
+  if constexpr (CL > 1) r = (int)cooperative_groups::this_cluster().block_rank();
+  const TrdClProb P = probs[blockIdx.x / CL];
+  const int n = P.n;
+  const size_t ld = (size_t)P.ld;
+  const int lds = trdc_ld(n);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int nwarps = TRDC1_NT / 32;
+  const int ncol = r < n ? (n - r + CL - 1) / CL : 0;
+  extern __shared__ double sm[];
+  double* Acol = sm;                                     // ncol columns, ld lds
+  double* v = Acol + (size_t)((n + CL - 1) / CL) * lds;  // n
+  double* cur = v + n;                                   // n: column c (rows c .. n-1)
+  double* ybuf = cur + n;                                // 2 x n (written by every CTA)
+  double* ypart = ybuf + 2 * (size_t)n;                  // TRDC1_NT partial column dots
+  double* pbuf = ypart + TRDC1_NT;                        // 2 x CL x nwarps parts of y^T v
+  double* psq = pbuf + 2 * CL * nwarps;                  // nwarps partial norms
+
+  for (int l = 0; l < ncol; ++l) {
+    const double* src = P.A + (size_t)(r + l * CL) * ld;
+    for (int i = tid; i < n; i += TRDC1_NT) Acol[(size_t)l * lds + i] = src[i];
+  }
+  // every CTA of the cluster has loaded before any of them reads another's
+  // shared memory; then column 0 from CTA 0
+  trdc_sync<CL>();
+  {
+    const double* c0 = trdc_at<CL>(Acol, 0);
+    double sq = 0.0;
+    for (int i = tid; i < n; i += TRDC1_NT) {
+      const double x = c0[i];
+      cur[i] = x;
+      if (i >= 2) sq += x * x;
+    }
+    sq = warp_sum(sq);
+    if (lane == 0) psq[warp] = sq;
+  }
+  __syncthreads();
+
+  for (int c = 0; c < n - 1; ++c) {
+    double* y = ybuf + (size_t)(c & 1) * n;
+    double* part = pbuf + (c & 1) * CL * nwarps;
+    // ---- a: reflector of column c, v, y_j for the columns held here ----
+    double ss = 0.0;
+#pragma unroll
+    for (int q = 0; q < nwarps; ++q) ss += psq[q];
+    const double alpha = cur[c + 1];
+    double beta = alpha, tc = 0.0, scal = 0.0;
+    if (ss != 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + ss), alpha);
+      tc = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    if (r == 0 && tid == 0) {
+      P.d[c] = cur[c];
+      P.e[c] = beta;
+      P.tau[c] = tc;
+    }
+    const bool own = r == c % CL;
+    for (int i = c + 1 + tid; i < n; i += TRDC1_NT) {
+      const double vi = (i == c + 1) ? 1.0 : cur[i] * scal;
+      v[i] = vi;
+      if (own && i >= c + 2) P.A[i + (size_t)c * ld] = vi;
+    }
+    __syncthreads();
+    // held columns after c: local indices l0 .. ncol-1
+    const int l0 = (c + 1 - r + CL - 1) / CL > 0 ? (c + 1 - r + CL - 1) / CL : 0;
+    const int nact = ncol > l0 ? ncol - l0 : 0;
+    double sp = 0.0;
+    if (nact <= TRDC_WARPCOL_MAX) {
+      for (int t0 = warp; t0 < nact; t0 += 4 * nwarps) {
+        const double* a[4];
+        bool on[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int t = t0 + k * nwarps;
+          on[k] = t < nact;
+          a[k] = Acol + (size_t)(l0 + (on[k] ? t : t0)) * lds;
+        }
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = c + 1 + lane; i < n; i += 32) {
+          const double vi = v[i];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc[k] += a[k][i] * vi;
+        }
+#pragma unroll
+        for (int o2 = 16; o2 > 0; o2 >>= 1) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o2);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if (!on[k]) continue;
+          const int j = r + (l0 + t0 + k * nwarps) * CL;
+          if (lane < CL) trdc_at<CL>(y, lane)[j] = acc[k];
+          sp += acc[k] * v[j];
+        }
+      }
+    } else {
+      const int chunks = (nact + 31) >> 5;
+      const int segs = max(1, nwarps / chunks);
+      if (warp < chunks * segs) {
+        const int ch = warp % chunks, sg = warp / chunks;
+        const int m = n - c - 1;
+        const int per = (m + segs - 1) / segs;
+        const int i0 = c + 1 + sg * per, i1 = min(n, i0 + per);
+        const int t = ch * 32 + lane;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        if (t < nact) {
+          const double* a = Acol + (size_t)(l0 + t) * lds;
+          int i = i0;
+          for (; i + 3 < i1; i += 4) {
+            s0 += a[i] * v[i];
+            s1 += a[i + 1] * v[i + 1];
+            s2 += a[i + 2] * v[i + 2];
+            s3 += a[i + 3] * v[i + 3];
+          }
+          for (; i < i1; ++i) s0 += a[i] * v[i];
+        }
+        ypart[sg * (chunks * 32) + t] = (s0 + s1) + (s2 + s3);
+      }
+      __syncthreads();
+      for (int t = tid; t < nact; t += TRDC1_NT) {
+        double yj = 0.0;
+        for (int sg = 0; sg < segs; ++sg) yj += ypart[sg * (chunks * 32) + t];
+        const int j = r + (l0 + t) * CL;
+#pragma unroll
+        for (int q = 0; q < CL; ++q) trdc_at<CL>(y, q)[j] = yj;
+        sp += yj * v[j];
+      }
+      sp = warp_sum(sp);
+    }
+    if (lane < CL) trdc_at<CL>(part, lane)[r * nwarps + warp] = sp;
+    trdc_sync<CL>();
+    // ---- b: column c+1 from its owner, the rank-2 update ----
+    const int cn = c + 1;
+    double xr[TRDC1_ROWS];
+    {
+      const double* ocol = trdc_at<CL>(Acol, cn % CL) + (size_t)(cn / CL) * lds;
+#pragma unroll
+      for (int k = 0; k < TRDC1_ROWS; ++k) {
+        const int i = cn + tid + k * TRDC1_NT;
+        xr[k] = i < n ? ocol[i] : 0.0;
+      }
+    }
+    double ytv = 0.0;
+    for (int q = lane; q < CL * nwarps; q += 32) ytv += part[q];
+    ytv = warp_sum(ytv);
+    const double a2 = -0.5 * tc * tc * ytv;
+    // held columns after c+1: local indices l1 .. ncol-1
+    const int l1 = (c + 2 - r + CL - 1) / CL > 0 ? (c + 2 - r + CL - 1) / CL : 0;
+    if (tc != 0.0) {
+      for (int l = l1 + 4 * warp; l < ncol; l += 4 * nwarps) {
+        const int nl = min(4, ncol - l);
+        double vj[4], wj[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int j = r + (l + min(k, nl - 1)) * CL;
+          vj[k] = v[j];
+          wj[k] = tc * y[j] + a2 * v[j];
+        }
+        double* a0 = Acol + (size_t)l * lds;
+        int i = c + 1 + lane;
+        for (; i + 32 < n; i += 64) {
+          const double v0 = v[i], v1 = v[i + 32];
+          const double w0 = tc * y[i] + a2 * v0, w1 = tc * y[i + 32] + a2 * v1;
+          double x[8];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            x[k] = k < nl ? a0[(size_t)k * lds + i] : 0.0;
+            x[4 + k] = k < nl ? a0[(size_t)k * lds + i + 32] : 0.0;
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            x[k] -= v0 * wj[k] + w0 * vj[k];
+            x[4 + k] -= v1 * wj[k] + w1 * vj[k];
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (k < nl) {
+              a0[(size_t)k * lds + i] = x[k];
+              a0[(size_t)k * lds + i + 32] = x[4 + k];
+            }
+        }
+        if (i < n) {
+          const double v0 = v[i];
+          const double w0 = tc * y[i] + a2 * v0;
+          double x[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) x[k] = k < nl ? a0[(size_t)k * lds + i] : 0.0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) x[k] -= v0 * wj[k] + w0 * vj[k];
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (k < nl) a0[(size_t)k * lds + i] = x[k];
+        }
+      }
+    }
+    {
+      // column c+1 after this step (rows c+1 .. n-1) and its partial norm
+      // over rows c+3 .. n-1 (v[c+1] = 1)
+      const double wn = tc * y[cn] + a2;
+      double sq = 0.0;
+#pragma unroll
+      for (int k = 0; k < TRDC1_ROWS; ++k) {
+        const int i = cn + tid + k * TRDC1_NT;
+        if (i < n) {
+          double x = xr[k];
+          if (tc != 0.0) x -= v[i] * wn + (tc * y[i] + a2 * v[i]);
+          cur[i] = x;
+          if (i >= cn + 2) sq += x * x;
+        }
+      }
+      sq = warp_sum(sq);
+      if (lane == 0) psq[warp] = sq;
+    }
+    __syncthreads();
+  }
+  if (n >= 1 && r == 0 && tid == 0) P.d[n - 1] = cur[n - 1];
+  // no CTA leaves while another may still read its shared memory
+  trdc_sync<CL>();
+}
+
 // Launch configuration of the cluster kernel for `nprob` blocks.  The
 // kernel's attributes (largest dynamic shared memory, non-portable cluster
 // size) are set once per device, at the largest size any launch uses, by the
 // solver's constructor (set_attr): setting them per launch to the launch's
 // own size would race between solver instances on other threads.
+// The cluster kernel of CL CTAs: one or two cluster barriers per column.
 template <int CL>
-cudaError_t trdc_config(size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int nprob,
+void (*trdc_kernel(bool one))(const TrdClProb*) {
+  return one ? trd_cluster1_kernel<CL> : trd_cluster_kernel<CL>;
+}
+
+template <int CL>
+cudaError_t trdc_config(bool one, size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int nprob,
                         cudaStream_t st, bool set_attr) {
   cfg = cudaLaunchConfig_t{};
   cfg.gridDim = dim3((unsigned)(nprob * CL));
-  cfg.blockDim = dim3(TRDC_NT);
+  cfg.blockDim = dim3(one ? TRDC1_NT : TRDC_NT);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -777,9 +1041,9 @@ cudaError_t trdc_config(size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribut
   cfg.attrs = at;
   cfg.numAttrs = 1;
   if (!set_attr) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(trd_cluster_kernel<CL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(trdc_kernel<CL>(one), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess && CL > 8)
-    e = cudaFuncSetAttribute(trd_cluster_kernel<CL>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    e = cudaFuncSetAttribute(trdc_kernel<CL>(one), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   return e;
 }
 
@@ -787,15 +1051,15 @@ cudaError_t trdc_config(size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribut
 // (0: this cluster size is not usable here); sets the kernel's attributes
 // for launches of up to `smem` bytes.
 template <int CL>
-int trdc_max_clusters(size_t smem) {
+int trdc_max_clusters(bool one, size_t smem) {
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute at[1];
-  if (trdc_config<CL>(smem, cfg, at, 1, nullptr, true) != cudaSuccess) {
+  if (trdc_config<CL>(one, smem, cfg, at, 1, nullptr, true) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
   int nc = 0;
-  if (cudaOccupancyMaxActiveClusters(&nc, trd_cluster_kernel<CL>, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&nc, trdc_kernel<CL>(one), &cfg) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -803,12 +1067,12 @@ int trdc_max_clusters(size_t smem) {
 }
 
 template <int CL>
-cudaError_t trdc_launch(const TrdClProb* d, int nprob, size_t smem, cudaStream_t st) {
+cudaError_t trdc_launch(bool one, const TrdClProb* d, int nprob, size_t smem, cudaStream_t st) {
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute at[1];
-  cudaError_t e = trdc_config<CL>(smem, cfg, at, nprob, st, false);
+  cudaError_t e = trdc_config<CL>(one, smem, cfg, at, nprob, st, false);
   if (e != cudaSuccess) return e;
-  return cudaLaunchKernelEx(&cfg, trd_cluster_kernel<CL>, d);
+  return cudaLaunchKernelEx(&cfg, trdc_kernel<CL>(one), d);
 }
 
 // A kernel's largest dynamic shared memory on the current device only grows:
@@ -1490,18 +1754,23 @@ SyevBatched::SyevBatched() {
   // (comparisons, or a device where cluster launches are unavailable)
   const char* path = getenv("NRGB_TRD_PATH");
   if (path && strcmp(path, "panel") == 0) cl_smem_ = 0;
+  // NRGB_TRDC_BARRIERS=2 selects the cluster kernel with two cluster
+  // barriers per column (comparisons); the default has one
+  const char* nb = getenv("NRGB_TRDC_BARRIERS");
+  cl_one_ = !(nb && strcmp(nb, "2") == 0);
   if (cl_smem_ > 0) {
-    cl_max_[0] = trdc_max_clusters<1>(cl_smem_);
-    cl_max_[1] = trdc_max_clusters<2>(cl_smem_);
-    cl_max_[2] = trdc_max_clusters<4>(cl_smem_);
-    cl_max_[3] = trdc_max_clusters<8>(cl_smem_);
-    cl_max_[4] = trdc_max_clusters<16>(cl_smem_);
+    cl_max_[0] = trdc_max_clusters<1>(cl_one_, cl_smem_);
+    cl_max_[1] = trdc_max_clusters<2>(cl_one_, cl_smem_);
+    cl_max_[2] = trdc_max_clusters<4>(cl_one_, cl_smem_);
+    cl_max_[3] = trdc_max_clusters<8>(cl_one_, cl_smem_);
+    cl_max_[4] = trdc_max_clusters<16>(cl_one_, cl_smem_);
   }
-  // largest block the cluster kernel holds
+  // largest block the cluster kernel holds (the one-barrier kernel also
+  // reads at most TRDC1_ROWS rows of a column per thread)
   for (int k = 4; k >= 0 && cl_nmax_ == 0; --k) {
     if (cl_max_[k] <= 0) continue;
     int n = 1;
-    while (trdc_smem_doubles(n + 1, 1 << k) * sizeof(double) <= cl_smem_) ++n;
+    while (trdc_bytes(n + 1, 1 << k) <= cl_smem_ && (!cl_one_ || n + 1 <= TRDC1_ROWS * TRDC1_NT)) ++n;
     cl_nmax_ = n > SMALL_N ? n : 0;
   }
   for (int i = 0; i < NAUX; ++i) {
@@ -1586,6 +1855,10 @@ size_t SyevBatched::workspace_bytes(const std::vector<int>& ns) {
                256 * 6 * (size_t)(nmx / NBB + 4));
   pl.add<TrdClProb>(2 * ns.size() + 16);
   return pl.bytes + (size_t)ns.size() * 4096 + (1 << 20);
+}
+
+size_t SyevBatched::trdc_bytes(int n, int cl) const {
+  return (cl_one_ ? trdc1_smem_doubles(n, cl) : trdc_smem_doubles(n, cl)) * sizeof(double);
 }
 
 int SyevBatched::cl_use() const {
@@ -1729,7 +2002,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       for (const TrdClProb& t : list) {
         const int n = t.n;
         for (int k = 0; k < 5; ++k) {
-          const size_t bytes = trdc_smem_doubles(n, 1 << k) * sizeof(double);
+          const size_t bytes = trdc_bytes(n, 1 << k);
           if (cl_max_[k] > 0 && bytes <= cl_smem_) {
             const int g = k > 0 ? k + 3 : (n <= 64 ? 0 : n <= 96 ? 1 : n <= 128 ? 2 : 3);
             grp[g].push_back(t);
@@ -1761,11 +2034,11 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         const int k = g > 3 ? g - 3 : 0;
         cudaError_t e = cudaSuccess;
         NRGB_LAUNCH("trd_cluster", sx,
-                    e = (k == 0)   ? trdc_launch<1>(dg[g], np, gsmem[g], sx)
-                        : (k == 1) ? trdc_launch<2>(dg[g], np, gsmem[g], sx)
-                        : (k == 2) ? trdc_launch<4>(dg[g], np, gsmem[g], sx)
-                        : (k == 3) ? trdc_launch<8>(dg[g], np, gsmem[g], sx)
-                                   : trdc_launch<16>(dg[g], np, gsmem[g], sx));
+                    e = (k == 0)   ? trdc_launch<1>(cl_one_, dg[g], np, gsmem[g], sx)
+                        : (k == 1) ? trdc_launch<2>(cl_one_, dg[g], np, gsmem[g], sx)
+                        : (k == 2) ? trdc_launch<4>(cl_one_, dg[g], np, gsmem[g], sx)
+                        : (k == 3) ? trdc_launch<8>(cl_one_, dg[g], np, gsmem[g], sx)
+                                   : trdc_launch<16>(cl_one_, dg[g], np, gsmem[g], sx));
         NRGB_CUDA(e);
         ++launches_;
         ++used;

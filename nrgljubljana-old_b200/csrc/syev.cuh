@@ -85,6 +85,9 @@ class SyevBatched : public EigSolver {
   int cl_max_[5] = {0, 0, 0, 0, 0};  // resident clusters of 1, 2, 4, 8, 16 CTAs (0: not usable)
   size_t cl_smem_ = 0;                // shared memory per CTA of the cluster kernel
   int cl_nmax_ = 0;                   // largest block it holds (0: cluster path off)
+  bool cl_one_ = true;                // one cluster barrier per column (else two)
+  // dynamic shared memory of one CTA of the cluster kernel in use
+  size_t trdc_bytes(int n, int cl) const;
   // blocks up to this size go to the cluster kernel whole: the capacity, or
   // the schedule's limit when it is lower (schedule.cuh)
   int cl_use() const;

@@ -71,7 +71,14 @@ GOLDEN_CASES = {
     # two-channel Kondo model at full size: J = 0.2 per channel, Lambda = 3,
     # Nmax = 40, keep 3000 (blocks up to ~8000), FDM spectra of three operator
     # pairs at T = 1e-6, 50 bins per decade
-    "kondo2ch_full": dict(model="kondo", J=[0.2, 0.2], Lambda=3.0, Nmax=40,
+    # The per-bin absolute floor of this case is n_max eps = 2e-12 of the
+    # largest bin instead of 1e-13: a bin's weight is a sum of products of
+    # eigenvector components of blocks up to ~8000 carried through 40
+    # recalculations, and two summation orders of n terms differ by up to
+    # about n eps of the sum of magnitudes.  Two FP64 GPU builds that differ
+    # only in the tridiagonalisation kernel differ by 1.7e-8 relative on a
+    # bin of 3e-5 of the largest (5e-13 of it).
+    "kondo2ch_full": dict(model="kondo", J=[0.2, 0.2], Lambda=3.0, Nmax=40, wabs=2e-12,
                           params={"keep": 3000, "fdm": True, "T": 1e-6, "spect": "SZd-SZd",
                                   "specd": "A_f0-A_f0 A_f1-A_f1", "bins": 50, "savebins": True,
                                   "broaden": False, "dumpannotated": 40}),
@@ -179,7 +186,7 @@ WABS = 1e-13        # ... plus the FP64 rounding floor of the sums that make a b
 RTOL_WMAX = 1e-8    # every bin (the tail included), relative to the largest bin
 
 
-def compare_outputs(got, ref, what=""):
+def compare_outputs(got, ref, what="", wabs=None):
     """Assert that run `got` reproduces run `ref` (dicts of load_outputs) at
     the FP64 targets: td and custom within 1e-8 relative (columns that vanish
     by symmetry against 1e-13 of the column scale), energies of the energy
@@ -190,7 +197,10 @@ def compare_outputs(got, ref, what=""):
     bin wherever |w| >= 1e-6 of the largest bin and within 1e-8 of the largest
     bin everywhere (the per-bin check allows an absolute 1e-13 of the
     largest bin, the FP64 rounding level of the sums behind a small bin),
-    broadened spectra within 1e-8 of their maximum."""
+    broadened spectra within 1e-8 of their maximum.  `wabs` replaces the
+    per-bin absolute floor (a fraction of the largest bin) for runs whose
+    blocks are large enough to need a higher one."""
+    wabs = WABS if wabs is None else wabs
     to, tg = ref["td"], got["td"]
     assert to.shape == tg.shape, (what, to.shape, tg.shape)
     tol = RTOL_TD * np.abs(to) + ATOL_TD
@@ -227,7 +237,7 @@ def compare_outputs(got, ref, what=""):
         err = np.abs(wg - wo)
         assert np.max(err) <= RTOL_WMAX * wmax, (what, name, "max-normalised", float(np.max(err) / wmax))
         big = np.abs(wo) >= WFLOOR * wmax
-        assert np.all(err[big] <= RTOL_W * np.abs(wo[big]) + WABS * wmax), \
+        assert np.all(err[big] <= RTOL_W * np.abs(wo[big]) + wabs * wmax), \
             (what, name, "per bin", float(np.max(err[big] / np.abs(wo[big]))))
     assert sorted(ref["dat"]) == sorted(got["dat"]), what
     for name in ref["dat"]:

@@ -77,11 +77,12 @@ def _random_sym(n, rng, kind):
 
 
 # covers the warp path (n <= 32), the cluster path (one cluster of 1..16 CTAs
-# per block; single-CTA launches split at 64, 96, 128; the cluster size
-# changes after 168, 237, 333, 469, and blocks above 656 take the
-# cooperative panel path) and the panel path
-SIZES = [1, 2, 3, 5, 16, 31, 32, 33, 40, 64, 65, 96, 97, 100, 128, 129, 168, 169, 237, 238, 257, 333, 334,
-         469, 470, 600, 656, 657, 1100]
+# per block; single-CTA launches split at 64, 96, 128; with the one-barrier
+# kernel the cluster size changes after 167, 235, 329, 461, and blocks above
+# 640 take the cooperative panel path; 168, 237, 333, 469 and 656 are the
+# two-barrier kernel's limits) and the panel path
+SIZES = [1, 2, 3, 5, 16, 31, 32, 33, 40, 64, 65, 96, 97, 100, 128, 129, 167, 168, 169, 235, 236, 237, 238, 257,
+         329, 330, 333, 334, 461, 462, 469, 470, 600, 640, 641, 656, 657, 1100]
 
 
 @pytest.mark.parametrize("kind", ["gauss", "logspaced", "degenerate"])

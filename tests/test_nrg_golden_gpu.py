@@ -36,4 +36,4 @@ def test_nrg_run_matches_oracle_golden(ctx, tmp_path, name):
     out_g = str(tmp_path / "gpu")
     os.makedirs(out_g)
     ctx.run(wd, out_g)
-    cases.compare_outputs(cases.load_outputs(out_g), ref, name)
+    cases.compare_outputs(cases.load_outputs(out_g), ref, name, wabs=cases.GOLDEN_CASES[name].get("wabs"))
