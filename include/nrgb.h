@@ -98,8 +98,13 @@ typedef struct {
   double scale, shift;
 } nrgb_diag_term;
 /* Off-diagonal term (offdiag_build, src/matrix.cc:86-137):
- *   H[offi + r, offj + c] = factor * src(r, c)  and the mirror entry,
- * src: handle of a rows x cols matrix (an <I||f||J> block). */
+ *   H[offi + r, offj + c] += factor * src(r, c)  and the mirror entry,
+ * src: handle of a rows x cols matrix (an <I||f||J> block), or -1 for the
+ * identity of a square sub-block (diag_offdiag_function,
+ * src/matrix.cc:256-276: SPSU2's on-site pairing).  Terms add: a sub-block
+ * may take several (SPSU2's hopping and anomalous hopping); the row range
+ * [offi, offi+rows) and the column range [offj, offj+cols) must not overlap,
+ * and two terms of one block cover the same sub-block or disjoint ones. */
 typedef struct {
   int blk, offi, offj, rows, cols, src;
   double factor;

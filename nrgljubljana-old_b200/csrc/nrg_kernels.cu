@@ -1,4 +1,6 @@
 // Device kernels of one NRG step besides the eigensolver and the GEMM.
+#include <map>
+#include <tuple>
 #include <math.h>
 
 #include "common.cuh"
@@ -30,8 +32,8 @@ __global__ void asm_off_kernel(const AsmOff* __restrict__ t) {
       const int r = r0 + threadIdx.x, c = c0 + cc;
       double v = 0.0;
       if (r < O.rows && c < O.cols) {
-        v = O.f * O.M[r + (size_t)c * O.ldm];
-        O.H[(size_t)(O.offi + r) + (size_t)(O.offj + c) * O.n] = v;
+        v = O.M ? O.f * O.M[r + (size_t)c * O.ldm] : (r == c ? O.f : 0.0);
+        O.H[(size_t)(O.offi + r) + (size_t)(O.offj + c) * O.n] += v;
       }
       tile[threadIdx.x][cc] = v;
     }
@@ -40,7 +42,7 @@ __global__ void asm_off_kernel(const AsmOff* __restrict__ t) {
     for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
       const int c = c0 + threadIdx.x, r = r0 + rr;
       if (r < O.rows && c < O.cols)
-        O.H[(size_t)(O.offj + c) + (size_t)(O.offi + r) * O.n] = tile[rr][threadIdx.x];
+        O.H[(size_t)(O.offj + c) + (size_t)(O.offi + r) * O.n] += tile[rr][threadIdx.x];
     }
     __syncthreads();
   }
@@ -260,6 +262,17 @@ cudaError_t assemble_launch(const AsmDiag* d_diag, int ndiag, const AsmOff* d_of
     NRGB_LAUNCH("assemble_off", st, asm_off_kernel<<<g, dim3(32, 8), 0, st>>>(d_off));
   }
   return cudaGetLastError();
+}
+
+std::vector<std::vector<AsmOff>> asm_off_layers(const std::vector<AsmOff>& terms) {
+  std::vector<std::vector<AsmOff>> layers;
+  std::map<std::tuple<double*, int, int>, int> seen;  // (H, lower offset, higher offset) -> terms so far
+  for (const AsmOff& t : terms) {
+    const int k = seen[std::make_tuple(t.H, std::min(t.offi, t.offj), std::max(t.offi, t.offj))]++;
+    if ((int)layers.size() <= k) layers.resize(k + 1);
+    layers[k].push_back(t);
+  }
+  return layers;
 }
 
 cudaError_t gather_diag_launch(const DiagGather* d_g, int ng, int max_len, double* dst, cudaStream_t st) {

@@ -1,6 +1,7 @@
 // Device kernels of one NRG step besides the eigensolver and the GEMM:
 // block-Hamiltonian assembly, gathers, spectral weights and log binning.
 #pragma once
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace nrgb {
@@ -13,8 +14,9 @@ struct AsmDiag {
   int n, off, len;
   double scale, shift;
 };
-// Off-diagonal sub-block: H[offi + r, offj + c] = f * M[r + c*ldm] and the
-// symmetric entry H[offj + c, offi + r] (both triangles are filled).
+// Off-diagonal sub-block: H[offi + r, offj + c] += f * M[r + c*ldm] and the
+// symmetric entry H[offj + c, offi + r] (both triangles are filled); M null:
+// the identity (f on the diagonal of a square sub-block).
 struct AsmOff {
   double* H;
   const double* M;
@@ -23,6 +25,11 @@ struct AsmOff {
 };
 cudaError_t assemble_launch(const AsmDiag* d_diag, int ndiag, const AsmOff* d_off, int noff,
                             int max_len, int max_rc, cudaStream_t st);
+// Splits off-diagonal terms into layers in which no two terms touch the same
+// sub-block or its mirror, so that the terms of one launch add without
+// races (symmetries whose couplings do not conserve charge give a sub-block
+// a hopping and an anomalous term).  Layers are launched one after another.
+std::vector<std::vector<AsmOff>> asm_off_layers(const std::vector<AsmOff>& terms);
 
 // ---- gathers ----
 // dst[dst_off[t] + r] = src[t][r * (ld[t] + 1)] for r < len[t]  (diagonals)

@@ -220,15 +220,29 @@ int nrgb_step(nrgb_ctx* ctx, const nrgb_step_plan* plan, int* z_handles, int* w_
       const nrgb_offdiag_term& o = plan->off[t];
       if (o.blk < 0 || o.blk >= nb) throw CudaError("nrgb_step: off-diagonal term: block out of range");
       const int n = plan->dim[o.blk];
-      if (o.offi < 0 || o.offj < 0 || o.offi + o.rows > n || o.offj + o.cols > n)
+      if (o.offi < 0 || o.offj < 0 || o.rows < 0 || o.cols < 0 || o.offi + o.rows > n || o.offj + o.cols > n)
         throw CudaError("nrgb_step: off-diagonal term out of its block");
-      const PlanMatrix& m = mat(ctx, o.src);
-      if (m.rows != o.rows || m.cols != o.cols) throw CudaError("nrgb_step: off-diagonal source size mismatch");
+      if (o.offi < o.offj + o.cols && o.offj < o.offi + o.rows && o.rows > 0 && o.cols > 0)
+        throw CudaError("nrgb_step: off-diagonal term overlaps the diagonal");
       if (!std::isfinite(o.factor)) throw CudaError("nrgb_step: off-diagonal factor not finite");
-      ao.push_back(AsmOff{H + hoff[o.blk], m.p, n, o.offi, o.offj, o.rows, o.cols, std::max(1, m.rows), o.factor});
+      const double* M = nullptr;  // src < 0: the identity (diag_offdiag_function, src/matrix.cc:256-276)
+      int ldm = 1;
+      if (o.src >= 0) {
+        const PlanMatrix& m = mat(ctx, o.src);
+        if (m.rows != o.rows || m.cols != o.cols) throw CudaError("nrgb_step: off-diagonal source size mismatch");
+        M = m.p;
+        ldm = std::max(1, m.rows);
+      } else if (o.rows != o.cols) {
+        throw CudaError("nrgb_step: identity term needs a square sub-block");
+      }
+      ao.push_back(AsmOff{H + hoff[o.blk], M, n, o.offi, o.offj, o.rows, o.cols, ldm, o.factor});
       maxrc = std::max(maxrc, o.rows * o.cols);
     }
-    NRGB_CUDA(assemble_launch(stage(ctx, ad), (int)ad.size(), stage(ctx, ao), (int)ao.size(), maxlen, maxrc, st));
+    const auto layers = asm_off_layers(ao);
+    NRGB_CUDA(assemble_launch(stage(ctx, ad), (int)ad.size(), layers.empty() ? nullptr : stage(ctx, layers[0]),
+                              layers.empty() ? 0 : (int)layers[0].size(), maxlen, maxrc, st));
+    for (size_t k = 1; k < layers.size(); ++k)
+      NRGB_CUDA(assemble_launch(nullptr, 0, stage(ctx, layers[k]), (int)layers[k].size(), 0, maxrc, st));
     // eigen-decomposition of every block
     std::vector<SyevDesc> sd;
     std::vector<int> zh(nb);

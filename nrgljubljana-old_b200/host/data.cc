@@ -62,14 +62,20 @@ void DataFile::read(const std::string& path) {
   }
   if (version != 9) throw std::runtime_error("data file version mismatch (expected 9)");
   T.line = pos;
+  // invariants are written with one integer per quantum number: SPSU2 has
+  // the spin alone (read as (0, SS))
+  const bool one_qn = symtype == "SPSU2";
+  auto read_invar = [&](Invar& I) {
+    I.first = one_qn ? 0 : T.i();
+    I.second = T.i();
+  };
   channels = T.i();
   Nmax = T.i();
   const int nsubs = T.i();
   if (nsubs <= 0) throw std::runtime_error("data file: no subspaces");
   for (int s = 0; s < nsubs; ++s) {
     Invar I;
-    I.first = T.i();
-    I.second = T.i();
+    read_invar(I);
     const int n = T.i();
     if (n <= 0) throw std::runtime_error("data file: empty subspace");
     std::vector<double> e(n);
@@ -80,10 +86,8 @@ void DataFile::read(const std::string& path) {
     const int nf = T.i();
     for (int k = 0; k < nf; ++k) {
       Invar I1, I2;
-      I1.first = T.i();
-      I1.second = T.i();
-      I2.first = T.i();
-      I2.second = T.i();
+      read_invar(I1);
+      read_invar(I2);
       HostMat M;
       M.rows = energies.count(I1) ? (int)energies[I1].size() : 0;
       M.cols = energies.count(I2) ? (int)energies[I2].size() : 0;
@@ -116,18 +120,18 @@ void DataFile::read(const std::string& path) {
     } else if (kind == 's' || kind == 'p' || kind == 'g' || kind == 'd' || kind == 't' ||
                kind == 'o' || kind == 'q') {
       read_blocks(ops[kind][name]);
-    } else if (kind == 'z') {
-      xi.resize(channels);
-      zeta.resize(channels);
-      for (int ch = 0; ch < channels; ++ch) {
-        const int n = T.i();
-        xi[ch].resize(n + 1);
-        for (auto& x : xi[ch]) x = T.d();
-      }
-      for (int ch = 0; ch < channels; ++ch) {
-        const int n = T.i();
-        zeta[ch].resize(n + 1);
-        for (auto& x : zeta[ch]) x = T.d();
+    } else if (kind == 'z' || kind == 'Z') {
+      // z: xi then zeta; Z: delta then kappa; one table per channel each
+      auto& t1 = kind == 'z' ? xi : delta;
+      auto& t2 = kind == 'z' ? zeta : kappa;
+      for (auto* t : {&t1, &t2}) {
+        t->resize(channels);
+        for (int ch = 0; ch < channels; ++ch) {
+          const int n = T.i();
+          if (n < 0) throw std::runtime_error("data file: bad coefficient table length");
+          (*t)[ch].resize(n + 1);
+          for (auto& x : (*t)[ch]) x = T.d();
+        }
       }
     } else {
       throw std::runtime_error(std::string("Unknown block ") + kind + " in data file.");

@@ -6,13 +6,14 @@
 // the Wilson-chain coefficient tables (z: xi, zeta per channel).
 #pragma once
 #include <map>
+#include <stdexcept>
 #include <string>
 #include <utility>
 #include <vector>
 
 namespace nrgb {
 
-using Invar = std::pair<int, int>;          // (Q, SS) for the QS symmetry
+using Invar = std::pair<int, int>;          // (Q, SS) for QS, (Q, SSZ) for QSZ, (0, SS) for SPSU2
 using Twoinvar = std::pair<Invar, Invar>;   // (bra, ket) subspaces
 
 struct HostMat {
@@ -30,6 +31,16 @@ struct DataFile {
   double gs_energy = 0.0;
   std::map<char, std::map<std::string, HostBlocks>> ops;       // kind -> name -> blocks
   std::vector<std::vector<double>> xi, zeta;                   // per channel, index 0..Nmax
+  // superconducting baths (block Z, src/nrg.cc:3383-3386): on-site pairing
+  // delta and anomalous hopping kappa per channel; empty when absent
+  std::vector<std::vector<double>> delta, kappa;
+
+  // Entry n of table t for channel ch, 0 where the file has no such table.
+  static double chain_coef(const std::vector<std::vector<double>>& t, int ch, int n) {
+    if (ch >= (int)t.size()) return 0.0;
+    if (n < 0 || n >= (int)t[ch].size()) throw std::runtime_error("chain coefficient index out of range");
+    return t[ch][n];
+  }
 
   void read(const std::string& path);
 };

@@ -818,9 +818,23 @@ struct NrgDriver::Impl {
         for (const OffdiagTerm& t : sym->offdiag(I)) {
           const int i0 = t.i - 1, j0 = t.j - 1;
           if (!(b.rmax[i0] > 0 && b.rmax[j0] > 0)) continue;
-          const double fs = t.factor * D.xi[t.ch][N] / scale1;
+          // coefficient of the term: hopping xi_N, anomalous hopping kappa_N,
+          // or the new site's pairing 2 delta_N+1 (src/sym-SPSU2.cc:107-113)
+          const double coef = t.kind == 0 ? D.xi[t.ch][N]
+                              : t.kind == 1 ? D.chain_coef(D.kappa, t.ch, N)
+                                            : 2.0 * D.chain_coef(D.delta, t.ch, N + 1);
+          const double fs = t.factor * coef / scale1;
           if (!std::isfinite(fs)) throw std::runtime_error("offdiag_function: factor is not finite");
           if (fabs(fs) < 1e-8) continue;
+          if (t.kind == 2) {
+            // identity between two combinations of the same ancestor
+            // (diag_offdiag_function, src/matrix.cc:256-276)
+            if (b.anc[i0] != b.anc[j0] || b.rmax[i0] != b.rmax[j0])
+              throw std::runtime_error("diag_offdiag_function: combinations of different ancestors");
+            ao.push_back(AsmOff{Hb, nullptr, b.dim, b.off[i0], b.off[j0], b.rmax[i0], b.rmax[j0], 1, fs});
+            maxrc = std::max(maxrc, b.rmax[i0] * b.rmax[j0]);
+            continue;
+          }
           auto it = opch[t.ch].find({b.anc[i0], b.anc[j0]});
           if (it == opch[t.ch].end()) throw std::runtime_error("offdiag_function: <||f||> subspace does not exist");
           const DevMat& M = it->second;
@@ -838,8 +852,12 @@ struct NrgDriver::Impl {
         NRGB_CUDA(cudaStreamSynchronize(st));
         load_transformations(N, S);
       } else {
-        NRGB_CUDA(assemble_launch(upload(ad), (int)ad.size(), upload(ao), (int)ao.size(), maxlen, maxrc, st));
-        launches += 2;
+        const auto layers = asm_off_layers(ao);
+        NRGB_CUDA(assemble_launch(upload(ad), (int)ad.size(), layers.empty() ? nullptr : upload(layers[0]),
+                                  layers.empty() ? 0 : (int)layers[0].size(), maxlen, maxrc, st));
+        for (size_t k = 1; k < layers.size(); ++k)
+          NRGB_CUDA(assemble_launch(nullptr, 0, upload(layers[k]), (int)layers[k].size(), 0, maxrc, st));
+        launches += 1 + (int)std::max<size_t>(1, layers.size());
         launches += syev->solve(sd, st);
         eig_calls += 1;
         if (!P.removefiles) store_transformations(N, S);
@@ -1418,7 +1436,7 @@ struct NrgDriver::Impl {
           int deg = 0;
           const size_t i0 = i;
           while (i < len && fcmp(l[i].first, l[i0].first)) {
-            qn.push_back(std::to_string(l[i].second.first) + " " + std::to_string(l[i].second.second));
+            qn.push_back(sym->label(l[i].second));
             deg += sym->mult(l[i].second);
             ++i;
           }
@@ -1427,7 +1445,7 @@ struct NrgDriver::Impl {
           F << " [" << deg << "]\n";
         }
       } else {
-        for (const auto& x : l) F << en(x.first) << " " << x.second.first << " " << x.second.second << "\n";
+        for (const auto& x : l) F << en(x.first) << " " << sym->label(x.second) << "\n";
       }
       F << "\n";
     }
@@ -1568,8 +1586,11 @@ struct NrgDriver::Impl {
       if (!P.spect.empty() || !P.specs.empty())
         throw std::runtime_error("symmetry type QSZ: only the spectral functions of doublet operators are built");
       sym.reset(new SymmetryQSZ());
+    } else if (D.symtype == "SPSU2") {
+      if (D.channels != 1) throw std::runtime_error("symmetry type SPSU2: one channel is built");
+      sym.reset(new SymmetrySPSU2());
     } else {
-      throw std::runtime_error("symmetry type " + D.symtype + " is not built (QS, QSZ)");
+      throw std::runtime_error("symmetry type " + D.symtype + " is not built (QS, QSZ, SPSU2)");
     }
     if (P.Nmax == 0) P.Nmax = D.Nmax;
     if ((int)D.xi[0].size() - 1 != P.Nmax) throw std::runtime_error("length of coefficient table != Nmax");

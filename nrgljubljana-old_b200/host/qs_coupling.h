@@ -22,7 +22,10 @@
 
 namespace nrgb {
 
-struct OffdiagTerm { int i, j, ch; double factor; };   // 1-based combination indices
+// 1-based combination indices.  kind 0: hopping xi_N <||f^dag||>; 1:
+// anomalous hopping kappa_N <||f^dag||>; 2: on-site pairing of the new site,
+// 2 delta_N+1 times the identity between two combinations of one ancestor.
+struct OffdiagTerm { int i, j, ch; double factor; int kind = 0; };
 struct DiagTerm { int i, ch; double number; };
 struct RecalcRow { int i1, ip; double factor; };
 struct RecalcTable { Invar Ip; int ch; std::vector<RecalcRow> rows; };

@@ -62,6 +62,9 @@ class Symmetry {
   // inequality for SU(2) symmetries; both spin components of a doublet for
   // the spin-projection symmetries).
   virtual bool connects(const Invar& I1, const Invar& Ip, const Invar& Iop) const { return triangle(I1, Ip, Iop); }
+  // The quantum numbers of a subspace as the reference prints them
+  // (annotated.dat): both numbers, or the spin alone for SPSU2.
+  virtual std::string label(const Invar& I) const { return std::to_string(I.first) + " " + std::to_string(I.second); }
   static Invar combine(const Invar& a, const Invar& b) { return {a.first + b.first, a.second + b.second}; }
   static Invar inverse(const Invar& a) { return {-a.first, -a.second}; }
 };
@@ -185,6 +188,128 @@ class SymmetryQS : public Symmetry {
  private:
   int nch_;
   std::unique_ptr<QSCoupling> cpl_;  // derived tables (2 channels)
+  std::vector<Invar> in_, qn_;
+};
+
+// SPSU2 plug-in: spin SU(2) without charge conservation (superconducting
+// baths), invariant subspaces SS = 2S+1, written (0, SS) (src/sym-SPSU2.cc),
+// one channel.  The combinations of a subspace SS add the new site empty
+// (ancestor SS), doubly occupied (ancestor SS), singly occupied on an
+// ancestor SS-1 and on an ancestor SS+1 (spsu2-1ch-In2.dat, QN.dat).  With
+// S = (SS-1)/2 and a = sqrt((SS-1)/SS), b = sqrt((SS+1)/SS):
+//  * hopping xi_N sum_s (f^dag_N,s f_N+1,s + h.c.): (1,3) 1, (1,4) 1,
+//    (3,2) -a, (4,2) b (spsu2-1ch-offdiag.dat);
+//  * anomalous hopping kappa_N (f^dag_N,up f^dag_N+1,dn - f^dag_N,dn
+//    f^dag_N+1,up + h.c.): (2,3) 1, (2,4) 1, (3,1) a, (4,1) -b
+//    (spsu2-1ch-anomalous.dat);
+//  * on-site pairing delta_N+1 (f^dag_N+1,up f^dag_N+1,dn + h.c.): the
+//    empty and the doubly occupied combinations, -1/2 times 2 delta
+//    (spsu2-1ch-isospinx.dat; ISOSPINX and ANOMALOUS, src/sym-SPSU2.cc:107-113);
+//  * electrons of the new site 0, 2, 1, 1 (spsu2-1ch-diag.dat).
+// The <f^dag>, doublet and triplet recalculation tables are those of QS with
+// the combinations renumbered (QS 1, 2, 3, 4 = SPSU2 1, 3, 4, 2) and the
+// charge dropped.  oracle/spsu2_derive.py derives every entry from the
+// site's Fock space; the tests check both against the reference's tables.
+// Thermodynamics column <Sz^2> (calculate_TD, src/sym-SPSU2.cc:81-94).
+class SymmetrySPSU2 : public Symmetry {
+ public:
+  SymmetrySPSU2() {
+    in_ = {{0, 0}, {0, 0}, {0, -1}, {0, 1}};
+    qn_ = {{0, 1}, {0, 1}, {0, 2}, {0, 2}};
+  }
+  std::string name() const override { return "SPSU2"; }
+  std::string label(const Invar& I) const override { return std::to_string(I.second); }
+  int combs() const override { return 4; }
+  const std::vector<Invar>& In() const override { return in_; }
+  const std::vector<Invar>& QN() const override { return qn_; }
+  int mult(const Invar& I) const override { return I.second; }
+  bool allowed(const Invar& I) const override { return I.second > 0; }
+  bool triangle(const Invar& a, const Invar& b, const Invar& c) const override {
+    return SymmetryQS::su2(a.second, b.second, c.second);
+  }
+  Invar singlet() const override { return {0, 1}; }
+  Invar doublet() const override { return {0, 2}; }
+  Invar triplet() const override { return {0, 3}; }
+
+  std::vector<OffdiagTerm> offdiag(const Invar& I) const override {
+    const double ss = I.second;
+    const double a = sqrt((ss - 1) / ss), b = sqrt((ss + 1) / ss);
+    return {{1, 3, 0, 1.0, 0}, {1, 4, 0, 1.0, 0}, {3, 2, 0, -a, 0}, {4, 2, 0, b, 0},
+            {2, 3, 0, 1.0, 1}, {2, 4, 0, 1.0, 1}, {3, 1, 0, a, 1},  {4, 1, 0, -b, 1},
+            {1, 2, 0, -0.5, 2}};
+  }
+  std::vector<DiagTerm> diag() const override { return {{1, 0, 0.0}, {2, 0, 2.0}, {3, 0, 1.0}, {4, 0, 1.0}}; }
+
+  std::vector<RecalcTable> recalc_f(const Invar& Ip) const override {
+    const int ssp = Ip.second;
+    std::vector<RecalcTable> t;
+    t.push_back({{0, ssp + 1}, 0, {{2, 4, -sqrt(double(ssp) / (ssp + 1))}, {3, 1, 1.0}}});
+    if (ssp > 1) t.push_back({{0, ssp - 1}, 0, {{2, 3, sqrt(double(ssp) / (ssp - 1))}, {4, 1, 1.0}}});
+    return t;
+  }
+  std::vector<RecalcTable> recalc_doublet(const Invar& I1) const override {
+    const int ss1 = I1.second;
+    const double c = sqrt(double(ss1 - 1) * (ss1 + 1)) / ss1;
+    std::vector<RecalcTable> t;
+    t.push_back({{0, ss1 + 1}, 0, {{1, 1, 1.0}, {2, 2, 1.0}, {3, 3, -c}, {4, 3, 1.0 / ss1}, {4, 4, -1.0}}});
+    if (ss1 > 1)
+      t.push_back({{0, ss1 - 1}, 0, {{1, 1, 1.0}, {2, 2, 1.0}, {3, 3, -1.0}, {3, 4, -1.0 / ss1}, {4, 4, -c}}});
+    return t;
+  }
+  std::vector<RecalcTable> recalc_triplet(const Invar& I1) const override {
+    const int ss1 = I1.second;
+    const double S = (ss1 - 1) / 2.0;
+    std::vector<RecalcTable> t;
+    if (S > 0) {
+      const double t33 = sqrt(1 - 1 / S + 2 / (1 + 2 * S));
+      const double t34 = 1 / sqrt((1 + S) * (1 + 2 * S));
+      const double t43 = -1 / sqrt(S * (1 + 2 * S));
+      const double t44 = sqrt(S * (1 + 2 * S) / (pow(1 + S, 3) * (3 + 2 * S))) * (1 + S) +
+                         2 * sqrt(S / (3 + 11 * S + 12 * S * S + 4 * S * S * S));
+      t.push_back({{0, ss1}, 0, {{1, 1, 1.0}, {2, 2, 1.0}, {3, 3, t33}, {3, 4, t34}, {4, 3, t43}, {4, 4, t44}}});
+    }
+    t.push_back({{0, ss1 + 2}, 0,
+                 {{1, 1, 1.0}, {2, 2, 1.0}, {3, 3, sqrt(1 + 1 / (1 + S) - 2 / (1 + 2 * S))},
+                  {4, 3, -1 / sqrt((1 + S) * (1 + 2 * S))}, {4, 4, 1.0}}});
+    if (S > 0.5) {
+      const double m44 = (sqrt((-1 + 4 * S * S) / (S + S * S)) + sqrt((-1 + 2 * S) / (S + 3 * S * S + 2 * S * S * S))) / 2;
+      t.push_back({{0, ss1 - 2}, 0, {{1, 1, 1.0}, {2, 2, 1.0}, {3, 3, 1.0}, {3, 4, 1 / sqrt(S * (1 + 2 * S))}, {4, 4, m44}}});
+    }
+    return t;
+  }
+  double specdens_factor(const Invar& Ip, const Invar& I1) const override {
+    const double Sp = (Ip.second - 1) / 2.0;
+    return I1.second == Ip.second + 1 ? Sp + 1.0 : Sp;
+  }
+  double dynsusc_factor(const Invar& Ip, const Invar& I1) const override {
+    const int ssp = Ip.second, ss1 = I1.second;
+    if (ss1 == ssp + 2) return 1.0 + (ssp - 1) / 3.0;
+    if (ss1 == ssp) return ssp / 3.0;
+    if (ss1 == ssp - 2) return (-2.0 + ssp) / 3.0;
+    throw std::runtime_error("dynsusc_factor: not a triplet pair");
+  }
+  std::vector<std::string> td_names() const override { return {"<Sz^2>"}; }
+  std::vector<double> td_values(const std::vector<std::pair<Invar, const std::vector<double>*>>& blocks,
+                                double factor, double Z) const override {
+    double trSZ = 0;
+    for (const auto& b : blocks) {
+      double sumZ = 0;
+      for (double x : *b.second) sumZ += exp(-factor * x);
+      const double ss = b.first.second;
+      trSZ += sumZ * mult(b.first) * (ss * ss - 1) / 12.0;
+    }
+    return {trSZ / Z};
+  }
+  std::vector<double> td_values_sums(const std::vector<std::pair<Invar, double>>& zsum, double Z) const override {
+    double trSZ = 0;
+    for (const auto& b : zsum) {
+      const double ss = b.first.second;
+      trSZ += b.second * mult(b.first) * (ss * ss - 1) / 12.0;
+    }
+    return {trSZ / Z};
+  }
+
+ private:
   std::vector<Invar> in_, qn_;
 };
 

@@ -336,15 +336,19 @@ class ClusterModel:
     triplet_ops: Dict[str, int] = field(default_factory=dict)   # name -> orbital (spin op)
 
 
-def siam_cluster(U: float, eps_d: float, V: float, zeta0: float = 0.0) -> ClusterModel:
+def siam_cluster(U: float, eps_d: float, V: float, zeta0: float = 0.0, delta0: float = 0.0) -> ClusterModel:
     """Single-impurity Anderson model, impurity d + first chain site f_0:
-    H = eps_d n_d + U n_up n_dn + V sum_s (d^dag_s f_0s + h.c.) + zeta0 (n_f0 - 1)."""
+    H = eps_d n_d + U n_up n_dn + V sum_s (d^dag_s f_0s + h.c.) + zeta0 (n_f0 - 1)
+        + delta0 (f^dag_0up f^dag_0dn + h.c.)   (pairing: superconducting bath)."""
     F = Fock(2)  # orbital 0 = d, orbital 1 = f0
     H = eps_d * F.n(0) + U * F.n(0, 0) @ F.n(0, 1)
     for s in (0, 1):
         hop = F.cd(0, s) @ F.c(1, s)
         H = H + V * (hop + hop.T)
     H = H + zeta0 * (F.n(1) - np.eye(F.dim))
+    if delta0:
+        pair = F.cd(1, 0) @ F.cd(1, 1)
+        H = H + delta0 * (pair + pair.T)
     m = ClusterModel(F, H, charge_orbitals=[0, 1], f_orbitals=[1], spin_orbitals=[0, 1],
                      basis_mask=np.ones(F.dim, dtype=bool))
     m.doublet_ops["A_d"] = 0
@@ -670,6 +674,120 @@ def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: in
     return {"subspaces": len(subs), "gs_energy": gs, "scale0": sc0}
 
 
+def decompose_spsu2(m: ClusterModel, tol: float = 1e-9) -> List[Subspace]:
+    """Eigenstates per spin subspace SS of the SPSU2 symmetry (spin SU(2),
+    charge not conserved, src/sym-SPSU2.cc): the highest-weight states of
+    every S_z = S sector over all charges; representative S_z = S.  The
+    Subspace field Q is 0."""
+    F = m.fock
+    Sp, Sz = _total_spin_ops(m)
+    sz = np.round(np.diag(Sz) * 2).astype(int)
+    subs = []
+    for two_s in sorted(set(sz[m.basis_mask])):
+        if two_s < 0:
+            continue
+        idx = np.where((sz == two_s) & m.basis_mask)[0]
+        idx_up = np.where((sz == two_s + 2) & m.basis_mask)[0]
+        if len(idx_up):
+            _, sv, vt = np.linalg.svd(Sp[np.ix_(idx_up, idx)])
+            B = vt[int((sv > tol).sum()):].T
+        else:
+            B = np.eye(len(idx))
+        if B.shape[1] == 0:
+            continue
+        Hs = B.T @ m.H[np.ix_(idx, idx)] @ B
+        e, w = np.linalg.eigh(0.5 * (Hs + Hs.T))
+        vec = np.zeros((F.dim, B.shape[1]))
+        vec[idx] = B @ w
+        subs.append(Subspace(0, int(two_s + 1), e, vec))
+    return subs
+
+
+def write_data_spsu2(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: int,
+                     xi: np.ndarray, zeta: np.ndarray, delta: np.ndarray, kappa: np.ndarray,
+                     discretization: str = "Y") -> dict:
+    """Write a version-9 `data` file of the SPSU2 symmetry (one channel):
+    subspaces labelled by SS alone, reduced matrix elements <SS1||a^dag||SS2>
+    of f_0 and of the doublet operators for |SS1 - SS2| = 1 in the
+    Wigner-Eckart normalisation of QS (ireducMatrixSpeedy, initial.m:2089),
+    singlet and triplet operators, the chain tables z (xi, zeta) and Z (delta:
+    on-site pairing, kappa: anomalous hopping; src/nrg.cc:3383-3386)."""
+    if len(m.f_orbitals) != 1:
+        raise ValueError("SPSU2 data: one channel")
+    F = m.fock
+    subs = decompose_spsu2(m)
+    smap = {s.SS: s for s in subs}
+    gs = min(s.energies[0] for s in subs)
+    sc0 = scale_factor(0, Lambda, z, discretization)
+
+    def doublet(orb):
+        out = {}
+        for ss2, s2 in smap.items():
+            for ss1 in (ss2 + 1, ss2 - 1):
+                if ss1 in smap:
+                    S1, S2 = (ss1 - 1) / 2, (ss2 - 1) / 2
+                    op = F.cd(orb, 0 if S1 > S2 else 1)
+                    out[(ss1, ss2)] = smap[ss1].vectors.T @ op @ s2.vectors / cg_half(S2, S1)
+        return out
+
+    def triplet(orb):
+        sp, sm, szo = F.spin_ops(orb)
+        out = {}
+        for ss2, s2 in smap.items():
+            for ss1 in (ss2 + 2, ss2, ss2 - 2):
+                if ss1 not in smap:
+                    continue
+                S1, S2 = (ss1 - 1) / 2, (ss2 - 1) / 2
+                q = int(round(S1 - S2))
+                op = {1: -sp / math.sqrt(2), 0: szo, -1: sm / math.sqrt(2)}[q]
+                c = cg_one(S2, S1)
+                if c != 0.0:
+                    out[(ss1, ss2)] = smap[ss1].vectors.T @ op @ s2.vectors / c
+        return out
+
+    lines = ["# Input file for NRG Ljubljana (generated by inputgen.py)",
+             "# symtype SPSU2",
+             "#!9",
+             "# Number of channels, chain sites, subspaces: ",
+             "%d %d %d" % (1, Nmax, len(subs)),
+             "# SCALE " + _fmt(sc0),
+             "# Energies (GS energy subtracted, multiplied by 1/SCALE):"]
+    for s in subs:
+        lines.append("%d" % s.SS)
+        lines.append("%d" % len(s.energies))
+        lines.append(" ".join(_fmt((e - gs) / sc0) for e in s.energies))
+
+    def blocks(kind_name, bl):
+        lines.append(kind_name)
+        lines.append("%d" % len(bl))
+        for (k1, k2), M in bl.items():
+            lines.append("%d %d" % (k1, k2))
+            _write_matrix(lines, M)
+
+    lines.append("# Irreducible matrix elements for Wilson chains:")
+    blocks("f 0 0", doublet(m.f_orbitals[0]))
+    lines.append("# GS energy in absolute units:")
+    lines.append("e")
+    lines.append(_fmt(gs))
+    lines.append("# Irreducible matrix elements for other operators:")
+    for name, op in m.singlet_ops.items():
+        blocks("s" + name, {(k, k): s.vectors.T @ op @ s.vectors for k, s in smap.items()})
+    for name, orb in m.doublet_ops.items():
+        blocks("d" + name, doublet(orb))
+    for name, orb in m.triplet_ops.items():
+        blocks("t" + name, triplet(orb))
+    lines.append("# Discretization tables:")
+    for tag, tabs in (("z", (xi, zeta)), ("Z", (delta, kappa))):
+        lines.append(tag)
+        for t in tabs:
+            lines.append("%d" % (len(t) - 1))
+            lines.extend(_fmt(x) for x in t)
+    lines.append("")
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines))
+    return {"subspaces": len(subs), "gs_energy": gs, "scale0": sc0}
+
+
 def write_param(path: str, params: Dict[str, object]) -> None:
     with open(path, "w") as fh:
         fh.write("[param]\n")
@@ -682,21 +800,33 @@ def write_param(path: str, params: Dict[str, object]) -> None:
 def make_siam(dirpath: str, U: float, eps_d: float, Gamma: float, Lambda: float,
               Nmax: int, z: float = 1.0, params: Dict[str, object] | None = None,
               V: float | None = None, dps: int = 200, discretization: str = "Y",
-              symtype: str = "QS") -> dict:
+              symtype: str = "QS", gap: float = 0.0) -> dict:
     """Generate `data` and `param` for a single-impurity Anderson model on a
-    flat band (D=1) in directory `dirpath`, symmetry QS or QSZ.  V defaults
-    to sqrt(2 Gamma/pi); discretization Y, C or Z (wilson_chain_flat)."""
+    flat band (D=1) in directory `dirpath`, symmetry QS, QSZ or SPSU2.  V
+    defaults to sqrt(2 Gamma/pi); discretization Y, C or Z
+    (wilson_chain_flat).  SPSU2 only: `gap` is the BCS gap of the band; the
+    pairing Delta sum_k (c^dag_k,up c^dag_k,dn + h.c.) is the identity in
+    the band's modes, so every chain site carries the same on-site pairing
+    delta_n = gap, and the anomalous hopping kappa_n vanishes."""
     os.makedirs(dirpath, exist_ok=True)
     if V is None:
         V = math.sqrt(2.0 * Gamma / math.pi)
     xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps, discretization=discretization)
-    m = siam_cluster(U, eps_d, V, zeta0=zeta[0])
-    if symtype == "QSZ":
+    if gap and symtype != "SPSU2":
+        raise ValueError("a superconducting band needs symtype SPSU2")
+    m = siam_cluster(U, eps_d, V, zeta0=zeta[0], delta0=gap)
+    delta = np.full(Nmax + 1, float(gap))
+    kappa = np.zeros(Nmax + 1)
+    if symtype == "SPSU2":
+        info = write_data_spsu2(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, delta, kappa,
+                                discretization)
+        info.update({"delta": delta, "kappa": kappa})
+    elif symtype == "QSZ":
         info = write_data_qsz(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, discretization)
     elif symtype == "QS":
         info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, 1, discretization)
     else:
-        raise ValueError("symtype QS or QSZ")
+        raise ValueError("symtype QS, QSZ or SPSU2")
     p = {"Lambda": Lambda, "z": z, "discretization": discretization}
     if params:
         p.update(params)
