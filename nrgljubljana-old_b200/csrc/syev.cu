@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <numeric>
+#include <type_traits>
 
 #include "gemm_f64.cuh"
 #include "syev.cuh"
@@ -38,6 +39,7 @@ constexpr int NBB = 64;         // back-transformation block of reflectors
 constexpr int TRD_NT = 256;     // threads of the panel kernel
 constexpr int TRDC_NT = 256;    // threads of a CTA of the cluster kernel
 constexpr size_t TRDC_SMEM = 227 * 1024;  // shared memory one CTA of the cluster kernel may use
+constexpr int TRDC_CL_MAX = 16;           // largest cluster (non-portable above 8)
 constexpr double EPS = 2.220446049250313e-16;
 
 // --------------------------------------------------------------------------
@@ -1015,19 +1017,250 @@ __global__ void __launch_bounds__(TRDC1_NT) trd_cluster1_kernel(const TrdClProb*
   trdc_sync<CL>();
 }
 
+// Doubles of dynamic shared memory of the fused kernel: the held columns, v
+// twice, the running copy of the next column, y twice, the parts of y^T v
+// twice, one partial norm per warp, scalars.
+__host__ __device__ inline size_t trdc2_smem_doubles(int n, int cl) {
+  return (size_t)((n + cl - 1) / cl) * trdc_ld(n) + 5 * (size_t)n + 2 * (size_t)cl * (TRDC1_NT / 32) +
+         (TRDC1_NT / 32) + 8;
+}
+
+// The one-barrier recurrence with the rank-2 update of step c and the
+// products of step c+1 in one pass over the held columns.  Right after the
+// cluster barrier of step c every CTA holds y_c, v_c and the parts of
+// y_c^T v_c, so it can finish column c+1 (read from its owner) and form
+// v_{c+1} before it touches its own columns; then each held column j > c+1
+// is updated and, while its rows are in registers, dotted with v_{c+1}.
+// Per column: one pass over the held columns, one CTA barrier (after the
+// next column's partial norms) and one cluster barrier (after y_{c+1} and
+// the parts of y_{c+1}^T v_{c+1} reach every CTA).  v, y and the parts
+// alternate between two buffers by column parity.  The loop starts at
+// c = -1 (no update; column 0 read raw), so the first products need no
+// separate pass.  Rows above c+2 of a held column are dead after step c and
+// are not updated.  Output as trd_cluster_kernel.
+template <int CL>
+__global__ void __launch_bounds__(TRDC1_NT) trd_cluster2_kernel(const TrdClProb* __restrict__ probs) {
+  int r = 0;
+  if constexpr (CL > 1) r = (int)cooperative_groups::this_cluster().block_rank();
+  const TrdClProb P = probs[blockIdx.x / CL];
+  const int n = P.n;
+  const size_t ld = (size_t)P.ld;
+  const int lds = trdc_ld(n);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int nwarps = TRDC1_NT / 32;
+  const int ncol = r < n ? (n - r + CL - 1) / CL : 0;
+  extern __shared__ double sm[];
+  double* Acol = sm;                                        // ncol columns, ld lds
+  double* vbuf = Acol + (size_t)((n + CL - 1) / CL) * lds;  // 2 x n
+  double* cur = vbuf + 2 * (size_t)n;                       // n: column c+1 (rows c+1 .. n-1)
+  double* ybuf = cur + n;                                   // 2 x n (written by every CTA)
+  double* pbuf = ybuf + 2 * (size_t)n;                      // 2 x CL x nwarps parts of y^T v
+  double* psq = pbuf + 2 * CL * nwarps;                     // nwarps partial norms
+
+  for (int l = 0; l < ncol; ++l) {
+    const double* src = P.A + (size_t)(r + l * CL) * ld;
+    for (int i = tid; i < n; i += TRDC1_NT) Acol[(size_t)l * lds + i] = src[i];
+  }
+  // every CTA of the cluster has loaded before any of them reads another's
+  trdc_sync<CL>();
+
+  double tc = 0.0;  // tau of column c (0 for c = -1)
+  for (int c = -1; c < n - 1; ++c) {
+    const int cn = c + 1;
+    const double* v = vbuf + (size_t)((c + 2) & 1) * n;  // v_c (parity of c, kept non-negative)
+    double* vn = vbuf + (size_t)((c + 1) & 1) * n;        // v_{c+1}
+    const double* y = ybuf + (size_t)((c + 2) & 1) * n;
+    double* yn = ybuf + (size_t)((c + 1) & 1) * n;
+    const double* part = pbuf + ((c + 2) & 1) * CL * nwarps;
+    double* partn = pbuf + ((c + 1) & 1) * CL * nwarps;
+    // ---- column c+1 from its owner, corrected by step c; its partial norm ----
+    double xr[TRDC1_ROWS];
+    {
+      const double* ocol = trdc_at<CL>(Acol, cn % CL) + (size_t)(cn / CL) * lds;
+#pragma unroll
+      for (int k = 0; k < TRDC1_ROWS; ++k) {
+        const int i = cn + tid + k * TRDC1_NT;
+        xr[k] = i < n ? ocol[i] : 0.0;
+      }
+    }
+    double a2 = 0.0;
+    if (c >= 0 && tc != 0.0) {
+      double ytv = 0.0;
+      for (int q = lane; q < CL * nwarps; q += 32) ytv += part[q];
+      ytv = warp_sum(ytv);
+      a2 = -0.5 * tc * tc * ytv;
+    }
+    {
+      const double wn = (c >= 0 && tc != 0.0) ? tc * y[cn] + a2 : 0.0;
+      double sq = 0.0;
+#pragma unroll
+      for (int k = 0; k < TRDC1_ROWS; ++k) {
+        const int i = cn + tid + k * TRDC1_NT;
+        if (i < n) {
+          double x = xr[k];
+          if (c >= 0 && tc != 0.0) x -= v[i] * wn + (tc * y[i] + a2 * v[i]);
+          cur[i] = x;
+          if (i >= cn + 2) sq += x * x;
+        }
+      }
+      sq = warp_sum(sq);
+      if (lane == 0) psq[warp] = sq;
+    }
+    __syncthreads();
+    if (cn == n - 1) {
+      if (r == 0 && tid == 0) P.d[n - 1] = cur[n - 1];
+      break;
+    }
+    // ---- reflector of column c+1 (every thread, same arithmetic) ----
+    double ss = 0.0;
+#pragma unroll
+    for (int q = 0; q < nwarps; ++q) ss += psq[q];
+    const double alpha = cur[cn + 1];
+    double beta = alpha, tcn = 0.0, scal = 0.0;
+    if (ss != 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + ss), alpha);
+      tcn = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    if (r == 0 && tid == 0) {
+      P.d[cn] = cur[cn];
+      P.e[cn] = beta;
+      P.tau[cn] = tcn;
+    }
+    const bool own = r == cn % CL;
+    for (int i = cn + 1 + tid; i < n; i += TRDC1_NT) {
+      const double vi = (i == cn + 1) ? 1.0 : cur[i] * scal;
+      vn[i] = vi;
+      if (own && i >= cn + 2) P.A[i + (size_t)cn * ld] = vi;
+    }
+    // ---- update of the held columns j > c+1 by step c, products with v_{c+1} ----
+    const int l1 = (c + 2 - r + CL - 1) / CL > 0 ? (c + 2 - r + CL - 1) / CL : 0;
+    const bool upd = c >= 0 && tc != 0.0;
+    double sp = 0.0;
+    for (int l = l1 + 4 * warp; l < ncol; l += 4 * nwarps) {
+      const int nl = min(4, ncol - l);
+      double vj[4], wj[4], acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int j = r + (l + min(k, nl - 1)) * CL;
+        vj[k] = upd ? v[j] : 0.0;
+        wj[k] = upd ? tc * y[j] + a2 * v[j] : 0.0;
+      }
+      double* a0 = Acol + (size_t)l * lds;
+      int i = cn + 1 + lane;
+      for (; i + 32 < n; i += 64) {
+        const double p0 = (i == cn + 1) ? 1.0 : cur[i] * scal;
+        const double p1 = cur[i + 32] * scal;
+        double x[8];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          x[k] = k < nl ? a0[(size_t)k * lds + i] : 0.0;
+          x[4 + k] = k < nl ? a0[(size_t)k * lds + i + 32] : 0.0;
+        }
+        if (upd) {
+          const double v0 = v[i], v1 = v[i + 32];
+          const double w0 = tc * y[i] + a2 * v0, w1 = tc * y[i + 32] + a2 * v1;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            x[k] -= v0 * wj[k] + w0 * vj[k];
+            x[4 + k] -= v1 * wj[k] + w1 * vj[k];
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (k < nl) {
+              a0[(size_t)k * lds + i] = x[k];
+              a0[(size_t)k * lds + i + 32] = x[4 + k];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[k] += x[k] * p0 + x[4 + k] * p1;
+      }
+      if (i < n) {
+        const double p0 = (i == cn + 1) ? 1.0 : cur[i] * scal;
+        double x[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) x[k] = k < nl ? a0[(size_t)k * lds + i] : 0.0;
+        if (upd) {
+          const double v0 = v[i];
+          const double w0 = tc * y[i] + a2 * v0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) x[k] -= v0 * wj[k] + w0 * vj[k];
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if (k < nl) a0[(size_t)k * lds + i] = x[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[k] += x[k] * p0;
+      }
+#pragma unroll
+      for (int o2 = 16; o2 > 0; o2 >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o2);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (k >= nl) continue;
+        const int j = r + (l + k) * CL;
+        if (lane < CL) trdc_at<CL>(yn, lane)[j] = acc[k];
+        sp += acc[k] * ((j == cn + 1) ? 1.0 : cur[j] * scal);
+      }
+    }
+    if (lane < CL) trdc_at<CL>(partn, lane)[r * nwarps + warp] = sp;
+    tc = tcn;
+    trdc_sync<CL>();
+  }
+  // no CTA leaves while another may still read its shared memory
+  trdc_sync<CL>();
+}
+
 // Launch configuration of the cluster kernel for `nprob` blocks.  The
 // kernel's attributes (largest dynamic shared memory, non-portable cluster
 // size) are set once per device, at the largest size any launch uses, by the
 // solver's constructor (set_attr): setting them per launch to the launch's
 // own size would race between solver instances on other threads.
-// The cluster kernel of CL CTAs: one or two cluster barriers per column.
+// The cluster kernel of CL CTAs: 0 two cluster barriers per column, 1 one,
+// 2 one with the update and the next products fused.  The default (1) is
+// built for every cluster size 1..16, the comparison forms for the powers
+// of two only.
 template <int CL>
-void (*trdc_kernel(bool one))(const TrdClProb*) {
-  return one ? trd_cluster1_kernel<CL> : trd_cluster_kernel<CL>;
+void (*trdc_kernel(int variant))(const TrdClProb*) {
+  if constexpr ((CL & (CL - 1)) == 0) {
+    if (variant == 2) return trd_cluster2_kernel<CL>;
+    if (variant == 0) return trd_cluster_kernel<CL>;
+  }
+  return trd_cluster1_kernel<CL>;
+}
+
+// Whether the cluster kernel of this variant is built for CL CTAs.
+inline bool trdc_size_built(int variant, int CL) {
+  return CL >= 1 && CL <= TRDC_CL_MAX && (variant == 1 || (CL & (CL - 1)) == 0);
+}
+
+// f(std::integral_constant<int, CL>{}) for a runtime cluster size 1..16.
+template <class F>
+auto trdc_with_cl(int CL, F&& f) {
+  switch (CL) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    case 7: return f(std::integral_constant<int, 7>{});
+    case 8: return f(std::integral_constant<int, 8>{});
+    case 9: return f(std::integral_constant<int, 9>{});
+    case 10: return f(std::integral_constant<int, 10>{});
+    case 11: return f(std::integral_constant<int, 11>{});
+    case 12: return f(std::integral_constant<int, 12>{});
+    case 13: return f(std::integral_constant<int, 13>{});
+    case 14: return f(std::integral_constant<int, 14>{});
+    case 15: return f(std::integral_constant<int, 15>{});
+    default: return f(std::integral_constant<int, 16>{});
+  }
 }
 
 template <int CL>
-cudaError_t trdc_config(bool one, size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int nprob,
+cudaError_t trdc_config(int one, size_t smem, cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int nprob,
                         cudaStream_t st, bool set_attr) {
   cfg = cudaLaunchConfig_t{};
   cfg.gridDim = dim3((unsigned)(nprob * CL));
@@ -1051,7 +1284,7 @@ cudaError_t trdc_config(bool one, size_t smem, cudaLaunchConfig_t& cfg, cudaLaun
 // (0: this cluster size is not usable here); sets the kernel's attributes
 // for launches of up to `smem` bytes.
 template <int CL>
-int trdc_max_clusters(bool one, size_t smem) {
+int trdc_max_clusters(int one, size_t smem) {
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute at[1];
   if (trdc_config<CL>(one, smem, cfg, at, 1, nullptr, true) != cudaSuccess) {
@@ -1067,7 +1300,7 @@ int trdc_max_clusters(bool one, size_t smem) {
 }
 
 template <int CL>
-cudaError_t trdc_launch(bool one, const TrdClProb* d, int nprob, size_t smem, cudaStream_t st) {
+cudaError_t trdc_launch(int one, const TrdClProb* d, int nprob, size_t smem, cudaStream_t st) {
   cudaLaunchConfig_t cfg;
   cudaLaunchAttribute at[1];
   cudaError_t e = trdc_config<CL>(one, smem, cfg, at, nprob, st, false);
@@ -1754,23 +1987,31 @@ SyevBatched::SyevBatched() {
   // (comparisons, or a device where cluster launches are unavailable)
   const char* path = getenv("NRGB_TRD_PATH");
   if (path && strcmp(path, "panel") == 0) cl_smem_ = 0;
-  // NRGB_TRDC_BARRIERS=2 selects the cluster kernel with two cluster
-  // barriers per column (comparisons); the default has one
+  // the cluster kernel (default: one barrier per column); for comparisons
+  // NRGB_TRDC_BARRIERS=2 selects the form with two cluster barriers per
+  // column and NRGB_TRDC_FUSED=1 the one-barrier form with the update and
+  // the next products fused (faster for a block alone, slower when many
+  // clusters run at once)
   const char* nb = getenv("NRGB_TRDC_BARRIERS");
-  cl_one_ = !(nb && strcmp(nb, "2") == 0);
+  const char* nf = getenv("NRGB_TRDC_FUSED");
+  cl_one_ = (nb && strcmp(nb, "2") == 0) ? 0 : (nf && strcmp(nf, "1") == 0) ? 2 : 1;
+  // NRGB_TRDC_POW2=1 restricts the default kernel to clusters of 1, 2, 4, 8
+  // and 16 CTAs (comparisons); otherwise a block takes the smallest cluster
+  // of any size that holds it
+  const char* np2 = getenv("NRGB_TRDC_POW2");
+  const bool pow2 = np2 && strcmp(np2, "1") == 0;
   if (cl_smem_ > 0) {
-    cl_max_[0] = trdc_max_clusters<1>(cl_one_, cl_smem_);
-    cl_max_[1] = trdc_max_clusters<2>(cl_one_, cl_smem_);
-    cl_max_[2] = trdc_max_clusters<4>(cl_one_, cl_smem_);
-    cl_max_[3] = trdc_max_clusters<8>(cl_one_, cl_smem_);
-    cl_max_[4] = trdc_max_clusters<16>(cl_one_, cl_smem_);
+    for (int cl = 1; cl <= TRDC_CL_MAX; ++cl) {
+      if (!trdc_size_built(cl_one_, cl) || (pow2 && (cl & (cl - 1)) != 0)) continue;
+      cl_max_[cl] = trdc_with_cl(cl, [&](auto c) { return trdc_max_clusters<decltype(c)::value>(cl_one_, cl_smem_); });
+    }
   }
-  // largest block the cluster kernel holds (the one-barrier kernel also
-  // reads at most TRDC1_ROWS rows of a column per thread)
-  for (int k = 4; k >= 0 && cl_nmax_ == 0; --k) {
-    if (cl_max_[k] <= 0) continue;
+  // largest block the cluster kernel holds (the one-barrier kernels also
+  // read at most TRDC1_ROWS rows of a column per thread)
+  for (int cl = TRDC_CL_MAX; cl >= 1 && cl_nmax_ == 0; --cl) {
+    if (cl_max_[cl] <= 0) continue;
     int n = 1;
-    while (trdc_bytes(n + 1, 1 << k) <= cl_smem_ && (!cl_one_ || n + 1 <= TRDC1_ROWS * TRDC1_NT)) ++n;
+    while (trdc_bytes(n + 1, cl) <= cl_smem_ && (!cl_one_ || n + 1 <= TRDC1_ROWS * TRDC1_NT)) ++n;
     cl_nmax_ = n > SMALL_N ? n : 0;
   }
   for (int i = 0; i < NAUX; ++i) {
@@ -1858,7 +2099,9 @@ size_t SyevBatched::workspace_bytes(const std::vector<int>& ns) {
 }
 
 size_t SyevBatched::trdc_bytes(int n, int cl) const {
-  return (cl_one_ ? trdc1_smem_doubles(n, cl) : trdc_smem_doubles(n, cl)) * sizeof(double);
+  return (cl_one_ == 2 ? trdc2_smem_doubles(n, cl) : cl_one_ == 1 ? trdc1_smem_doubles(n, cl)
+                                                                   : trdc_smem_doubles(n, cl)) *
+         sizeof(double);
 }
 
 int SyevBatched::cl_use() const {
@@ -1993,18 +2236,19 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
     // blocks follow on the main stream.
     std::vector<char> via_cluster(nbig, 0);
     // Launch the cluster tridiagonalisation for `list`: groups by cluster size
-    // (single-CTA clusters split at n = 64, 96, 128), concurrently on side
-    // streams, joined into `st`.  Every entry must fit some cluster size.
+    // (the smallest cluster whose shared memory holds the block; single-CTA
+    // clusters split at n = 64, 96, 128), concurrently on side streams,
+    // joined into `st`.  Every entry must fit some cluster size.
     auto launch_clusters = [&](const std::vector<TrdClProb>& list) {
-      constexpr int NG = 8;
+      constexpr int NG = TRDC_CL_MAX + 3;  // group 0..3: one CTA; group CL + 2: CL CTAs
       std::vector<TrdClProb> grp[NG];
       size_t gsmem[NG] = {};
       for (const TrdClProb& t : list) {
         const int n = t.n;
-        for (int k = 0; k < 5; ++k) {
-          const size_t bytes = trdc_bytes(n, 1 << k);
-          if (cl_max_[k] > 0 && bytes <= cl_smem_) {
-            const int g = k > 0 ? k + 3 : (n <= 64 ? 0 : n <= 96 ? 1 : n <= 128 ? 2 : 3);
+        for (int cl = 1; cl <= TRDC_CL_MAX; ++cl) {
+          const size_t bytes = trdc_bytes(n, cl);
+          if (cl_max_[cl] > 0 && bytes <= cl_smem_) {
+            const int g = cl > 1 ? cl + 2 : (n <= 64 ? 0 : n <= 96 ? 1 : n <= 128 ? 2 : 3);
             grp[g].push_back(t);
             gsmem[g] = std::max(gsmem[g], bytes);
             break;
@@ -2031,14 +2275,11 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         KernelStats::get().add_work("trd_cluster", fl);
         KernelStats::get().add_work("trd_cluster_hbm", by);
         const int np = (int)grp[g].size();
-        const int k = g > 3 ? g - 3 : 0;
+        const int cl = g > 3 ? g - 2 : 1;
         cudaError_t e = cudaSuccess;
-        NRGB_LAUNCH("trd_cluster", sx,
-                    e = (k == 0)   ? trdc_launch<1>(cl_one_, dg[g], np, gsmem[g], sx)
-                        : (k == 1) ? trdc_launch<2>(cl_one_, dg[g], np, gsmem[g], sx)
-                        : (k == 2) ? trdc_launch<4>(cl_one_, dg[g], np, gsmem[g], sx)
-                        : (k == 3) ? trdc_launch<8>(cl_one_, dg[g], np, gsmem[g], sx)
-                                   : trdc_launch<16>(cl_one_, dg[g], np, gsmem[g], sx));
+        NRGB_LAUNCH("trd_cluster", sx, e = trdc_with_cl(cl, [&](auto c) {
+                      return trdc_launch<decltype(c)::value>(cl_one_, dg[g], np, gsmem[g], sx);
+                    }));
         NRGB_CUDA(e);
         ++launches_;
         ++used;

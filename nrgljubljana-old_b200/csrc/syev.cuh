@@ -82,10 +82,10 @@ class SyevBatched : public EigSolver {
   bool inject_shortfall_ = false;
   int coop_ctas_ = 0;
   int sms_ = 0;
-  int cl_max_[5] = {0, 0, 0, 0, 0};  // resident clusters of 1, 2, 4, 8, 16 CTAs (0: not usable)
+  int cl_max_[17] = {};               // resident clusters of CL = 1..16 CTAs (0: not usable or not built)
   size_t cl_smem_ = 0;                // shared memory per CTA of the cluster kernel
   int cl_nmax_ = 0;                   // largest block it holds (0: cluster path off)
-  bool cl_one_ = true;                // one cluster barrier per column (else two)
+  int cl_one_ = 1;                    // cluster kernel: 0 two barriers per column, 1 one, 2 one and fused
   // dynamic shared memory of one CTA of the cluster kernel in use
   size_t trdc_bytes(int n, int cl) const;
   // blocks up to this size go to the cluster kernel whole: the capacity, or

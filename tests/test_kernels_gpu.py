@@ -1,6 +1,8 @@
 """Numerics of the CUDA kernels through the C ABI, against FP64 references:
 torch float64 matmul for the grouped GEMM, LAPACK (numpy eigh) for the
 batched eigensolver (eigenvalues, residual, orthogonality)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -77,12 +79,14 @@ def _random_sym(n, rng, kind):
 
 
 # covers the warp path (n <= 32), the cluster path (one cluster of 1..16 CTAs
-# per block; single-CTA launches split at 64, 96, 128; with the one-barrier
-# kernel the cluster size changes after 167, 235, 329, 461, and blocks above
-# 640 take the cooperative panel path; 168, 237, 333, 469 and 656 are the
-# two-barrier kernel's limits) and the panel path
+# per block, the smallest that holds it: the size changes after 167, 235,
+# 287, 329, 367, 402, 433, 461, 486, 511, 539, 559, 583, 602, 619; single-CTA
+# launches split at 64, 96, 128; blocks above 640 take the cooperative panel
+# path; 168, 237, 333, 469 and 656 are the two-barrier kernel's limits) and
+# the panel path
 SIZES = [1, 2, 3, 5, 16, 31, 32, 33, 40, 64, 65, 96, 97, 100, 128, 129, 167, 168, 169, 235, 236, 237, 238, 257,
-         329, 330, 333, 334, 461, 462, 469, 470, 600, 640, 641, 656, 657, 1100]
+         287, 288, 329, 330, 333, 334, 367, 368, 402, 403, 433, 434, 461, 462, 469, 470, 486, 487, 511, 512, 539,
+         540, 559, 560, 583, 584, 600, 602, 603, 619, 620, 640, 641, 656, 657, 1100]
 
 
 @pytest.mark.parametrize("kind", ["gauss", "logspaced", "degenerate"])
@@ -100,6 +104,39 @@ def test_syev_batched_host_api(ctx, kind):
         assert res <= 1e-13 * nrm * max(10, n)
         orth = np.abs(Zi.T @ Zi - np.eye(n)).max()
         assert orth <= 1e-13 * max(10, n)
+
+
+@pytest.mark.parametrize("env", [{"NRGB_TRDC_BARRIERS": "2"}, {"NRGB_TRDC_FUSED": "1"}, {"NRGB_TRDC_POW2": "1"}])
+def test_syev_cluster_kernel_variants(env):
+    """The other forms of the cluster tridiagonalisation (two cluster
+    barriers per column; one barrier with the update and the next products
+    fused; clusters of 1, 2, 4, 8, 16 CTAs only), selected when a context is
+    created, solve the cluster-sized blocks to the same bounds."""
+    import nrgb
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        c = nrgb.Context(0)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    try:
+        rng = np.random.default_rng(5)
+        mats = [_random_sym(n, rng, kind) for n in (33, 100, 167, 200, 300, 461, 600, 640, 700)
+                for kind in ("gauss", "degenerate")]
+        w, Z = c.syev_batched(mats)
+    finally:
+        c.close()
+    for A, wi, Zi in zip(mats, w, Z):
+        n = A.shape[0]
+        ref = np.linalg.eigvalsh(A)
+        nrm = max(np.abs(ref).max(), 1e-300)
+        assert np.max(np.abs(wi - ref)) <= 1e-13 * nrm * max(10, n)
+        assert np.abs(A @ Zi - Zi * wi).max() <= 1e-13 * nrm * max(10, n)
+        assert np.abs(Zi.T @ Zi - np.eye(n)).max() <= 1e-13 * max(10, n)
 
 
 def test_syev_per_block_mode_matches_batched(ctx):
