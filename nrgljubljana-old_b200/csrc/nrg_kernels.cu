@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(SPEC_NT) spec_fdm_kernel(const SpecFdmPair* __
       const bool idisc = i >= P.reti, jdisc = j >= P.retj;
       // greater correlation function
       if (idisc) {
-        wg = P.sf * o1 * P.op2[io] * wnf * exp(-Ei / T);  // A3, A2
+        wg = P.sf * o1 * P.op2[io] * wnf * P.XEi[i];  // A3, A2
         ong = true;
       } else if (jdisc) {
         wg = P.sf * o1 * P.O2R[(size_t)j + (size_t)i * P.allj];  // A1
@@ -192,13 +192,13 @@ __global__ void __launch_bounds__(SPEC_NT) spec_fdm_kernel(const SpecFdmPair* __
       }
       // lesser correlation function
       if (idisc && jdisc) {
-        wl = P.sf * o1 * P.op2[io] * msign * wnf * exp(-Ej / T);  // B3
+        wl = P.sf * o1 * P.op2[io] * msign * wnf * P.XEj[j];  // B3
         onl = true;
       } else if (idisc && !jdisc) {
         wl = P.sf * o1 * P.RO2[(size_t)j + (size_t)i * P.retj] * msign;  // B2
         onl = true;
       } else if (!idisc && jdisc) {
-        wl = P.sf * o1 * P.op2[io] * msign * wnf * exp(-Ej / T);  // B1
+        wl = P.sf * o1 * P.op2[io] * msign * wnf * P.XEj[j];  // B1
         onl = true;
       }
     }

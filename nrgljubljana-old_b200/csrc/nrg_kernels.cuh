@@ -68,6 +68,8 @@ struct SpecFdmPair {
   const double* RO2;   // rho_j * op2[:retj, :alli] (retj x alli, ld retj), may be null
   const double* Ej;    // absolute energies (shifted by the ground state)
   const double* Ei;
+  const double* XEj;   // their Boltzmann factors exp(-E/T), one per state
+  const double* XEi;
   int ldo, allj, alli, retj, reti;
   double sf;
 };

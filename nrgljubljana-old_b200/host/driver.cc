@@ -1264,17 +1264,22 @@ struct NrgDriver::Impl {
       t_recalc += secs(t0);
       sections["sweep2 recalc"] += secs(t0);
       t0 = Clock::now();
-      // absolute energies shifted by the absolute ground state (FDM)
-      std::map<Invar, double*> absdev;
+      // absolute energies shifted by the absolute ground state (FDM), and
+      // their Boltzmann factors exp(-E/T) once per state, not per matrix
+      // element of the spectral sums
+      std::map<Invar, double*> absdev, boltzdev;
       if (P.fdm) {
         wstage.clear();
         for (const auto& kv : S.blocks)
           for (int r = 0; r < kv.second.dim; ++r) wstage.push_back(kv.second.absE[r] - GSenergy);
+        const size_t ns = wstage.size();
+        for (size_t r = 0; r < ns; ++r) wstage.push_back(exp(-wstage[r] / P.T));
         double* d = nslab->alloc(wstage.size());
         NRGB_CUDA(cudaMemcpyAsync(d, wstage.data(), wstage.size() * sizeof(double), cudaMemcpyHostToDevice, st));
         h2d += wstage.size() * sizeof(double);
         for (const auto& kv : S.blocks) {
           absdev[kv.first] = d;
+          boltzdev[kv.first] = d + ns;
           d += kv.second.dim;
         }
       }
@@ -1350,7 +1355,8 @@ struct NrgDriver::Impl {
                 g.out(RO2, retj, retj, alli, 0.0, {seg(rj->second.p, rj->second.ld, 0, a2->second.p, a2->second.ld, 0, retj, 1.0)});
               }
               pr.push_back(SpecFdmPair{a1->second.p, a2->second.p, O2R, RO2, absdev.at(bj.first),
-                                       absdev.at(bi.first), a1->second.ld, allj, alli, retj, reti, sf});
+                                       absdev.at(bi.first), boltzdev.at(bj.first), boltzdev.at(bi.first),
+                                       a1->second.ld, allj, alli, retj, reti, sf});
               maxe = std::max(maxe, allj * alli);
             }
           run_gemm(g);
