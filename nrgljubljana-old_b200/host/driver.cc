@@ -1593,8 +1593,8 @@ struct NrgDriver::Impl {
         throw std::runtime_error("symmetry type QSZ: only the spectral functions of doublet operators are built");
       sym.reset(new SymmetryQSZ());
     } else if (D.symtype == "SPSU2") {
-      if (D.channels != 1) throw std::runtime_error("symmetry type SPSU2: one channel is built");
-      sym.reset(new SymmetrySPSU2());
+      if (D.channels != 1 && D.channels != 2) throw std::runtime_error("symmetry type SPSU2: 1 and 2 channels are built");
+      sym.reset(new SymmetrySPSU2(D.channels));
     } else {
       throw std::runtime_error("symmetry type " + D.symtype + " is not built (QS, QSZ, SPSU2)");
     }

@@ -26,6 +26,14 @@ const ComboDef COMBOS_2CH[] = {{{0, 0}, 0.0, 2, 0},   {{0, 1}, 0.5, 1, -1},  {{0
                                {{1, 2}, 0.5, -1, 1},  {{2, 1}, 0.5, -1, -1}, {{2, 1}, 0.5, -1, 1},
                                {{2, 2}, 0.0, -2, 0}};
 
+// The same for SPSU2 (no charge: every In is (0, dss)), in the order of
+// coefnew/spsu2/spsu2-<P>ch-In2.dat: site singlets, doublets, the triplet.
+const ComboDef SPSU2_1CH[] = {{{0, 0}, 0.0, 0, 0}, {{2, 0}, 0.0, 0, 0}, {{1, 0}, 0.5, 0, -1}, {{1, 0}, 0.5, 0, 1}};
+const ComboDef SPSU2_2CH[] = {{{0, 0}, 0.0, 0, 0},  {{0, 2}, 0.0, 0, 0},  {{1, 1}, 0.0, 0, 0},  {{2, 0}, 0.0, 0, 0},
+                              {{2, 2}, 0.0, 0, 0},  {{0, 1}, 0.5, 0, -1}, {{0, 1}, 0.5, 0, 1},  {{1, 0}, 0.5, 0, -1},
+                              {{1, 0}, 0.5, 0, 1},  {{1, 2}, 0.5, 0, -1}, {{1, 2}, 0.5, 0, 1},  {{2, 1}, 0.5, 0, -1},
+                              {{2, 1}, 0.5, 0, 1},  {{1, 1}, 1.0, 0, -2}, {{1, 1}, 1.0, 0, 0},  {{1, 1}, 1.0, 0, 2}};
+
 // Phase of each site multiplet relative to the highest-weight state whose
 // first nonzero amplitude (bit k = mode k = 2*channel + spin, up first) is
 // positive: the reference's conventions.
@@ -62,10 +70,10 @@ double clebsch_gordan(double j1, double m1, double j2, double m2, double J, doub
   return s;
 }
 
-QSCoupling::QSCoupling(int channels) : P_(channels) {
+QSCoupling::QSCoupling(int channels, bool spsu2) : P_(channels), spsu2_(spsu2) {
   if (channels != 1 && channels != 2) throw std::runtime_error("QS symmetry: tables for 1 and 2 channels");
   dim_ = 1 << (2 * P_);
-  const ComboDef* defs = P_ == 1 ? COMBOS_1CH : COMBOS_2CH;
+  const ComboDef* defs = spsu2 ? (P_ == 1 ? SPSU2_1CH : SPSU2_2CH) : (P_ == 1 ? COMBOS_1CH : COMBOS_2CH);
   const int n = P_ == 1 ? 4 : 16;
   for (int i = 0; i < n; ++i) {
     Combo c;
@@ -76,7 +84,7 @@ QSCoupling::QSCoupling(int channels) : P_(channels) {
     in_.push_back(c.In);
     int ne = 0;
     for (int x : c.occ) ne += x;
-    qn_.push_back({ne - P_, (int)lround(2 * c.s) + 1});
+    qn_.push_back({spsu2 ? 0 : ne - P_, (int)lround(2 * c.s) + 1});
   }
   // creation operators (Jordan-Wigner order of the site's 2P modes)
   const int nm = 2 * P_;
@@ -92,6 +100,23 @@ QSCoupling::QSCoupling(int channels) : P_(channels) {
     const std::pair<int, int> k2{key, (int)lround(2 * c.s)};
     if (!mult_.count(k2)) mult_[k2] = multiplet(c.occ, c.s, site_sign(P_, c.occ, c.s));
   }
+  // the site's pairing operator f^dag_up f^dag_dn + h.c. per channel (SPSU2)
+  if (spsu2)
+    for (int ch = 0; ch < P_; ++ch) {
+      const Vec& a = cd_[2 * ch];
+      const Vec& b = cd_[2 * ch + 1];
+      Vec pr((size_t)dim_ * dim_, 0.0);
+      for (int r = 0; r < dim_; ++r)
+        for (int k = 0; k < dim_; ++k) {
+          const double x = a[(size_t)r * dim_ + k];
+          if (x == 0.0) continue;
+          for (int c2 = 0; c2 < dim_; ++c2) pr[(size_t)r * dim_ + c2] += x * b[(size_t)k * dim_ + c2];
+        }
+      Vec sym(pr);
+      for (int r = 0; r < dim_; ++r)
+        for (int c2 = 0; c2 < dim_; ++c2) sym[(size_t)r * dim_ + c2] += pr[(size_t)c2 * dim_ + r];
+      pair_.push_back(sym);
+    }
 }
 
 QSCoupling::Vec QSCoupling::apply(const Vec& op, const Vec& v) const {
@@ -276,15 +301,43 @@ const std::vector<OffdiagTerm>& QSCoupling::offdiag(int ss) {
   const double S = (ss - 1) / 2.0;
   std::vector<OffdiagTerm> out;
   const int n = combs();
+  // QS: the combinations are ordered by the site's electrons, so the hopping
+  // connects i < j only; SPSU2: every ordered pair, and the anomalous
+  // hopping f^dag_{N,up} f^dag_{N+1,dn} - f^dag_{N,dn} f^dag_{N+1,up}
   for (int i = 0; i < n; ++i)
-    for (int j = i + 1; j < n; ++j)
+    for (int j = spsu2_ ? 0 : i + 1; j < n; ++j) {
+      if (i == j) continue;
       for (int ch = 0; ch < P_; ++ch) {
         // sum over spin of f^dag_{N,ch,sigma} f_{N+1,ch,sigma}: the site's
         // annihilator is the transpose of its creation operator
-        double v = elem(i, S, S, j, S, S, 0.5, 0.5, &cd_[2 * ch], true, true) +
-                   elem(i, S, S, j, S, S, 0.5, -0.5, &cd_[2 * ch + 1], true, true);
-        if (fabs(v) > 1e-13) out.push_back({i + 1, j + 1, ch, v});
+        const double v = elem(i, S, S, j, S, S, 0.5, 0.5, &cd_[2 * ch], true, true) +
+                         elem(i, S, S, j, S, S, 0.5, -0.5, &cd_[2 * ch + 1], true, true);
+        if (fabs(v) > 1e-13) out.push_back({i + 1, j + 1, ch, v, 0});
       }
+    }
+  if (spsu2_) {
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        if (i == j) continue;
+        for (int ch = 0; ch < P_; ++ch) {
+          const double v = elem(i, S, S, j, S, S, 0.5, 0.5, &cd_[2 * ch + 1], false, true) -
+                           elem(i, S, S, j, S, S, 0.5, -0.5, &cd_[2 * ch], false, true);
+          if (fabs(v) > 1e-13) out.push_back({i + 1, j + 1, ch, v, 1});
+        }
+      }
+    // on-site pairing between combinations of one ancestor, in units of
+    // 2 delta; the reference writes the pairing of every channel after the
+    // first with the opposite sign along the chain and its tables with the
+    // opposite sign to match (initial.m, bcsgap section).  The element does
+    // not depend on the subspace; it is taken at S = 2.
+    for (int ch = 0; ch < P_; ++ch)
+      for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) {
+          if (combos_[i].In != combos_[j].In) continue;
+          const double v = elem(i, 2.0, 2.0, j, 2.0, 2.0, -1.0, 0.0, &pair_[ch], false, false);
+          if (fabs(v) > 1e-13) out.push_back({i + 1, j + 1, ch, (ch == 0 ? 0.5 : -0.5) * v, 2});
+        }
+  }
   return off_[ss] = out;
 }
 
@@ -293,7 +346,7 @@ const std::vector<RecalcTable>& QSCoupling::recalc_f(const Invar& Ip) {
   if (it != rf_.end()) return it->second;
   std::vector<RecalcTable> out;
   for (int dss : {1, -1}) {
-    const Invar I1{Ip.first + 1, Ip.second + dss};
+    const Invar I1{spsu2_ ? 0 : Ip.first + 1, Ip.second + dss};
     if (I1.second < 1) continue;
     for (int ch = 0; ch < P_; ++ch) {
       RecalcTable t{I1, ch, {}};
@@ -330,7 +383,8 @@ const std::vector<RecalcTable>& QSCoupling::doublet(const Invar& I1) {
   auto it = dbl_.find(I1);
   if (it != dbl_.end()) return it->second;
   std::vector<RecalcTable> out;
-  const Invar plus{I1.first - 1, I1.second + 1}, minus{I1.first - 1, I1.second - 1};
+  const int q = spsu2_ ? 0 : I1.first - 1;
+  const Invar plus{q, I1.second + 1}, minus{q, I1.second - 1};
   out.push_back({plus, 0, chain_op(I1, plus, 0.5, true)});
   if (I1.second > 1) out.push_back({minus, 0, chain_op(I1, minus, 0.5, true)});
   return dbl_[I1] = out;

@@ -33,9 +33,12 @@ struct RecalcTable { Invar Ip; int ch; std::vector<RecalcRow> rows; };
 // <j1 m1; j2 m2 | J M> (Racah's formula; spins and projections as doubles)
 double clebsch_gordan(double j1, double m1, double j2, double m2, double J, double M);
 
+// With spsu2 set: the SPSU2 tables (spin SU(2), charge not conserved; the
+// combinations of coefnew/spsu2/spsu2-<P>ch-In2.dat; offdiag also returns
+// the anomalous hopping (kind 1) and the on-site pairing (kind 2) terms).
 class QSCoupling {
  public:
-  explicit QSCoupling(int channels);
+  explicit QSCoupling(int channels, bool spsu2 = false);
   int combs() const { return (int)combos_.size(); }
   const std::vector<Invar>& In() const { return in_; }
   const std::vector<Invar>& QN() const { return qn_; }
@@ -59,6 +62,8 @@ class QSCoupling {
     double Sa = 0;
   };
   int P_, dim_;
+  bool spsu2_ = false;
+  std::vector<Vec> pair_;               // per channel: f^dag_up f^dag_dn + h.c. of the site (SPSU2)
   std::vector<Combo> combos_;
   std::vector<Invar> in_, qn_;
   std::vector<Vec> cd_;                 // creation operators, dim x dim, row-major

@@ -213,13 +213,23 @@ class SymmetryQS : public Symmetry {
 // Thermodynamics column <Sz^2> (calculate_TD, src/sym-SPSU2.cc:81-94).
 class SymmetrySPSU2 : public Symmetry {
  public:
-  SymmetrySPSU2() {
+  // One channel: the closed forms below; two channels: the tables derived by
+  // QSCoupling in its SPSU2 mode (16 combinations of coefnew/spsu2/
+  // spsu2-2ch-In2.dat), checked against the reference's by the tests.
+  explicit SymmetrySPSU2(int channels = 1) {
+    if (channels == 2) {
+      cpl_.reset(new QSCoupling(2, true));
+      in_ = cpl_->In();
+      qn_ = cpl_->QN();
+      return;
+    }
+    if (channels != 1) throw std::runtime_error("SPSU2 symmetry: this build provides the 1- and 2-channel tables");
     in_ = {{0, 0}, {0, 0}, {0, -1}, {0, 1}};
     qn_ = {{0, 1}, {0, 1}, {0, 2}, {0, 2}};
   }
   std::string name() const override { return "SPSU2"; }
   std::string label(const Invar& I) const override { return std::to_string(I.second); }
-  int combs() const override { return 4; }
+  int combs() const override { return cpl_ ? cpl_->combs() : 4; }
   const std::vector<Invar>& In() const override { return in_; }
   const std::vector<Invar>& QN() const override { return qn_; }
   int mult(const Invar& I) const override { return I.second; }
@@ -232,15 +242,20 @@ class SymmetrySPSU2 : public Symmetry {
   Invar triplet() const override { return {0, 3}; }
 
   std::vector<OffdiagTerm> offdiag(const Invar& I) const override {
+    if (cpl_) return cpl_->offdiag(I.second);
     const double ss = I.second;
     const double a = sqrt((ss - 1) / ss), b = sqrt((ss + 1) / ss);
     return {{1, 3, 0, 1.0, 0}, {1, 4, 0, 1.0, 0}, {3, 2, 0, -a, 0}, {4, 2, 0, b, 0},
             {2, 3, 0, 1.0, 1}, {2, 4, 0, 1.0, 1}, {3, 1, 0, a, 1},  {4, 1, 0, -b, 1},
             {1, 2, 0, -0.5, 2}};
   }
-  std::vector<DiagTerm> diag() const override { return {{1, 0, 0.0}, {2, 0, 2.0}, {3, 0, 1.0}, {4, 0, 1.0}}; }
+  std::vector<DiagTerm> diag() const override {
+    if (cpl_) return cpl_->diag();
+    return {{1, 0, 0.0}, {2, 0, 2.0}, {3, 0, 1.0}, {4, 0, 1.0}};
+  }
 
   std::vector<RecalcTable> recalc_f(const Invar& Ip) const override {
+    if (cpl_) return cpl_->recalc_f(Ip);
     const int ssp = Ip.second;
     std::vector<RecalcTable> t;
     t.push_back({{0, ssp + 1}, 0, {{2, 4, -sqrt(double(ssp) / (ssp + 1))}, {3, 1, 1.0}}});
@@ -248,6 +263,7 @@ class SymmetrySPSU2 : public Symmetry {
     return t;
   }
   std::vector<RecalcTable> recalc_doublet(const Invar& I1) const override {
+    if (cpl_) return cpl_->doublet(I1);
     const int ss1 = I1.second;
     const double c = sqrt(double(ss1 - 1) * (ss1 + 1)) / ss1;
     std::vector<RecalcTable> t;
@@ -257,6 +273,7 @@ class SymmetrySPSU2 : public Symmetry {
     return t;
   }
   std::vector<RecalcTable> recalc_triplet(const Invar& I1) const override {
+    if (cpl_) return cpl_->triplet(I1);
     const int ss1 = I1.second;
     const double S = (ss1 - 1) / 2.0;
     std::vector<RecalcTable> t;
@@ -310,6 +327,7 @@ class SymmetrySPSU2 : public Symmetry {
   }
 
  private:
+  std::unique_ptr<QSCoupling> cpl_;  // derived tables (2 channels)
   std::vector<Invar> in_, qn_;
 };
 

@@ -706,14 +706,17 @@ def decompose_spsu2(m: ClusterModel, tol: float = 1e-9) -> List[Subspace]:
 def write_data_spsu2(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: int,
                      xi: np.ndarray, zeta: np.ndarray, delta: np.ndarray, kappa: np.ndarray,
                      discretization: str = "Y") -> dict:
-    """Write a version-9 `data` file of the SPSU2 symmetry (one channel):
-    subspaces labelled by SS alone, reduced matrix elements <SS1||a^dag||SS2>
-    of f_0 and of the doublet operators for |SS1 - SS2| = 1 in the
-    Wigner-Eckart normalisation of QS (ireducMatrixSpeedy, initial.m:2089),
-    singlet and triplet operators, the chain tables z (xi, zeta) and Z (delta:
-    on-site pairing, kappa: anomalous hopping; src/nrg.cc:3383-3386)."""
-    if len(m.f_orbitals) != 1:
-        raise ValueError("SPSU2 data: one channel")
+    """Write a version-9 `data` file of the SPSU2 symmetry (one or two
+    channels): subspaces labelled by SS alone, reduced matrix elements
+    <SS1||a^dag||SS2> of f_0 of each channel and of the doublet operators for
+    |SS1 - SS2| = 1 in the Wigner-Eckart normalisation of QS
+    (ireducMatrixSpeedy, initial.m:2089), singlet and triplet operators, the
+    chain tables z (xi, zeta) and Z (delta: on-site pairing, kappa: anomalous
+    hopping; src/nrg.cc:3383-3386), each the same for every channel or given
+    per channel (one row per channel)."""
+    nch = len(m.f_orbitals)
+    if nch not in (1, 2):
+        raise ValueError("SPSU2 data: one or two channels")
     F = m.fock
     subs = decompose_spsu2(m)
     smap = {s.SS: s for s in subs}
@@ -749,7 +752,7 @@ def write_data_spsu2(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: 
              "# symtype SPSU2",
              "#!9",
              "# Number of channels, chain sites, subspaces: ",
-             "%d %d %d" % (1, Nmax, len(subs)),
+             "%d %d %d" % (nch, Nmax, len(subs)),
              "# SCALE " + _fmt(sc0),
              "# Energies (GS energy subtracted, multiplied by 1/SCALE):"]
     for s in subs:
@@ -765,7 +768,8 @@ def write_data_spsu2(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: 
             _write_matrix(lines, M)
 
     lines.append("# Irreducible matrix elements for Wilson chains:")
-    blocks("f 0 0", doublet(m.f_orbitals[0]))
+    for ch in range(nch):
+        blocks("f %d 0" % ch, doublet(m.f_orbitals[ch]))
     lines.append("# GS energy in absolute units:")
     lines.append("e")
     lines.append(_fmt(gs))
@@ -780,8 +784,11 @@ def write_data_spsu2(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: 
     for tag, tabs in (("z", (xi, zeta)), ("Z", (delta, kappa))):
         lines.append(tag)
         for t in tabs:
-            lines.append("%d" % (len(t) - 1))
-            lines.extend(_fmt(x) for x in t)
+            rows = np.atleast_2d(np.asarray(t, dtype=float))
+            for ch in range(nch):
+                r = rows[min(ch, rows.shape[0] - 1)]
+                lines.append("%d" % (len(r) - 1))
+                lines.extend(_fmt(x) for x in r)
     lines.append("")
     with open(path, "w") as fh:
         fh.write("\n".join(lines))
@@ -836,11 +843,22 @@ def make_siam(dirpath: str, U: float, eps_d: float, Gamma: float, Lambda: float,
 
 
 def make_kondo(dirpath: str, J: List[float], Lambda: float, Nmax: int, z: float = 1.0,
-               params: Dict[str, object] | None = None, dps: int = 200, discretization: str = "Y") -> dict:
+               params: Dict[str, object] | None = None, dps: int = 200, discretization: str = "Y",
+               symtype: str = "QS") -> dict:
+    """Generate `data` and `param` for the Kondo model with len(J) channels on
+    a flat band, symmetry QS or SPSU2 (SPSU2: a normal band, the pairing
+    and anomalous-hopping tables zero)."""
     os.makedirs(dirpath, exist_ok=True)
     xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps, discretization=discretization)
     m = kondo_cluster(J)
-    info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, len(J), discretization)
+    if symtype == "SPSU2":
+        zero = np.zeros(Nmax + 1)
+        info = write_data_spsu2(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, zero, zero,
+                                discretization)
+    elif symtype == "QS":
+        info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, len(J), discretization)
+    else:
+        raise ValueError("symtype QS or SPSU2")
     p = {"Lambda": Lambda, "z": z, "discretization": discretization}
     if params:
         p.update(params)

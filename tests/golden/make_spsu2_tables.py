@@ -1,7 +1,8 @@
-"""Generate tests/golden/spsu2_tables.json from the reference's 1-channel
-SPSU2 coefficient tables (coefnew/spsu2/spsu2-1ch-*.dat, included by
-src/sym-SPSU2.cc:35-58 and :120-126 and src/nrg-recalc-SPSU2.cc), evaluated
-numerically for a range of spin multiplicities.  Run in a container that has
+"""Generate tests/golden/spsu2_tables.json and spsu2_tables_2ch.json from the
+reference's 1- and 2-channel SPSU2 coefficient tables
+(coefnew/spsu2/spsu2-<P>ch-*.dat, included by src/sym-SPSU2.cc:35-58 and
+:120-138 and src/nrg-recalc-SPSU2.cc), evaluated numerically for a range of
+spin multiplicities.  Run in a container that has
 the reference checkout:
 
     python tests/golden/make_spsu2_tables.py /root/reference
@@ -20,14 +21,15 @@ from make_qs_tables import _eval, _split_args  # noqa: E402
 
 FILES = ["offdiag", "anomalous", "isospinx", "diag", "spinupa", "spindowna", "doubletp", "doubletm",
          "triplets", "tripletp", "tripletm", "singlet", "In2", "QN"]
+FILES_2CH = FILES + ["spinupb", "spindownb"]
 
 
-def main(refroot, out):
+def main(refroot, out, channels=1, files=FILES):
     base = os.path.join(refroot, "coefnew", "spsu2")
     result = {"ss_range": [1, 40], "tables": {}}
-    for name in FILES:
+    for name in files:
         rows = []
-        with open(os.path.join(base, "spsu2-1ch-%s.dat" % name)) as fh:
+        with open(os.path.join(base, "spsu2-%dch-%s.dat" % (channels, name))) as fh:
             for line in fh:
                 line = line.strip()
                 if not line:
@@ -61,4 +63,6 @@ def main(refroot, out):
 
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    main(ref, os.path.join(os.path.dirname(os.path.abspath(__file__)), "spsu2_tables.json"))
+    here = os.path.dirname(os.path.abspath(__file__))
+    main(ref, os.path.join(here, "spsu2_tables.json"))
+    main(ref, os.path.join(here, "spsu2_tables_2ch.json"), channels=2, files=FILES_2CH)

@@ -2,7 +2,7 @@
 // tables of the host's plug-in (host/symmetry.h) as JSON, one object per
 // line, for comparison with the oracle's derivation and the reference's
 // tables.
-//   spsu2_dump <largest SS>
+//   spsu2_dump <channels> <largest SS>
 #include <cstdio>
 #include <cstdlib>
 
@@ -23,9 +23,9 @@ static void rows(const std::vector<RecalcTable>& ts) {
 }
 
 int main(int argc, char** argv) {
-  if (argc != 2) return 2;
-  const int ssmax = atoi(argv[1]);
-  nrgb::SymmetrySPSU2 S;
+  if (argc != 3) return 2;
+  const int P = atoi(argv[1]), ssmax = atoi(argv[2]);
+  nrgb::SymmetrySPSU2 S(P);
   printf("{\"kind\":\"diag\",\"rows\":[");
   const auto d = S.diag();
   for (size_t k = 0; k < d.size(); ++k) printf("%s[%d,%d,%.17g]", k ? "," : "", d[k].i, d[k].ch, d[k].number);

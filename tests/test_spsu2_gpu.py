@@ -1,5 +1,5 @@
-"""The SPSU2 symmetry plug-in (spin SU(2), charge not conserved, one
-channel) on the GPU.
+"""The SPSU2 symmetry plug-in (spin SU(2), charge not conserved, one and
+two channels) on the GPU.
 
 * Normal band (no pairing): the single-impurity Anderson model in SPSU2 and
   in QS keeps the same states under an energy cutoff, so the thermodynamic
@@ -10,7 +10,9 @@ channel) on the GPU.
   levels of the first steps equal the exact diagonalisation of the chain
   (impurity, sites f_0 .. f_N+1) with on-site pairing delta_n and anomalous
   hopping kappa_n, which tests the pairing and anomalous tables and the Z
-  block of the data file."""
+  block of the data file.
+* Two channels: the two-channel Kondo model in SPSU2 and in QS agree the
+  same way, spin (triplet) spectrum included."""
 import os
 
 import numpy as np
@@ -137,3 +139,46 @@ def test_spsu2_pairing_matches_exact_diagonalisation(tmp_path, gap, kap):
         got = np.sort(np.concatenate([[e] * int(lab[0]) for e, lab, _ in step]))
         assert got.shape == ev.shape, (N, got.shape, ev.shape)
         assert np.max(np.abs(got - ev)) < 1e-10, (N, float(np.max(np.abs(got - ev))))
+
+
+def test_spsu2_two_channels_matches_qs(tmp_path):
+    """Two-channel Kondo model (no pairing) in SPSU2 and in QS: the tables
+    of both are derived for 16 combinations (QSCoupling in its two modes);
+    thermodynamics, energy flow and the f and spin spectra (doublet and
+    triplet operators) agree."""
+    import nrgb
+    params = {"keep": 100000, "keepenergy": 5.0, "keepmin": 1, "T": 1e-3, "fdm": True, "dmnrg": True,
+              "spect": "SZd-SZd", "specd": "A_f0-A_f0", "bins": 30, "savebins": True, "broaden": False,
+              "dumpannotated": 100000, "prec_td": 16, "dumpprecision": 16}
+    out = {}
+    ctx = nrgb.Context(0)
+    try:
+        for sym in ("QS", "SPSU2"):
+            wd = str(tmp_path / ("in" + sym))
+            inputgen.make_kondo(wd, [0.2, 0.2], 3.0, 8, symtype=sym, params=dict(params))
+            od = str(tmp_path / ("out" + sym))
+            os.makedirs(od)
+            ctx.run(wd, od)
+            out[sym] = od
+    finally:
+        ctx.close()
+    nq, tq = _td(os.path.join(out["QS"], "td"))
+    ns, ts = _td(os.path.join(out["SPSU2"], "td"))
+    assert tq.shape[0] == ts.shape[0]
+    for name in ("T", "<Sz^2>", "<E>", "<E^2>", "C", "F", "S"):
+        a, b = tq[:, nq.index(name)], ts[:, ns.index(name)]
+        assert np.all(np.abs(a - b) <= 1e-8 * np.abs(a) + 1e-11), (name, float(np.max(np.abs(a - b))))
+    aq = cases.read_annotated(os.path.join(out["QS"], "annotated.dat"))
+    as_ = cases.read_annotated(os.path.join(out["SPSU2"], "annotated.dat"))
+    assert len(aq) == len(as_)
+    for sq, ss in zip(aq, as_):
+        lq, ls = _levels(sq), _levels(ss)
+        assert lq.shape == ls.shape
+        assert np.max(np.abs(lq - ls)) <= 1e-9 * max(1.0, np.max(np.abs(lq)))
+    for fname in ("spec_FDM_dens_A_f0-A_f0.bin", "spin_FDM_dens_SZd-SZd.bin", "spec_DMNRG_dens_A_f0-A_f0.bin"):
+        q = cases.read_bins(os.path.join(out["QS"], fname))
+        s = cases.read_bins(os.path.join(out["SPSU2"], fname))
+        dq, ds = dict(zip(q[:, 0], q[:, 1])), dict(zip(s[:, 0], s[:, 1]))
+        wmax = max(abs(v) for v in dq.values())
+        err = max(abs(dq.get(k, 0.0) - ds.get(k, 0.0)) for k in set(dq) | set(ds))
+        assert err <= 1e-8 * wmax, (fname, err / wmax)

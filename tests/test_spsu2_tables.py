@@ -1,8 +1,9 @@
-"""The SPSU2 coefficient tables (spin SU(2) without charge conservation):
-the oracle's derivation from the site's Fock space (oracle/spsu2_derive.py)
-and the host's plug-in (host/symmetry.h, SymmetrySPSU2) against the
-reference's tables (coefnew/spsu2/spsu2-1ch-*.dat, evaluated into
-tests/golden/spsu2_tables.json by tests/golden/make_spsu2_tables.py):
+"""The SPSU2 coefficient tables (spin SU(2) without charge conservation), 1
+and 2 channels: the oracle's derivation from the site's Fock space
+(oracle/spsu2_derive.py) and the host's plug-in (host/symmetry.h,
+SymmetrySPSU2, with host/qs_coupling.cc for two channels) against the
+reference's tables (coefnew/spsu2/spsu2-<P>ch-*.dat, evaluated into
+tests/golden/spsu2_tables*.json by tests/golden/make_spsu2_tables.py):
 hopping, anomalous hopping, on-site pairing, site occupancies, <f^dag>
 recalculation, doublet and triplet operator tables.
 
@@ -11,7 +12,6 @@ forms (an ancestor SS < 1, or an operator that the triangle rule forbids
 between the two subspaces) are not compared: the reference's run never
 evaluates them either."""
 import json
-import math
 import os
 import shutil
 import subprocess
@@ -21,31 +21,40 @@ import pytest
 import spsu2_derive as SD
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-GOLD = json.load(open(os.path.join(ROOT, "tests", "golden", "spsu2_tables.json")))["tables"]
-SSMAX = 20
+SSMAX = {1: 20, 2: 12}
 TOL = 1e-12
-IN = {1: 0, 2: 0, 3: -1, 4: 1}   # ancestor SS offset of each combination
+
+
+def _gold(P):
+    name = "spsu2_tables.json" if P == 1 else "spsu2_tables_2ch.json"
+    return json.load(open(os.path.join(ROOT, "tests", "golden", name)))["tables"]
+
+
+class _Offsets(dict):
+    """Ancestor SS offset of each (1-based) combination, with the site's SS."""
+
+    def __init__(self, P):
+        super().__init__({i + 1: c[2][1] for i, c in enumerate(SD.COMBOS[P])})
+        self.site = {i + 1: int(round(2 * c[1])) + 1 for i, c in enumerate(SD.COMBOS[P])}
+
+    def formed(self, ss, i):
+        """Combination i exists in subspace ss: its ancestor exists and the
+        ancestor's spin and the site's couple to S."""
+        a = ss + self[i]
+        return ss >= 1 and a >= 1 and _su2(ss, a, self.site[i])
+
+
+def _in(P):
+    return _Offsets(P)
 
 
 def _su2(a, b, c):
     return abs(a - b) <= c - 1 and abs(b - c) <= a - 1 and abs(c - a) <= b - 1
 
 
-def _used(ss1, ssp, i1, ip, rank_ss):
+def _used(IN, ss1, ssp, i1, ip, rank_ss):
     """An entry (i1, ip) between subspaces ss1 and ssp is formed in a run."""
-    a1, ap = ss1 + IN[i1], ssp + IN[ip]
-    return ss1 >= 1 and ssp >= 1 and a1 >= 1 and ap >= 1 and _su2(ss1, ssp, rank_ss)
-
-
-def _ref_rows(name, ss, rank_ss, dss):
-    out = {}
-    for r in GOLD[name]:
-        v = r["factor"][str(ss)]
-        if v is None:
-            continue
-        if _used(ss, ss + dss, r["i1"], r["ip"], rank_ss):
-            out[(r["i1"], r["ip"])] = v
-    return out
+    return IN.formed(ss1, i1) and IN.formed(ssp, ip) and _su2(ss1, ssp, rank_ss)
 
 
 def _check(got, ref):
@@ -57,61 +66,65 @@ def _check(got, ref):
     return len(ref)
 
 
-def _python_tables(ss):
-    T = SD.tables()
-    off = {}
-    for kind, fn in ((0, T.offdiag), (1, T.anomalous)):
-        for i, j, ch, v in fn(ss):
-            off[(i, j, kind)] = v
-    for i, j, ch, v in T.isospinx():
-        off[(i, j, 2)] = v
-    return off
-
-
-def _ref_offdiag(ss):
+def _python_offdiag(P, ss):
+    T = SD.tables(P)
+    IN = _in(P)
     out = {}
-    for name, kind in (("offdiag", 0), ("anomalous", 1), ("isospinx", 2)):
-        for r in GOLD[name]:
-            v = r["factor"][str(ss)]
-            a_i, a_j = ss + IN[r["i"]], ss + IN[r["j"]]
-            if v is not None and a_i >= 1 and a_j >= 1:
-                out[(r["i"], r["j"], kind)] = v
+    for kind, rows in ((0, T.offdiag(ss)), (1, T.anomalous(ss)), (2, T.isospinx())):
+        for i, j, ch, v in rows:
+            if IN.formed(ss, i) and IN.formed(ss, j):
+                out[(i, j, ch, kind)] = v
     return out
 
 
-def test_derivation_matches_reference_hamiltonian_tables():
-    n = 0
-    for ss in range(1, SSMAX + 1):
-        ref = _ref_offdiag(ss)
-        got = {k: v for k, v in _python_tables(ss).items() if ss + IN[k[0]] >= 1 and ss + IN[k[1]] >= 1}
-        n += _check(got, ref)
-    assert n > 150
-    assert sorted((r["i"], r["number"]) for r in GOLD["diag"]) == sorted((i, v) for i, ch, v in SD.tables().diag())
-    assert [r["qn"][0] for r in sorted(GOLD["In2"], key=lambda r: r["i"])] == [IN[i] for i in (1, 2, 3, 4)]
+def _ref_offdiag(P, ss):
+    G, IN = _gold(P), _in(P)
+    out = {}
+    for name, kind in (("offdiag", 0), ("anomalous", 1), ("isospinx", 2)):
+        for r in G[name]:
+            v = r["factor"][str(ss)]
+            if v is not None and IN.formed(ss, r["i"]) and IN.formed(ss, r["j"]):
+                out[(r["i"], r["j"], r["ch"], kind)] = v
+    return out
 
 
-def test_derivation_matches_reference_recalc_tables():
-    T = SD.tables()
+@pytest.mark.parametrize("P", [1, 2])
+def test_derivation_matches_reference_hamiltonian_tables(P):
     n = 0
-    for ss in range(1, SSMAX + 1):
+    for ss in range(1, SSMAX[P] + 1):
+        n += _check(_python_offdiag(P, ss), _ref_offdiag(P, ss))
+    assert n > (150 if P == 1 else 900)
+    G = _gold(P)
+    assert sorted((r["i"], r["ch"], r["number"]) for r in G["diag"]) == sorted(SD.tables(P).diag())
+    assert [r["qn"][0] for r in sorted(G["In2"], key=lambda r: r["i"])] == [_in(P)[i] for i in sorted(_in(P))]
+
+
+@pytest.mark.parametrize("P", [1, 2])
+def test_derivation_matches_reference_recalc_tables(P):
+    T, G, IN = SD.tables(P), _gold(P), _in(P)
+    n = 0
+    for ss in range(1, SSMAX[P] + 1):
         for I1, ch, rows in T.recalc_f((0, ss)):
             d = I1[1] - ss
-            name = "spinupa" if d == 1 else "spindowna"
-            # <f> tables are indexed by the ket subspace ssp = ss
+            name = ("spinup" if d == 1 else "spindown") + "ab"[ch]
             ref = {}
-            for r in GOLD[name]:
+            for r in G[name]:
                 v = r["factor"][str(ss)]
-                if v is not None and I1[1] + IN[r["i1"]] >= 1 and ss + IN[r["ip"]] >= 1:
+                if v is not None and IN.formed(I1[1], r["i1"]) and IN.formed(ss, r["ip"]):
                     ref[(r["i1"], r["ip"])] = v
-            n += _check({(a, b): v for a, b, v in rows}, ref)
+            n += _check({(a, b): v for a, b, v in rows if IN.formed(I1[1], a) and IN.formed(ss, b)}, ref)
         for fn, rank_ss, names in ((T.doublet, 2, {1: "doubletp", -1: "doubletm"}),
                                    (T.triplet, 3, {0: "triplets", 2: "tripletp", -2: "tripletm"})):
             for Ip, rows in fn((0, ss)):
                 d = Ip[1] - ss
-                ref = _ref_rows(names[d], ss, rank_ss, d)
-                got = {(a, b): v for a, b, v in rows if _used(ss, Ip[1], a, b, rank_ss)}
+                ref = {}
+                for r in G[names[d]]:
+                    v = r["factor"][str(ss)]
+                    if v is not None and _used(IN, ss, ss + d, r["i1"], r["ip"], rank_ss):
+                        ref[(r["i1"], r["ip"])] = v
+                got = {(a, b): v for a, b, v in rows if _used(IN, ss, Ip[1], a, b, rank_ss)}
                 n += _check(got, ref)
-    assert n > 400
+    assert n > (400 if P == 1 else 1500)
 
 
 @pytest.fixture(scope="module")
@@ -122,34 +135,38 @@ def dump(tmp_path_factory):
     exe = str(tmp_path_factory.mktemp("spsu2") / "spsu2_dump")
     subprocess.run([cxx, "-O1", "-std=c++17", "-o", exe, os.path.join(ROOT, "tests", "spsu2_dump.cc"),
                     os.path.join(ROOT, "nrgljubljana-old_b200", "host", "qs_coupling.cc")], check=True)
-    out = subprocess.run([exe, str(SSMAX)], check=True, capture_output=True, text=True).stdout
-    return [json.loads(line) for line in out.splitlines()]
+
+    def run(P):
+        out = subprocess.run([exe, str(P), str(SSMAX[P])], check=True, capture_output=True, text=True).stdout
+        return [json.loads(line) for line in out.splitlines()]
+    return run
 
 
-def test_plugin_matches_derivation(dump):
-    T = SD.tables()
+@pytest.mark.parametrize("P", [1, 2])
+def test_plugin_matches_derivation(dump, P):
+    T, IN = SD.tables(P), _in(P)
     n = 0
-    for rec in dump:
+    for rec in dump(P):
         kind = rec["kind"]
         if kind == "diag":
             assert sorted(map(tuple, rec["rows"])) == sorted(T.diag())
             continue
         if kind == "offdiag":
             ss = rec["ss"]
-            got = {(i, j, k): v for i, j, ch, v, k in rec["rows"] if ss + IN[i] >= 1 and ss + IN[j] >= 1}
-            py = {k: v for k, v in _python_tables(ss).items() if ss + IN[k[0]] >= 1 and ss + IN[k[1]] >= 1}
-            n += _check(got, py)
+            got = {(i, j, ch, k): v for i, j, ch, v, k in rec["rows"] if IN.formed(ss, i) and IN.formed(ss, j)}
+            n += _check(got, _python_offdiag(P, ss))
             continue
         ss = rec["I"][1]
         if kind == "recalc_f":
-            got = {(tuple(I1), a, b): v for I1, ch, rs in rec["tables"] for a, b, v in rs
-                   if I1[1] + IN[a] >= 1 and ss + IN[b] >= 1}
-            py = {(tuple(I1), a, b): v for I1, ch, rs in T.recalc_f((0, ss)) for a, b, v in rs}
+            got = {(tuple(I1), ch, a, b): v for I1, ch, rs in rec["tables"] for a, b, v in rs
+                   if IN.formed(I1[1], a) and IN.formed(ss, b)}
+            py = {(tuple(I1), ch, a, b): v for I1, ch, rs in T.recalc_f((0, ss)) for a, b, v in rs
+                  if IN.formed(I1[1], a) and IN.formed(ss, b)}
             n += _check(got, py)
             continue
         fn, rank_ss = (T.doublet, 2) if kind == "doublet" else (T.triplet, 3)
         got = {(tuple(Ip), a, b): v for Ip, ch, rs in rec["tables"] for a, b, v in rs
-               if _used(ss, Ip[1], a, b, rank_ss)}
-        py = {(tuple(Ip), a, b): v for Ip, rs in fn((0, ss)) for a, b, v in rs if _used(ss, Ip[1], a, b, rank_ss)}
+               if _used(IN, ss, Ip[1], a, b, rank_ss)}
+        py = {(tuple(Ip), a, b): v for Ip, rs in fn((0, ss)) for a, b, v in rs if _used(IN, ss, Ip[1], a, b, rank_ss)}
         n += _check(got, py)
-    assert n > 500
+    assert n > (500 if P == 1 else 1500)
