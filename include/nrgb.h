@@ -156,6 +156,75 @@ typedef struct {
 int nrgb_recalc(nrgb_ctx* ctx, int nout, const nrgb_recalc_out* outs, int nterms, const nrgb_recalc_term* terms,
                 int* out_handles);
 
+/* Density-matrix backward step (calc_densitymatrix, src/dmnrg.h:327-475; the
+ * DM-NRG and FDM sweeps of src/nrg.cc:1877-1913):
+ * output o (r1 x rp) = sum over its terms of
+ *   factor * Z1[off1 : off1+r1, 0 : k1] * rho[0 : k1, 0 : kp] * Zp[offp : offp+rp, 0 : kp]^T
+ * the adjoint of nrgb_recalc's product: the eigenvector sub-blocks of the
+ * subspaces of step N+1 carry their density matrices rho (k1 x kp kept
+ * states) back to the sub-blocks of their ancestors at step N.  Z1, Zp:
+ * eigenvector handles of nrgb_step; rho: any matrix handle.  out_handles[o]
+ * receives a new handle per output. */
+typedef struct {
+  int z1, off1, k1;
+  int zp, offp, kp;
+  int rho;
+  double factor;
+} nrgb_dm_term;
+typedef struct {
+  int r1, rp;
+  int term0, nterms;
+} nrgb_dm_out;
+int nrgb_dm_backward(nrgb_ctx* ctx, int nout, const nrgb_dm_out* outs, int nterms, const nrgb_dm_term* terms,
+                     int* out_handles);
+
+/* FDM spectral weights of one step (SPEC_FDMgt + SPEC_FDMls,
+ * src/spec_FDM.cc:41-119) for a list of block pairs (ket block i, bra block
+ * j): the greater and lesser sums over the discarded and kept sectors, at
+ * the energies E_j - E_i, binned on the logarithmic grid of
+ * src/bins.h:22-131 (lowest point 10^floor(log10 emin), bins_per_decade,
+ * highest 10^ceil(log10 emax); nbins must equal
+ * (int)((ceil(log10 emax) - floor(log10 emin)) * bins_per_decade + 1)) and
+ * ADDED to bins[0 .. 2*nbins) (host memory: positive energies, then
+ * negative ones, each nbins long).  Weights below discard * |E| are dropped
+ * (discard_immediately).  op1, op2: the blocks <j|O1|i>, <j|O2|i>
+ * (allj x alli); rho_i, rho_j: the density matrices of the kept states
+ * (reti x reti, retj x retj; unused when reti / retj is 0, as at the last
+ * step); e_i, e_j: the absolute energies of both blocks' states (shifted by
+ * the ground state of the whole run), alli and allj values; factor: the
+ * symmetry's spectral-density factor.  T: temperature; wn: the step's
+ * weight w_N (src/dmnrg.h:487-596); fermionic: 1 for fermionic operators
+ * (the lesser sum enters with +), 0 for bosonic. */
+typedef struct {
+  int op1, op2;
+  int rho_i, rho_j;
+  int e_i, e_j;
+  int reti, retj;
+  double factor;
+} nrgb_fdm_pair;
+int nrgb_spectrum_fdm(nrgb_ctx* ctx, int npairs, const nrgb_fdm_pair* pairs, double T, double wn, int fermionic,
+                      double bins_per_decade, double emin, double emax, double discard, int nbins, double* bins);
+
+/* DM-NRG spectral weights of one step (SPEC_DMNRG::calc,
+ * src/spec_DMNRG.cc:13-52) for a list of block pairs (ket block p, bra block
+ * 1) over their kept states: w = factor * (op1 (op2 rho_p) + s op2 (rho_1
+ * op1)) elementwise, s = +1 for fermionic operators and -1 for bosonic, at
+ * E = E_1 - E_p, kept where ewin_min <= |E| <= ewin_max (the step's window,
+ * src/spectrumrealfreq.cc) and binned at scale * E on the grid of
+ * nrgb_spectrum_fdm, ADDED to bins.  rho_1, rho_p: the density matrices of
+ * the kept states (dim1 x dim1, dimp x dimp; their sizes give the kept
+ * counts); op1, op2: the blocks <1|O|p> (at least dim1 x dimp, same shape);
+ * e_1, e_p: the step's energies (at least dim1 / dimp values). */
+typedef struct {
+  int op1, op2;
+  int rho_1, rho_p;
+  int e_1, e_p;
+  double factor;
+} nrgb_dmnrg_pair;
+int nrgb_spectrum_dmnrg(nrgb_ctx* ctx, int npairs, const nrgb_dmnrg_pair* pairs, double scale, double ewin_min,
+                        double ewin_max, int fermionic, double bins_per_decade, double emin, double emax,
+                        double discard, int nbins, double* bins);
+
 /* Split-precision form of nrgb_gemm_grouped_dev (same descriptors): every
  * product is computed from `slices` (2..8) signed 7-bit slices of each
  * operand, with power-of-two scales per row of op(A) and per column of op(B),

@@ -390,4 +390,270 @@ int nrgb_recalc(nrgb_ctx* ctx, int nout, const nrgb_recalc_out* outs, int nterms
   });
 }
 
+int nrgb_dm_backward(nrgb_ctx* ctx, int nout, const nrgb_dm_out* outs, int nterms, const nrgb_dm_term* terms,
+                     int* out_handles) {
+  if (nout < 0 || nterms < 0 || (nout > 0 && (!outs || !out_handles)) || (nterms > 0 && !terms)) return 1;
+  return guarded(ctx, [&] {
+    using namespace nrgb;
+    cudaStream_t st = ctx->stream;
+    // output (r1 x rp) = sum factor * Z1sub * rho * Zpsub^T with Zsub = Z[off : off+r, 0 : k]:
+    // first T = rho * Zpsub^T (k1 x rp), then factor * Z1sub * T
+    std::vector<GemmProb> p1, p2;
+    std::vector<GemmSeg> s1, s2;
+    int t1 = 0, st1 = 0, t2 = 0, st2 = 0;
+    size_t tbytes = 0;
+    for (int o = 0; o < nout; ++o)
+      for (int t = outs[o].term0; t < outs[o].term0 + outs[o].nterms; ++t) {
+        if (t < 0 || t >= nterms) throw CudaError("nrgb_dm_backward: term range out of bounds");
+        if (terms[t].k1 > 0) tbytes += ((size_t)terms[t].k1 * std::max(0, outs[o].rp) * sizeof(double) + 255) & ~size_t(255);
+      }
+    ctx->scratch.reserve(tbytes + (size_t)(2 * nterms + 2 * nout + 8) * (sizeof(GemmProb) + sizeof(GemmSeg)) + 8192);
+    ctx->scratch.reset();
+    for (int o = 0; o < nout; ++o) {
+      const nrgb_dm_out& Y = outs[o];
+      if (Y.r1 < 0 || Y.rp < 0) throw CudaError("nrgb_dm_backward: negative output size");
+      const int h = new_mat(ctx, Y.r1, Y.rp);
+      out_handles[o] = h;
+      double* C = ctx->plan.mats[h].p;
+      if (Y.r1 == 0 || Y.rp == 0) continue;
+      std::vector<GemmSeg> segs;
+      for (int t = Y.term0; t < Y.term0 + Y.nterms; ++t) {
+        const nrgb_dm_term& x = terms[t];
+        if (x.k1 <= 0 || x.kp <= 0) continue;
+        const PlanMatrix& Z1 = mat(ctx, x.z1);
+        const PlanMatrix& Zp = mat(ctx, x.zp);
+        const PlanMatrix& R = mat(ctx, x.rho);
+        if (x.off1 < 0 || x.off1 + Y.r1 > Z1.rows || x.k1 > Z1.cols || x.offp < 0 || x.offp + Y.rp > Zp.rows ||
+            x.kp > Zp.cols)
+          throw CudaError("nrgb_dm_backward: sub-block outside its eigenvector matrix");
+        if (R.rows < x.k1 || R.cols < x.kp) throw CudaError("nrgb_dm_backward: density matrix too small");
+        double* Tm = static_cast<double*>(ctx->scratch.alloc((size_t)x.k1 * Y.rp * sizeof(double)));
+        GemmProb a{};
+        a.C = Tm;
+        a.ldc = x.k1;
+        a.m = x.k1;
+        a.n = Y.rp;
+        a.beta = 0.0;
+        a.seg0 = (int)s1.size();
+        a.nseg = 1;
+        gemm_assign_tiles(a, t1, st1);
+        p1.push_back(a);
+        // op(B)[p, j] = Zp[offp + j, p]: the sub-block read transposed
+        s1.push_back(GemmSeg{R.p, Zp.p + x.offp, std::max(1, R.rows), Zp.rows, x.kp, 0, 1, 1.0});
+        segs.push_back(GemmSeg{Z1.p + x.off1, Tm, Z1.rows, x.k1, x.k1, 0, 0, x.factor});
+      }
+      if (segs.empty()) {
+        NRGB_CUDA(cudaMemsetAsync(C, 0, (size_t)Y.r1 * Y.rp * sizeof(double), st));
+        continue;
+      }
+      GemmProb b{};
+      b.C = C;
+      b.ldc = Y.r1;
+      b.m = Y.r1;
+      b.n = Y.rp;
+      b.beta = 0.0;
+      b.seg0 = (int)s2.size();
+      b.nseg = (int)segs.size();
+      gemm_assign_tiles(b, t2, st2);
+      p2.push_back(b);
+      s2.insert(s2.end(), segs.begin(), segs.end());
+    }
+    auto launch = [&](std::vector<GemmProb>& P, std::vector<GemmSeg>& Sg, int tiles, int stiles) {
+      if (P.empty()) return;
+      GemmProb* dP = stage(ctx, P);
+      GemmSeg* dS = stage(ctx, Sg);
+      KernelStats::get().add_work("gemm_f64_dm", gemm_flops(P.data(), (int)P.size(), Sg.data()));
+      NRGB_CUDA(gemm_grouped_launch(dP, (int)P.size(), dS, tiles, st, "gemm_f64_dm", stiles));
+    };
+    launch(p1, s1, t1, st1);
+    launch(p2, s2, t2, st2);
+    NRGB_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int nrgb_spectrum_fdm(nrgb_ctx* ctx, int npairs, const nrgb_fdm_pair* pairs, double T, double wn, int fermionic,
+                      double bins_per_decade, double emin, double emax, double discard, int nbins, double* bins) {
+  if (npairs < 0 || (npairs > 0 && !pairs) || !bins || !(T > 0.0) || !(bins_per_decade > 0.0) || !(emin > 0.0) ||
+      !(emax > emin) || !(discard >= 0.0))
+    return 1;
+  return guarded(ctx, [&] {
+    using namespace nrgb;
+    cudaStream_t st = ctx->stream;
+    // the logarithmic grid of src/bins.h:22-131, as the whole-run driver builds it
+    BinGrid grid{};
+    const double l0 = floor(log10(emin)), l1 = ceil(log10(emax));
+    grid.l0 = l0;
+    grid.bpd = bins_per_decade;
+    grid.nbins = (int)((l1 - l0) * bins_per_decade + 1.0);
+    grid.discard = discard;
+    if (grid.nbins != nbins) throw CudaError("nrgb_spectrum_fdm: nbins does not match the grid");
+    // per pair: the two products with the density matrices and the
+    // Boltzmann factors of both blocks' states
+    size_t bytes = 2 * (size_t)nbins * sizeof(double) + (size_t)npairs * sizeof(SpecFdmPair) + 8192;
+    std::vector<double> hx;  // exp(-E/T) of every pair's two energy lists, back to back
+    std::vector<size_t> xo(2 * (size_t)npairs);
+    for (int k = 0; k < npairs; ++k) {
+      const nrgb_fdm_pair& q = pairs[k];
+      const PlanMatrix& A = mat(ctx, q.op1);
+      const PlanMatrix& B = mat(ctx, q.op2);
+      if (A.rows != B.rows || A.cols != B.cols) throw CudaError("nrgb_spectrum_fdm: operator blocks differ in shape");
+      if (q.reti < 0 || q.retj < 0 || q.reti > A.cols || q.retj > A.rows)
+        throw CudaError("nrgb_spectrum_fdm: kept states outside the block");
+      bytes += (((size_t)A.rows * q.reti + (size_t)q.retj * A.cols) * sizeof(double) + 512);
+      for (int side = 0; side < 2; ++side) {
+        const PlanMatrix& E = mat(ctx, side ? q.e_j : q.e_i);
+        const int want = side ? A.rows : A.cols;
+        if ((long)E.rows * E.cols != want) throw CudaError("nrgb_spectrum_fdm: energy list length differs from the block");
+        std::vector<double> e(want);
+        if (want) NRGB_CUDA(cudaMemcpyAsync(e.data(), E.p, want * sizeof(double), cudaMemcpyDeviceToHost, st));
+        NRGB_CUDA(cudaStreamSynchronize(st));
+        xo[2 * k + side] = hx.size();
+        for (double x : e) hx.push_back(exp(-x / T));
+      }
+    }
+    bytes += hx.size() * sizeof(double) + (size_t)(4 * npairs + 16) * 512;  // allocations and their alignment
+    ctx->scratch.reserve(bytes + (size_t)(2 * npairs + 8) * (sizeof(GemmProb) + sizeof(GemmSeg)));
+    ctx->scratch.reset();
+    double* dx = static_cast<double*>(ctx->scratch.alloc(std::max<size_t>(1, hx.size()) * sizeof(double)));
+    if (!hx.empty()) NRGB_CUDA(cudaMemcpyAsync(dx, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    std::vector<GemmProb> gp;
+    std::vector<GemmSeg> gs;
+    int tiles = 0, stiles = 0;
+    auto product = [&](double* C, int m, int n, const double* a, int lda, const double* b, int ldb, int k) {
+      GemmProb g{};
+      g.C = C;
+      g.ldc = m;
+      g.m = m;
+      g.n = n;
+      g.beta = 0.0;
+      g.seg0 = (int)gs.size();
+      g.nseg = 1;
+      gemm_assign_tiles(g, tiles, stiles);
+      gp.push_back(g);
+      gs.push_back(GemmSeg{a, b, lda, ldb, k, 0, 0, 1.0});
+    };
+    std::vector<SpecFdmPair> sp;
+    int maxe = 0;
+    for (int k = 0; k < npairs; ++k) {
+      const nrgb_fdm_pair& q = pairs[k];
+      const PlanMatrix& A = mat(ctx, q.op1);
+      const PlanMatrix& B = mat(ctx, q.op2);
+      const int allj = A.rows, alli = A.cols;
+      if (!allj || !alli) continue;
+      double* O2R = nullptr;
+      double* RO2 = nullptr;
+      if (q.reti > 0) {  // op2[:allj, :reti] * rho_i
+        const PlanMatrix& R = mat(ctx, q.rho_i);
+        if (R.rows < q.reti || R.cols < q.reti) throw CudaError("nrgb_spectrum_fdm: rho_i too small");
+        O2R = static_cast<double*>(ctx->scratch.alloc((size_t)allj * q.reti * sizeof(double)));
+        product(O2R, allj, q.reti, B.p, B.rows, R.p, R.rows, q.reti);
+      }
+      if (q.retj > 0) {  // rho_j * op2[:retj, :alli]
+        const PlanMatrix& R = mat(ctx, q.rho_j);
+        if (R.rows < q.retj || R.cols < q.retj) throw CudaError("nrgb_spectrum_fdm: rho_j too small");
+        RO2 = static_cast<double*>(ctx->scratch.alloc((size_t)q.retj * alli * sizeof(double)));
+        product(RO2, q.retj, alli, R.p, R.rows, B.p, B.rows, q.retj);
+      }
+      sp.push_back(SpecFdmPair{A.p, B.p, O2R, RO2, mat(ctx, q.e_j).p, mat(ctx, q.e_i).p, dx + xo[2 * k + 1],
+                               dx + xo[2 * k], A.rows, allj, alli, q.retj, q.reti, q.factor});
+      maxe = std::max(maxe, allj * alli);
+    }
+    if (!gp.empty()) {
+      GemmProb* dP = stage(ctx, gp);
+      GemmSeg* dS = stage(ctx, gs);
+      NRGB_CUDA(gemm_grouped_launch(dP, (int)gp.size(), dS, tiles, st, "gemm_f64_spec", stiles));
+    }
+    double* dbins = static_cast<double*>(ctx->scratch.alloc(2 * (size_t)nbins * sizeof(double)));
+    NRGB_CUDA(cudaMemsetAsync(dbins, 0, 2 * (size_t)nbins * sizeof(double), st));
+    if (!sp.empty())
+      NRGB_CUDA(spec_fdm_launch(stage(ctx, sp), (int)sp.size(), maxe, grid, T, wn, fermionic ? 1.0 : -1.0, dbins, st));
+    std::vector<double> hb(2 * (size_t)nbins);
+    NRGB_CUDA(cudaMemcpyAsync(hb.data(), dbins, hb.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    NRGB_CUDA(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < hb.size(); ++i) bins[i] += hb[i];
+  });
+}
+
+int nrgb_spectrum_dmnrg(nrgb_ctx* ctx, int npairs, const nrgb_dmnrg_pair* pairs, double scale, double ewin_min,
+                        double ewin_max, int fermionic, double bins_per_decade, double emin, double emax,
+                        double discard, int nbins, double* bins) {
+  if (npairs < 0 || (npairs > 0 && !pairs) || !bins || !(scale > 0.0) || !(ewin_max >= ewin_min) ||
+      !(bins_per_decade > 0.0) || !(emin > 0.0) || !(emax > emin) || !(discard >= 0.0))
+    return 1;
+  return guarded(ctx, [&] {
+    using namespace nrgb;
+    cudaStream_t st = ctx->stream;
+    BinGrid grid{};
+    const double l0 = floor(log10(emin)), l1 = ceil(log10(emax));
+    grid.l0 = l0;
+    grid.bpd = bins_per_decade;
+    grid.nbins = (int)((l1 - l0) * bins_per_decade + 1.0);
+    grid.discard = discard;
+    if (grid.nbins != nbins) throw CudaError("nrgb_spectrum_dmnrg: nbins does not match the grid");
+    size_t bytes = 2 * (size_t)nbins * sizeof(double) + (size_t)(4 * npairs + 16) * 512 +
+                   (size_t)(2 * npairs + 8) * (sizeof(GemmProb) + sizeof(GemmSeg) + sizeof(SpecDmnrgPair));
+    for (int k = 0; k < npairs; ++k) {
+      const int d1 = mat(ctx, pairs[k].rho_1).rows, dp = mat(ctx, pairs[k].rho_p).rows;
+      bytes += 2 * (size_t)d1 * dp * sizeof(double);
+    }
+    ctx->scratch.reserve(bytes);
+    ctx->scratch.reset();
+    std::vector<GemmProb> gp;
+    std::vector<GemmSeg> gs;
+    int tiles = 0, stiles = 0;
+    auto product = [&](double* C, int m, int n, const double* a, int lda, const double* b, int ldb, int k) {
+      GemmProb g{};
+      g.C = C;
+      g.ldc = m;
+      g.m = m;
+      g.n = n;
+      g.beta = 0.0;
+      g.seg0 = (int)gs.size();
+      g.nseg = 1;
+      gemm_assign_tiles(g, tiles, stiles);
+      gp.push_back(g);
+      gs.push_back(GemmSeg{a, b, lda, ldb, k, 0, 0, 1.0});
+    };
+    std::vector<SpecDmnrgPair> sp;
+    int maxe = 0;
+    for (int k = 0; k < npairs; ++k) {
+      const nrgb_dmnrg_pair& q = pairs[k];
+      const PlanMatrix& A = mat(ctx, q.op1);
+      const PlanMatrix& B = mat(ctx, q.op2);
+      const PlanMatrix& R1 = mat(ctx, q.rho_1);
+      const PlanMatrix& Rp = mat(ctx, q.rho_p);
+      const int d1 = R1.rows, dp = Rp.rows;
+      if (R1.cols != d1 || Rp.cols != dp) throw CudaError("nrgb_spectrum_dmnrg: density matrices must be square");
+      if (A.rows != B.rows || A.cols != B.cols || A.rows < d1 || A.cols < dp)
+        throw CudaError("nrgb_spectrum_dmnrg: operator blocks smaller than the kept states or of different shapes");
+      const PlanMatrix& E1 = mat(ctx, q.e_1);
+      const PlanMatrix& Ep = mat(ctx, q.e_p);
+      if ((long)E1.rows * E1.cols < d1 || (long)Ep.rows * Ep.cols < dp)
+        throw CudaError("nrgb_spectrum_dmnrg: energy list shorter than the kept states");
+      if (!d1 || !dp) continue;
+      // SA = op2[:d1, :dp] * rho_p,  SB = rho_1 * op1[:d1, :dp]  (src/spec_DMNRG.cc:13-52)
+      double* SA = static_cast<double*>(ctx->scratch.alloc((size_t)d1 * dp * sizeof(double)));
+      double* SB = static_cast<double*>(ctx->scratch.alloc((size_t)d1 * dp * sizeof(double)));
+      product(SA, d1, dp, B.p, B.rows, Rp.p, Rp.rows, dp);
+      product(SB, d1, dp, R1.p, R1.rows, A.p, A.rows, d1);
+      sp.push_back(SpecDmnrgPair{A.p, B.p, SA, SB, E1.p, Ep.p, A.rows, d1, dp, q.factor});
+      maxe = std::max(maxe, d1 * dp);
+    }
+    if (!gp.empty()) {
+      GemmProb* dP = stage(ctx, gp);
+      GemmSeg* dS = stage(ctx, gs);
+      NRGB_CUDA(gemm_grouped_launch(dP, (int)gp.size(), dS, tiles, st, "gemm_f64_spec", stiles));
+    }
+    double* dbins = static_cast<double*>(ctx->scratch.alloc(2 * (size_t)nbins * sizeof(double)));
+    NRGB_CUDA(cudaMemsetAsync(dbins, 0, 2 * (size_t)nbins * sizeof(double), st));
+    if (!sp.empty())
+      NRGB_CUDA(spec_dmnrg_launch(stage(ctx, sp), (int)sp.size(), maxe, grid, scale, ewin_min, ewin_max,
+                                  fermionic ? 1.0 : -1.0, dbins, st));
+    std::vector<double> hb(2 * (size_t)nbins);
+    NRGB_CUDA(cudaMemcpyAsync(hb.data(), dbins, hb.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    NRGB_CUDA(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < hb.size(); ++i) bins[i] += hb[i];
+  });
+}
+
 }  // extern "C"

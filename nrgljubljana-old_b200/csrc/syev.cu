@@ -2014,6 +2014,10 @@ SyevBatched::SyevBatched() {
     while (trdc_bytes(n + 1, cl) <= cl_smem_ && (!cl_one_ || n + 1 <= TRDC1_ROWS * TRDC1_NT)) ++n;
     cl_nmax_ = n > SMALL_N ? n : 0;
   }
+  // one side stream per launch group of the cluster kernel (up to 19
+  // groups: single-CTA launches in four shared-memory sizes and one per
+  // cluster size), so that no group waits behind another on a shared stream
+  if (const char* ns = getenv("NRGB_SIDE_STREAMS")) naux_ = std::max(1, std::min(NAUX, atoi(ns)));
   for (int i = 0; i < NAUX; ++i) {
     NRGB_CUDA(cudaStreamCreateWithFlags(&aux_[i], cudaStreamNonBlocking));
     NRGB_CUDA(cudaEventCreateWithFlags(&join_[i], cudaEventDisableTiming));
@@ -2265,8 +2269,8 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
       NRGB_CUDA(cudaEventRecord(fork_, st));
       for (int g = NG - 1; g >= 0; --g) {
         if (grp[g].empty()) continue;
-        cudaStream_t sx = aux_[used % NAUX];
-        if (used < NAUX) NRGB_CUDA(cudaStreamWaitEvent(sx, fork_, 0));
+        cudaStream_t sx = aux_[used % naux_];
+        if (used < naux_) NRGB_CUDA(cudaStreamWaitEvent(sx, fork_, 0));
         double fl = 0, by = 0;
         for (const TrdClProb& t : grp[g]) {
           fl += 4.0 / 3.0 * (double)t.n * t.n * t.n;
@@ -2284,7 +2288,7 @@ void SyevBatched::run(const std::vector<SyevDesc>& probs, cudaStream_t st) {
         ++launches_;
         ++used;
       }
-      for (int i = 0; i < std::min(used, NAUX); ++i) {
+      for (int i = 0; i < std::min(used, naux_); ++i) {
         NRGB_CUDA(cudaEventRecord(join_[i], aux_[i]));
         NRGB_CUDA(cudaStreamWaitEvent(st, join_[i], 0));
       }

@@ -92,7 +92,8 @@ class SyevBatched : public EigSolver {
   // the schedule's limit when it is lower (schedule.cuh)
   int cl_use() const;
   // side streams on which the cluster launches of different sizes overlap
-  static constexpr int NAUX = 6;
+  static constexpr int NAUX = 16;
+  int naux_ = NAUX;  // side streams in use (NRGB_SIDE_STREAMS, for comparisons)
   cudaStream_t aux_[NAUX] = {};
   cudaEvent_t fork_ = nullptr, join_[NAUX] = {};
   // the warp solver for blocks up to 32 runs beside the larger blocks' work

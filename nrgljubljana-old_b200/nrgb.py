@@ -6,6 +6,7 @@ fails loudly when the shared object is missing or no CUDA device is present.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -20,7 +21,7 @@ EXPORTS = ["nrgb_create", "nrgb_destroy", "nrgb_last_error", "nrgb_version",
            "nrgb_set_wait_limit", "nrgb_inject_barrier_shortfall",
            "nrgb_autotune", "nrgb_set_schedule", "nrgb_get_schedule",
            "nrgb_mat_upload", "nrgb_mat_download", "nrgb_mat_shape", "nrgb_mat_free", "nrgb_run_begin",
-           "nrgb_step", "nrgb_recalc",
+           "nrgb_step", "nrgb_recalc", "nrgb_dm_backward", "nrgb_spectrum_fdm", "nrgb_spectrum_dmnrg",
            "nrgb_server_create", "nrgb_server_submit", "nrgb_server_wait", "nrgb_server_error",
            "nrgb_server_counters", "nrgb_server_destroy", "nrgb_project_bytes"]
 
@@ -55,6 +56,25 @@ class RecalcTerm(C.Structure):
 
 class RecalcOut(C.Structure):
     _fields_ = [("k1", C.c_int), ("kp", C.c_int), ("term0", C.c_int), ("nterms", C.c_int)]
+
+
+class DmTerm(C.Structure):
+    _fields_ = [("z1", C.c_int), ("off1", C.c_int), ("k1", C.c_int), ("zp", C.c_int), ("offp", C.c_int),
+                ("kp", C.c_int), ("rho", C.c_int), ("factor", C.c_double)]
+
+
+class DmOut(C.Structure):
+    _fields_ = [("r1", C.c_int), ("rp", C.c_int), ("term0", C.c_int), ("nterms", C.c_int)]
+
+
+class FdmPair(C.Structure):
+    _fields_ = [("op1", C.c_int), ("op2", C.c_int), ("rho_i", C.c_int), ("rho_j", C.c_int), ("e_i", C.c_int),
+                ("e_j", C.c_int), ("reti", C.c_int), ("retj", C.c_int), ("factor", C.c_double)]
+
+
+class DmnrgPair(C.Structure):
+    _fields_ = [("op1", C.c_int), ("op2", C.c_int), ("rho_1", C.c_int), ("rho_p", C.c_int), ("e_1", C.c_int),
+                ("e_p", C.c_int), ("factor", C.c_double)]
 
 
 class GemmOut(C.Structure):
@@ -95,6 +115,11 @@ def load(path: str = LIBPATH):
     lib.nrgb_run_begin.argtypes = [vp]
     lib.nrgb_step.argtypes = [vp, C.POINTER(StepPlan), ip, ip, ip, dp, dp]
     lib.nrgb_recalc.argtypes = [vp, C.c_int, C.POINTER(RecalcOut), C.c_int, C.POINTER(RecalcTerm), ip]
+    lib.nrgb_dm_backward.argtypes = [vp, C.c_int, C.POINTER(DmOut), C.c_int, C.POINTER(DmTerm), ip]
+    lib.nrgb_spectrum_fdm.argtypes = [vp, C.c_int, C.POINTER(FdmPair), C.c_double, C.c_double, C.c_int,
+                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, dp]
+    lib.nrgb_spectrum_dmnrg.argtypes = [vp, C.c_int, C.POINTER(DmnrgPair), C.c_double, C.c_double, C.c_double,
+                                        C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, dp]
     lib.nrgb_set_schedule.argtypes = [vp, C.c_int, C.c_int]
     lib.nrgb_get_schedule.argtypes = [vp, ip, ip, ip]
     lib.nrgb_inject_barrier_shortfall.argtypes = [vp, C.c_int]
@@ -284,6 +309,41 @@ class Context:
         hs = (C.c_int * max(1, n))()
         self._check(self.lib.nrgb_recalc(self.h, n, o, len(terms), t, hs), "nrgb_recalc")
         return list(hs)[:n]
+
+    def dm_backward(self, outs, terms):
+        """Density-matrix backward step (nrgb_dm_backward): one new handle per
+        output, out = sum factor * Z1sub rho Zpsub^T."""
+        n = len(outs)
+        o = (DmOut * max(1, n))(*outs)
+        t = (DmTerm * max(1, len(terms)))(*terms)
+        hs = (C.c_int * max(1, n))()
+        self._check(self.lib.nrgb_dm_backward(self.h, n, o, len(terms), t, hs), "nrgb_dm_backward")
+        return list(hs)[:n]
+
+    def spectrum_fdm(self, pairs, T, wn, fermionic, bins_per_decade, emin, emax, discard=1e-16):
+        """FDM spectral weights of block pairs binned on the log grid
+        (nrgb_spectrum_fdm): returns (positive, negative) bin arrays."""
+        import numpy as np
+        nb = int((math.ceil(math.log10(emax)) - math.floor(math.log10(emin))) * bins_per_decade + 1.0)
+        p = (FdmPair * max(1, len(pairs)))(*pairs)
+        out = np.zeros(2 * nb)
+        self._check(self.lib.nrgb_spectrum_fdm(self.h, len(pairs), p, T, wn, int(fermionic), bins_per_decade, emin,
+                                               emax, discard, nb, out.ctypes.data_as(C.POINTER(C.c_double))),
+                    "nrgb_spectrum_fdm")
+        return out[:nb], out[nb:]
+
+    def spectrum_dmnrg(self, pairs, scale, ewin_min, ewin_max, fermionic, bins_per_decade, emin, emax,
+                       discard=1e-16):
+        """DM-NRG spectral weights of block pairs binned on the log grid
+        (nrgb_spectrum_dmnrg): returns (positive, negative) bin arrays."""
+        import numpy as np
+        nb = int((math.ceil(math.log10(emax)) - math.floor(math.log10(emin))) * bins_per_decade + 1.0)
+        p = (DmnrgPair * max(1, len(pairs)))(*pairs)
+        out = np.zeros(2 * nb)
+        self._check(self.lib.nrgb_spectrum_dmnrg(self.h, len(pairs), p, scale, ewin_min, ewin_max, int(fermionic),
+                                                 bins_per_decade, emin, emax, discard, nb,
+                                                 out.ctypes.data_as(C.POINTER(C.c_double))), "nrgb_spectrum_dmnrg")
+        return out[:nb], out[nb:]
 
     def set_wait_limit(self, poll_log2: int):
         """Device barrier waits give up after 2**poll_log2 polls (default 23)."""
