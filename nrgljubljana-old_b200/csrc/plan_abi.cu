@@ -490,7 +490,7 @@ int nrgb_spectrum_fdm(nrgb_ctx* ctx, int npairs, const nrgb_fdm_pair* pairs, dou
     // per pair: the two products with the density matrices and the
     // Boltzmann factors of both blocks' states
     size_t bytes = 2 * (size_t)nbins * sizeof(double) + (size_t)npairs * sizeof(SpecFdmPair) + 8192;
-    std::vector<double> hx;  // exp(-E/T) of every pair's two energy lists, back to back
+    std::vector<double> hx;  // every pair's two energy lists, back to back, then exp(-E/T) in place
     std::vector<size_t> xo(2 * (size_t)npairs);
     for (int k = 0; k < npairs; ++k) {
       const nrgb_fdm_pair& q = pairs[k];
@@ -504,13 +504,20 @@ int nrgb_spectrum_fdm(nrgb_ctx* ctx, int npairs, const nrgb_fdm_pair* pairs, dou
         const PlanMatrix& E = mat(ctx, side ? q.e_j : q.e_i);
         const int want = side ? A.rows : A.cols;
         if ((long)E.rows * E.cols != want) throw CudaError("nrgb_spectrum_fdm: energy list length differs from the block");
-        std::vector<double> e(want);
-        if (want) NRGB_CUDA(cudaMemcpyAsync(e.data(), E.p, want * sizeof(double), cudaMemcpyDeviceToHost, st));
-        NRGB_CUDA(cudaStreamSynchronize(st));
         xo[2 * k + side] = hx.size();
-        for (double x : e) hx.push_back(exp(-x / T));
+        hx.resize(hx.size() + want);
       }
     }
+    for (int k = 0; k < npairs; ++k)
+      for (int side = 0; side < 2; ++side) {
+        const PlanMatrix& E = mat(ctx, side ? pairs[k].e_j : pairs[k].e_i);
+        const size_t want = (size_t)E.rows * E.cols;
+        if (want)
+          NRGB_CUDA(cudaMemcpyAsync(hx.data() + xo[2 * k + side], E.p, want * sizeof(double), cudaMemcpyDeviceToHost,
+                                    st));
+      }
+    NRGB_CUDA(cudaStreamSynchronize(st));
+    for (double& x : hx) x = exp(-x / T);
     bytes += hx.size() * sizeof(double) + (size_t)(4 * npairs + 16) * 512;  // allocations and their alignment
     ctx->scratch.reserve(bytes + (size_t)(2 * npairs + 8) * (sizeof(GemmProb) + sizeof(GemmSeg)));
     ctx->scratch.reset();

@@ -332,34 +332,63 @@ class SymmetrySPSU2 : public Symmetry {
 };
 
 // QSZ plug-in: charge U(1) x spin-projection U(1), invariant subspaces
-// (Q, SSZ) with SSZ = 2 S_z (src/sym-QSZ.cc), one channel.  Every state is
-// its own multiplet (mult 1); both spin components of f^dag share one list of
-// matrix elements <I1|f^dag_sigma|I2>, I1 = I2 + (1, +-1) (the reference's
-// perchannel = 1 for QSZ, src/read-input.cc:67-74).
+// (Q, SSZ) with SSZ = 2 S_z (src/sym-QSZ.cc), one or two channels.  Every
+// state is its own multiplet (mult 1); both spin components of f^dag share
+// one list of matrix elements <I1|f^dag_sigma|I2> per channel, I1 = I2 +
+// (1, +-1) (the reference's perchannel = 1 for QSZ, src/read-input.cc:67-74).
 //
-// Tables (coefnew/qsz/qsz-1ch-*.dat): combination i of a subspace I has the
-// ancestor I + In[i] and the new site in state i: empty, down, up, doubly
-// occupied (QN).  With the new site's operators to the left of the chain's,
-// |s_i, a> = c_i |a>, c = (1, f^dag_dn, f^dag_up, f^dag_up f^dag_dn):
-//  * hopping f^dag_N,s f_N+1,s (+ h.c.) between combinations i < j: the
-//    site's f_s takes c_j to c_i with sign +-1 and f^dag_N,s passes the n_i
-//    site electrons of c_i: (1,2) +1, (1,3) +1, (2,4) -1, (3,4) +1
-//    (qsz-1ch-offdiag.dat);
-//  * <f^dag_s> of the new site: up (I1 = Ip + (1, 1)): (3 <- 1) +1,
-//    (4 <- 2) +1 (qsz-1ch-spinupa.dat); down (I1 = Ip + (1, -1)): (2 <- 1)
-//    +1, (4 <- 3) -1 (qsz-1ch-spindowna.dat);
-//  * electrons of the new site per combination 0, 1, 1, 2 (qsz-1ch-diag.dat).
-// Thermodynamics columns <Sz^2>, <Sz>, <Q>, <Q^2> (calculate_TD,
+// Without spin multiplets every combination of a subspace is one Fock state
+// of the added site (modes 2 ch + spin, spin up first, creation operators
+// applied in increasing mode order, phase +1) on an ancestor I - QN(state);
+// the tables follow from the site's operators alone:
+//  * hopping f^dag_N,ch,s f_N+1,ch,s (+ h.c.) between combinations i < j:
+//    the site's f_ch,s takes state j to state i (sign from the modes below)
+//    and f^dag_N,ch,s passes the n_i site electrons of i (qsz-<P>ch-offdiag);
+//  * <f^dag_ch,s> of the new site between combinations of one ancestor
+//    (qsz-<P>ch-spinup*, spindown*);
+//  * doublet operators of the chain through the site: rows (i, i) with sign
+//    (-1)^n_i (qsz-<P>ch-doubletp, doubletm);
+//  * electrons of the new site per channel (qsz-<P>ch-diag).
+// The combinations are listed in the reference's order (its In2/QN tables);
+// the tests check every table entry against the reference's for 1 and 2
+// channels.  Thermodynamics columns <Sz^2>, <Sz>, <Q>, <Q^2> (calculate_TD,
 // src/sym-QSZ.cc:73-94).  Doublet operators and their spin-resolved
 // spectral functions are provided; triplet operators are not.
 class SymmetryQSZ : public Symmetry {
  public:
-  SymmetryQSZ() {
-    in_ = {{1, 0}, {0, 1}, {0, -1}, {-1, 0}};
-    qn_ = {{-1, 0}, {0, -1}, {0, 1}, {1, 0}};
+  explicit SymmetryQSZ(int channels = 1) : nch_(channels) {
+    // site Fock states of the combinations (bit 2 ch + s: channel ch, spin s = 0 up, 1 down)
+    static const int COMB_1CH[] = {0x0, 0x2, 0x1, 0x3};
+    static const int COMB_2CH[] = {0x0, 0x8, 0x2, 0x4, 0x1, 0xA, 0xC, 0x6, 0x9, 0x3, 0x5, 0xE, 0xB, 0xD, 0x7, 0xF};
+    if (channels != 1 && channels != 2) throw std::runtime_error("QSZ symmetry: this build provides 1 and 2 channels");
+    const int* cb = channels == 1 ? COMB_1CH : COMB_2CH;
+    const int n = 1 << (2 * channels);
+    for (int i = 0; i < n; ++i) {
+      bits_.push_back(cb[i]);
+      int ne = 0, sz = 0;
+      for (int m = 0; m < 2 * channels; ++m)
+        if ((cb[i] >> m) & 1) {
+          ++ne;
+          sz += (m & 1) ? -1 : 1;
+        }
+      qn_.push_back({ne - channels, sz});
+      in_.push_back({channels - ne, -sz});
+    }
+    // hopping terms (they do not depend on the subspace)
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j)
+        for (int ch = 0; ch < channels; ++ch) {
+          double v = 0.0;
+          for (int sp = 0; sp < 2; ++sp) {
+            int b = 0;
+            const int sg = annihilate(bits_[j], 2 * ch + sp, b);
+            if (sg && b == bits_[i]) v += sg * ((popc(bits_[i]) & 1) ? -1.0 : 1.0);
+          }
+          if (v != 0.0) off_.push_back({i + 1, j + 1, ch, v});
+        }
   }
   std::string name() const override { return "QSZ"; }
-  int combs() const override { return 4; }
+  int combs() const override { return (int)bits_.size(); }
   const std::vector<Invar>& In() const override { return in_; }
   const std::vector<Invar>& QN() const override { return qn_; }
   int mult(const Invar&) const override { return 1; }
@@ -370,22 +399,39 @@ class SymmetryQSZ : public Symmetry {
   Invar singlet() const override { return {0, 0}; }
   Invar doublet() const override { return {1, 1}; }
   Invar triplet() const override { return {0, 2}; }
-  std::vector<OffdiagTerm> offdiag(const Invar&) const override {
-    return {{1, 2, 0, 1.0}, {1, 3, 0, 1.0}, {2, 4, 0, -1.0}, {3, 4, 0, 1.0}};
+  std::vector<OffdiagTerm> offdiag(const Invar&) const override { return off_; }
+  std::vector<DiagTerm> diag() const override {
+    std::vector<DiagTerm> out;
+    for (int ch = 0; ch < nch_; ++ch)
+      for (int i = 0; i < combs(); ++i)
+        out.push_back({i + 1, ch, (double)(((bits_[i] >> (2 * ch)) & 1) + ((bits_[i] >> (2 * ch + 1)) & 1))});
+    return out;
   }
-  std::vector<DiagTerm> diag() const override { return {{1, 0, 0.0}, {2, 0, 1.0}, {3, 0, 1.0}, {4, 0, 2.0}}; }
   std::vector<RecalcTable> recalc_f(const Invar& Ip) const override {
-    const int qp = Ip.first, zp = Ip.second;
-    return {{{qp + 1, zp + 1}, 0, {{3, 1, 1.0}, {4, 2, 1.0}}},
-            {{qp + 1, zp - 1}, 0, {{2, 1, 1.0}, {4, 3, -1.0}}}};
+    std::vector<RecalcTable> out;
+    for (int sp = 0; sp < 2; ++sp)  // up: I1 = Ip + (1, 1); down: Ip + (1, -1)
+      for (int ch = 0; ch < nch_; ++ch) {
+        const Invar I1{Ip.first + 1, Ip.second + (sp ? -1 : 1)};
+        RecalcTable t{I1, ch, {}};
+        for (int i1 = 0; i1 < combs(); ++i1)
+          for (int ip = 0; ip < combs(); ++ip) {
+            if (combine(in_[i1], I1) != combine(in_[ip], Ip)) continue;
+            int b = 0;
+            const int sg = create(bits_[ip], 2 * ch + sp, b);
+            if (sg && b == bits_[i1]) t.rows.push_back({i1 + 1, ip + 1, (double)sg});
+          }
+        out.push_back(t);
+      }
+    return out;
   }
   // Doublet operators (d^dag_s of the impurity) recalculated through the new
   // site: d^dag passes the n_i electrons of the site, rows (i, i) with sign
   // (-1)^n_i, for the spin-up component (Ip = I1 - (1, 1)) and the spin-down
-  // one (Ip = I1 - (1, -1)) (qsz-1ch-doubletp.dat, qsz-1ch-doubletm.dat).
+  // one (Ip = I1 - (1, -1)) (qsz-<P>ch-doubletp.dat, qsz-<P>ch-doubletm.dat).
   std::vector<RecalcTable> recalc_doublet(const Invar& I1) const override {
     const int q1 = I1.first, z1 = I1.second;
-    const std::vector<RecalcRow> rows = {{1, 1, 1.0}, {2, 2, -1.0}, {3, 3, -1.0}, {4, 4, 1.0}};
+    std::vector<RecalcRow> rows;
+    for (int i = 0; i < combs(); ++i) rows.push_back({i + 1, i + 1, (popc(bits_[i]) & 1) ? -1.0 : 1.0});
     return {{{q1 - 1, z1 - 1}, 0, rows}, {{q1 - 1, z1 + 1}, 0, rows}};
   }
   std::vector<RecalcTable> recalc_triplet(const Invar&) const override {
@@ -429,7 +475,22 @@ class SymmetryQSZ : public Symmetry {
   }
 
  private:
+  static int popc(int b) { return __builtin_popcount((unsigned)b); }
+  // sign of the fermion operator on Fock state b (modes below m counted), 0 if it vanishes
+  static int create(int b, int m, int& out) {
+    if ((b >> m) & 1) return 0;
+    out = b | (1 << m);
+    return (popc(b & ((1 << m) - 1)) & 1) ? -1 : 1;
+  }
+  static int annihilate(int b, int m, int& out) {
+    if (!((b >> m) & 1)) return 0;
+    out = b & ~(1 << m);
+    return (popc(b & ((1 << m) - 1)) & 1) ? -1 : 1;
+  }
+  int nch_;
+  std::vector<int> bits_;
   std::vector<Invar> in_, qn_;
+  std::vector<OffdiagTerm> off_;
 };
 
 }  // namespace nrgb

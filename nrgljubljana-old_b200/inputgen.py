@@ -602,14 +602,16 @@ def decompose_qsz(m: ClusterModel) -> List[Subspace]:
 
 def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: int,
                    xi: np.ndarray, zeta: np.ndarray, discretization: str = "Y") -> dict:
-    """Write a version-9 `data` file of the QSZ symmetry (one channel): the
-    sector energies, the matrix elements <I1|f^dag_sigma|I2> of the first chain
-    site for both spins in one list (I1 = I2 + (1, +-1); the reference keeps
-    one f list per channel for QSZ, src/read-input.cc:67-74, 131-145), the
-    singlet operators and the doublet operators (both spins in one list, like
-    f).  Triplet operators are not written."""
-    if len(m.f_orbitals) != 1:
-        raise ValueError("QSZ data: one channel")
+    """Write a version-9 `data` file of the QSZ symmetry (one or two
+    channels): the sector energies, the matrix elements <I1|f^dag_sigma|I2>
+    of the first chain site of each channel for both spins in one list
+    (I1 = I2 + (1, +-1); the reference keeps one f list per channel for QSZ,
+    src/read-input.cc:67-74, 131-145), the singlet operators and the doublet
+    operators (both spins in one list, like f).  Triplet operators are not
+    written."""
+    nch = len(m.f_orbitals)
+    if nch not in (1, 2):
+        raise ValueError("QSZ data: one or two channels")
     F = m.fock
     subs = decompose_qsz(m)
     smap = {(s.Q, s.SS): s for s in subs}
@@ -619,7 +621,7 @@ def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: in
              "# symtype QSZ",
              "#!9",
              "# Number of channels, chain sites, subspaces: ",
-             "%d %d %d" % (1, Nmax, len(subs)),
+             "%d %d %d" % (nch, Nmax, len(subs)),
              "# SCALE " + _fmt(sc0),
              "# Energies (GS energy subtracted, multiplied by 1/SCALE):"]
     for s in subs:
@@ -627,18 +629,19 @@ def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: in
         lines.append("%d" % len(s.energies))
         lines.append(" ".join(_fmt((e - gs) / sc0) for e in s.energies))
     lines.append("# Irreducible matrix elements for Wilson chains:")
-    orb = m.f_orbitals[0]
-    f = {}
-    for (q2, z2), s2 in smap.items():
-        for spin, dz in ((0, +1), (1, -1)):
-            key1 = (q2 + 1, z2 + dz)
-            if key1 in smap:
-                f[(key1, (q2, z2))] = smap[key1].vectors.T @ F.cd(orb, spin) @ s2.vectors
-    lines.append("f 0 0")
-    lines.append("%d" % len(f))
-    for (k1, k2), M in f.items():
-        lines.append("%d %d %d %d" % (k1[0], k1[1], k2[0], k2[1]))
-        _write_matrix(lines, M)
+    for ch in range(nch):
+        orb = m.f_orbitals[ch]
+        f = {}
+        for (q2, z2), s2 in smap.items():
+            for spin, dz in ((0, +1), (1, -1)):
+                key1 = (q2 + 1, z2 + dz)
+                if key1 in smap:
+                    f[(key1, (q2, z2))] = smap[key1].vectors.T @ F.cd(orb, spin) @ s2.vectors
+        lines.append("f %d 0" % ch)
+        lines.append("%d" % len(f))
+        for (k1, k2), M in f.items():
+            lines.append("%d %d %d %d" % (k1[0], k1[1], k2[0], k2[1]))
+            _write_matrix(lines, M)
     lines.append("# GS energy in absolute units:")
     lines.append("e")
     lines.append(_fmt(gs))
@@ -664,10 +667,10 @@ def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: in
             _write_matrix(lines, M)
     lines.append("# Discretization tables:")
     lines.append("z")
-    lines.append("%d" % (len(xi) - 1))
-    lines.extend(_fmt(x) for x in xi)
-    lines.append("%d" % (len(zeta) - 1))
-    lines.extend(_fmt(x) for x in zeta)
+    for t in (xi, zeta):
+        for ch in range(nch):
+            lines.append("%d" % (len(t) - 1))
+            lines.extend(_fmt(x) for x in t)
     lines.append("")
     with open(path, "w") as fh:
         fh.write("\n".join(lines))
@@ -846,8 +849,8 @@ def make_kondo(dirpath: str, J: List[float], Lambda: float, Nmax: int, z: float 
                params: Dict[str, object] | None = None, dps: int = 200, discretization: str = "Y",
                symtype: str = "QS") -> dict:
     """Generate `data` and `param` for the Kondo model with len(J) channels on
-    a flat band, symmetry QS or SPSU2 (SPSU2: a normal band, the pairing
-    and anomalous-hopping tables zero)."""
+    a flat band, symmetry QS, QSZ or SPSU2 (SPSU2: a normal band, the
+    pairing and anomalous-hopping tables zero)."""
     os.makedirs(dirpath, exist_ok=True)
     xi, zeta = wilson_chain_flat(Lambda, z, Nmax, dps=dps, discretization=discretization)
     m = kondo_cluster(J)
@@ -855,10 +858,12 @@ def make_kondo(dirpath: str, J: List[float], Lambda: float, Nmax: int, z: float 
         zero = np.zeros(Nmax + 1)
         info = write_data_spsu2(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, zero, zero,
                                 discretization)
+    elif symtype == "QSZ":
+        info = write_data_qsz(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, discretization)
     elif symtype == "QS":
         info = write_data(os.path.join(dirpath, "data"), m, Lambda, z, Nmax, xi, zeta, len(J), discretization)
     else:
-        raise ValueError("symtype QS or SPSU2")
+        raise ValueError("symtype QS, QSZ or SPSU2")
     p = {"Lambda": Lambda, "z": z, "discretization": discretization}
     if params:
         p.update(params)
