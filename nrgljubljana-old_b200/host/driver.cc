@@ -1588,7 +1588,7 @@ struct NrgDriver::Impl {
     if (D.symtype == "QS") {
       sym.reset(new SymmetryQS(D.channels));
     } else if (D.symtype == "QSZ") {
-      if (D.channels != 1 && D.channels != 2) throw std::runtime_error("symmetry type QSZ: 1 and 2 channels are built");
+      if (D.channels < 1 || D.channels > 3) throw std::runtime_error("symmetry type QSZ: 1 to 3 channels are built");
       if (!P.spect.empty() || !P.specs.empty())
         throw std::runtime_error("symmetry type QSZ: only the spectral functions of doublet operators are built");
       sym.reset(new SymmetryQSZ(D.channels));

@@ -332,7 +332,7 @@ class SymmetrySPSU2 : public Symmetry {
 };
 
 // QSZ plug-in: charge U(1) x spin-projection U(1), invariant subspaces
-// (Q, SSZ) with SSZ = 2 S_z (src/sym-QSZ.cc), one or two channels.  Every
+// (Q, SSZ) with SSZ = 2 S_z (src/sym-QSZ.cc), one to three channels.  Every
 // state is its own multiplet (mult 1); both spin components of f^dag share
 // one list of matrix elements <I1|f^dag_sigma|I2> per channel, I1 = I2 +
 // (1, +-1) (the reference's perchannel = 1 for QSZ, src/read-input.cc:67-74).
@@ -350,7 +350,7 @@ class SymmetrySPSU2 : public Symmetry {
 //    (-1)^n_i (qsz-<P>ch-doubletp, doubletm);
 //  * electrons of the new site per channel (qsz-<P>ch-diag).
 // The combinations are listed in the reference's order (its In2/QN tables);
-// the tests check every table entry against the reference's for 1 and 2
+// the tests check every table entry against the reference's for 1 to 3
 // channels.  Thermodynamics columns <Sz^2>, <Sz>, <Q>, <Q^2> (calculate_TD,
 // src/sym-QSZ.cc:73-94).  Doublet operators and their spin-resolved
 // spectral functions are provided; triplet operators are not.
@@ -360,8 +360,13 @@ class SymmetryQSZ : public Symmetry {
     // site Fock states of the combinations (bit 2 ch + s: channel ch, spin s = 0 up, 1 down)
     static const int COMB_1CH[] = {0x0, 0x2, 0x1, 0x3};
     static const int COMB_2CH[] = {0x0, 0x8, 0x2, 0x4, 0x1, 0xA, 0xC, 0x6, 0x9, 0x3, 0x5, 0xE, 0xB, 0xD, 0x7, 0xF};
-    if (channels != 1 && channels != 2) throw std::runtime_error("QSZ symmetry: this build provides 1 and 2 channels");
-    const int* cb = channels == 1 ? COMB_1CH : COMB_2CH;
+    static const int COMB_3CH[] = {
+        0x00, 0x20, 0x08, 0x02, 0x10, 0x04, 0x01, 0x28, 0x22, 0x0A, 0x30, 0x18, 0x24, 0x0C, 0x12, 0x06,
+        0x21, 0x09, 0x03, 0x14, 0x11, 0x05, 0x2A, 0x38, 0x2C, 0x32, 0x1A, 0x26, 0x0E, 0x29, 0x23, 0x0B,
+        0x34, 0x1C, 0x16, 0x31, 0x19, 0x25, 0x0D, 0x13, 0x07, 0x15, 0x3A, 0x2E, 0x2B, 0x3C, 0x36, 0x1E,
+        0x39, 0x2D, 0x33, 0x1B, 0x27, 0x0F, 0x35, 0x1D, 0x17, 0x3E, 0x3B, 0x2F, 0x3D, 0x37, 0x1F, 0x3F};
+    if (channels < 1 || channels > 3) throw std::runtime_error("QSZ symmetry: this build provides 1 to 3 channels");
+    const int* cb = channels == 1 ? COMB_1CH : channels == 2 ? COMB_2CH : COMB_3CH;
     const int n = 1 << (2 * channels);
     for (int i = 0; i < n; ++i) {
       bits_.push_back(cb[i]);

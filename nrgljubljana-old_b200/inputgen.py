@@ -602,7 +602,7 @@ def decompose_qsz(m: ClusterModel) -> List[Subspace]:
 
 def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: int,
                    xi: np.ndarray, zeta: np.ndarray, discretization: str = "Y") -> dict:
-    """Write a version-9 `data` file of the QSZ symmetry (one or two
+    """Write a version-9 `data` file of the QSZ symmetry (one to three
     channels): the sector energies, the matrix elements <I1|f^dag_sigma|I2>
     of the first chain site of each channel for both spins in one list
     (I1 = I2 + (1, +-1); the reference keeps one f list per channel for QSZ,
@@ -610,8 +610,8 @@ def write_data_qsz(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: in
     operators (both spins in one list, like f).  Triplet operators are not
     written."""
     nch = len(m.f_orbitals)
-    if nch not in (1, 2):
-        raise ValueError("QSZ data: one or two channels")
+    if nch not in (1, 2, 3):
+        raise ValueError("QSZ data: one to three channels")
     F = m.fock
     subs = decompose_qsz(m)
     smap = {(s.Q, s.SS): s for s in subs}

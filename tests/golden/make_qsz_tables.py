@@ -1,5 +1,5 @@
-"""Generate tests/golden/qsz_tables.json from the reference's 1- and
-2-channel QSZ coefficient tables (coefnew/qsz/qsz-<P>ch-*.dat, included by
+"""Generate tests/golden/qsz_tables.json from the reference's 1-, 2- and
+3-channel QSZ coefficient tables (coefnew/qsz/qsz-<P>ch-*.dat, included by
 src/sym-QSZ.cc:38-60, :133-160 and src/nrg-recalc-QSZ.cc).  Run in a
 container that has the reference checkout:
 
@@ -19,7 +19,9 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 from make_qs_tables import _eval, _split_args  # noqa: E402
 
 FILES = {1: ["In2", "QN", "offdiag", "diag", "spinupa", "spindowna", "doubletp", "doubletm"],
-         2: ["In2", "QN", "offdiag", "diag", "spinupa", "spinupb", "spindowna", "spindownb", "doubletp", "doubletm"]}
+         2: ["In2", "QN", "offdiag", "diag", "spinupa", "spinupb", "spindowna", "spindownb", "doubletp", "doubletm"],
+         3: ["In2", "QN", "offdiag", "diag", "spinupa", "spinupb", "spinupc", "spindowna", "spindownb",
+             "spindownc", "doubletp", "doubletm"]}
 
 
 def main(refroot, out):

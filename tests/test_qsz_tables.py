@@ -1,7 +1,7 @@
 """The QSZ plug-in's tables (host/symmetry.h, SymmetryQSZ: every
 combination one Fock state of the added site) against the reference's
 (coefnew/qsz/qsz-<P>ch-*.dat, evaluated into tests/golden/qsz_tables.json by
-tests/golden/make_qsz_tables.py), for 1 and 2 channels: the combinations'
+tests/golden/make_qsz_tables.py), for 1 to 3 channels: the combinations'
 quantum numbers, hopping, site occupancies, the <f^dag> recalculation of
 both spins and channels, and the doublet recalculation.  The plug-in is
 compiled with the host compiler into a small dump program (no device)."""
@@ -31,7 +31,7 @@ def dump(tmp_path_factory):
     return run
 
 
-@pytest.mark.parametrize("P", [1, 2])
+@pytest.mark.parametrize("P", [1, 2, 3])
 def test_qsz_plugin_matches_reference_tables(dump, P):
     G, D = GOLD[str(P)], dump(P)
     assert sorted(map(tuple, D["In"]["rows"])) == sorted(map(tuple, G["In2"]))
@@ -41,7 +41,7 @@ def test_qsz_plugin_matches_reference_tables(dump, P):
     # <f^dag>: I1 = Ip + (1, +1) (spin up) and Ip + (1, -1) (spin down), per channel
     got = {}
     for I1, ch, rows in D["recalc_f"]["tables"]:
-        name = ("spinup" if I1[1] == 1 else "spindown") + "ab"[ch]
+        name = ("spinup" if I1[1] == 1 else "spindown") + "abc"[ch]
         got[name] = sorted(map(tuple, rows))
     for name in got:
         assert got[name] == sorted(map(tuple, G[name])), name
