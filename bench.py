@@ -773,6 +773,58 @@ def run_split_micro(edge, slices, nprob):
     return 0
 
 
+def run_gemm_micro():
+    """Grouped FP64 GEMM (the kernel NRGB_GEMM_PIPE selects in this process)
+    on square problems in all four transpose combinations, and cuBLAS DGEMM
+    (torch.bmm) on the same untransposed problems; device-resident inputs,
+    CUDA events on the launch stream, best of 5.  Prints one JSON object of
+    TF/s per case."""
+    import torch
+
+    import nrgb
+    dev = torch.device("cuda", 0)
+    ctx = nrgb.Context(0)
+    st = torch.cuda.current_stream(dev)
+    g = torch.Generator(device=dev).manual_seed(SEED)
+
+    def best_ms(fn):
+        fn()
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(st)
+            fn()
+            t1.record(st)
+            torch.cuda.synchronize()
+            best = min(best, t0.elapsed_time(t1))
+        return best
+
+    pipe = os.environ.get("NRGB_GEMM_PIPE") or "3"
+    out = {"kernel": "register-staged" if pipe == "0" else "pipelined, %s stages" % pipe}
+    for edge, nprob, nseg in ((2048, 4, 1), (1024, 16, 1), (512, 64, 1), (384, 64, 3), (256, 128, 2)):
+        for ta, tb in ((0, 0), (1, 0), (0, 1), (1, 1)):
+            A = [torch.randn(edge, edge, generator=g, device=dev, dtype=torch.float64) for _ in range(nprob * nseg)]
+            B = [torch.randn(edge, edge, generator=g, device=dev, dtype=torch.float64) for _ in range(nprob * nseg)]
+            C = [torch.empty(edge, edge, device=dev, dtype=torch.float64) for _ in range(nprob)]
+            terms = [nrgb.GemmTerm(a.data_ptr(), b.data_ptr(), edge, edge, edge, ta, tb, 1.0) for a, b in zip(A, B)]
+            outs = [nrgb.GemmOut(c.data_ptr(), edge, edge, edge, 0.0, i * nseg, nseg) for i, c in enumerate(C)]
+            ms = best_ms(lambda: ctx.gemm_grouped_dev(outs, terms, stream=st.cuda_stream))
+            key = "%dx%d^3 (%d segments) t%d%d" % (nprob, edge, nseg, ta, tb)
+            out[key] = round(2.0 * edge ** 3 * nprob * nseg / ms / 1e9, 2)
+            if ta == 0 and tb == 0:
+                Ab, Bb = torch.stack(A[:nprob]), torch.stack(B[:nprob])
+                ms2 = best_ms(lambda: torch.bmm(Ab, Bb))
+                out["cublas %dx%d^3" % (nprob, edge)] = round(2.0 * edge ** 3 * nprob / ms2 / 1e9, 2)
+                del Ab, Bb
+            del A, B, C
+            torch.cuda.empty_cache()
+    ctx.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_configs(args):
     """Wall time of one run of each workload through nrgb_run on the GPU
     (batched eigensolves per step; one eigensolver call per block; split
@@ -888,6 +940,8 @@ def main():
     ap.add_argument("--nmax", type=int, default=4096, help="cap on block sizes of the microbenchmark")
     ap.add_argument("--split-micro", type=int, default=0,
                     help="time the split-precision grouped GEMM against FP64 on problems of this edge")
+    ap.add_argument("--gemm-micro", action="store_true",
+                    help="time the grouped FP64 GEMM in all transpose combinations against cuBLAS")
     ap.add_argument("--slices", type=int, default=8)
     ap.add_argument("--one-run", default="", help="one nrgb_run of a test workload (profiling)")
     ap.add_argument("--configs", action="store_true",
@@ -904,6 +958,8 @@ def main():
         return run_ncu_small(args.ncu_small)
     if args.split_micro:
         return run_split_micro(args.split_micro, args.slices, args.nprob)
+    if args.gemm_micro:
+        return run_gemm_micro()
     if args.configs:
         return run_configs(args)
     if args.one_run:

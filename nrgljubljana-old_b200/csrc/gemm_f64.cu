@@ -2,9 +2,13 @@
 // See gemm_f64.cuh for the contract.
 //
 // Tile: 64x64 per CTA, 4 warps of 32x32, K staged 16 at a time through
-// double-buffered shared memory (k-major, padded so the DMMA fragment loads
-// are bank-conflict free).  mma.sync.m8n8k4.f64: A fragment A[g][t],
-// B fragment B[t][g], accumulator C[g][2t..2t+1] with g = lane/4, t = lane%4.
+// shared memory laid out so that the DMMA fragment loads are bank-conflict
+// free: by default a 3-stage cp.async ring (gemm_grouped_pipe_kernel), else
+// register-staged double buffering (gemm_grouped_kernel; also the kernel of
+// the allocation-free entry point) or 128x128 tiles where the schedule picks
+// them.  mma.sync.m8n8k4.f64 (the m16n8k4/k8/k16 f64 shapes run at the same
+// rate on B200): A fragment A[g][t], B fragment B[t][g], accumulator
+// C[g][2t..2t+1] with g = lane/4, t = lane%4.
 #include <atomic>
 #include "common.cuh"
 #include "gemm_f64.cuh"
@@ -379,6 +383,258 @@ __global__ void __launch_bounds__(LNT) gemm_grouped_large_kernel(const GemmProb*
 }
 
 constexpr size_t LSMEM = 2 * (size_t)LSTAGES * BK * LLDS * sizeof(double);
+
+// ---------------------------------------------------------------------------
+// Pipelined variant: the same 64x64 tile, 4 warps of 32x32 and K step of 16,
+// with the operands copied by cp.async into an S-stage ring (no register
+// staging, S-1 K tiles in flight).  Each operand tile keeps the direction in
+// which it is contiguous in global memory:
+//   mn-contiguous (A as stored, B transposed): [BK][64 + 4]
+//   k-contiguous  (A transposed, B as stored): [64][BK], the 16-byte pairs of
+//     row r at pair index (p/2) ^ (2r mod 8)
+// and both are read bank-conflict free by the fragment loads (within a
+// half-warp, lanes g, t hit double offsets 4t + g, resp. 2((k/2 + t/2) ^ 2g)
+// + t%2, mod 16, all distinct).  A segment whose base address
+// and leading dimension are 16-byte aligned is copied in element pairs
+// (16-byte cp.async; the half of a pair outside the matrix is zero-filled),
+// any other segment element by element.
+// ---------------------------------------------------------------------------
+constexpr int PLD_MN = BM + 4;        // 68
+constexpr int PTILE = BK * PLD_MN;    // 1088 doubles >= BM * BK = 1024
+
+// offset of element (row r, K index p) in a k-contiguous tile
+__device__ __forceinline__ int pipe_kofs(int r, int p) {
+  return r * BK + ((((p >> 1) ^ (2 * r)) & 7) << 1) + (p & 1);
+}
+
+__device__ __forceinline__ void cp_async16(double* smem, const double* gmem, int bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+
+// Copy one 64 x BK operand tile: rows mn0 .. mn0+63 (< mnlim) and K columns
+// k0 .. k0+15 (< klim) of a matrix whose element (mn, k) sits at
+// base[mn + k*ld] (mn-contiguous) or base[k + mn*ld] (k-contiguous).
+__device__ __forceinline__ void pipe_load_tile(double* dst, const double* base, int ld, bool kcontig,
+                                               bool vec, int mn0, int mnlim, int k0, int klim, int tid) {
+  if (!kcontig) {
+    if (vec) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int c = tid + NT * r, p = c >> 5, i = 2 * (c & 31);
+        const int gi = mn0 + i, gp = k0 + p;
+        const int bytes = gp < klim ? (gi + 1 < mnlim ? 16 : (gi < mnlim ? 8 : 0)) : 0;
+        cp_async16(dst + p * PLD_MN + i, bytes ? base + (size_t)gp * ld + gi : base, bytes);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int e = tid + NT * r, p = e >> 6, i = e & 63;
+        const int gi = mn0 + i, gp = k0 + p;
+        const bool ok = gi < mnlim && gp < klim;
+        cp_async8(dst + p * PLD_MN + i, ok ? base + (size_t)gp * ld + gi : base, ok);
+      }
+    }
+  } else {
+    if (vec) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int c = tid + NT * r, i = c >> 3, p = 2 * (c & 7);
+        const int gi = mn0 + i, gp = k0 + p;
+        const int bytes = gi < mnlim ? (gp + 1 < klim ? 16 : (gp < klim ? 8 : 0)) : 0;
+        cp_async16(dst + pipe_kofs(i, p), bytes ? base + (size_t)gi * ld + gp : base, bytes);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int e = tid + NT * r, i = e >> 4, p = e & 15;
+        const int gi = mn0 + i, gp = k0 + p;
+        const bool ok = gi < mnlim && gp < klim;
+        cp_async8(dst + pipe_kofs(i, p), ok ? base + (size_t)gi * ld + gp : base, ok);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ bool pipe_vec_ok(const double* p, int ld) {
+  return ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && ((ld & 1) == 0);
+}
+
+// 128 registers at most, so that four CTAs (16 warps) share an SM with the
+// 3-stage ring (52 KB of shared memory each)
+template <int S>
+__global__ void __launch_bounds__(NT, 4) gemm_grouped_pipe_kernel(const GemmProb* __restrict__ probs,
+                                                               int nprob,
+                                                               const GemmSeg* __restrict__ segs) {
+  extern __shared__ __align__(16) double psm[];
+  double* As = psm;                  // [S][PTILE]
+  double* Bs = psm + S * PTILE;      // [S][PTILE]
+  __shared__ double salpha[S];
+  __shared__ int sflags[S];          // bit 0: A k-contiguous, bit 1: B k-contiguous
+
+  const int tile = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (probs[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+  }
+  const GemmProb P = probs[lo];
+  const int ks = P.ksplit > 1 ? P.ksplit : 1;
+  const int t = (tile - P.tile0) / ks;
+  const int kc = (tile - P.tile0) % ks;
+  const int row0 = (t / P.tiles_n) * BM;
+  const int col0 = (t % P.tiles_n) * BN;
+  const int m = P.m, n = P.n;
+  if (row0 >= m || col0 >= n) return;  // shapes may be set on the device below the planned bound
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  // this CTA's share of the flattened (segment, K tile) sequence
+  const int send = P.seg0 + P.nseg;
+  int ktot = 0;
+  for (int q = P.seg0; q < send; ++q) ktot += segs[q].k > 0 ? (segs[q].k + BK - 1) / BK : 0;
+  const int per = (ktot + ks - 1) / ks;
+  const int kt0 = kc * per;
+  const int nk = max(0, min(ktot, kt0 + per) - kt0);
+  int ls = P.seg0, lk0 = 0;
+  {
+    int kt = 0;
+    while (ls < send) {
+      const int nt = segs[ls].k > 0 ? (segs[ls].k + BK - 1) / BK : 0;
+      if (kt + nt > kt0) break;
+      kt += nt;
+      ++ls;
+    }
+    lk0 = (kt0 - kt) * BK;
+  }
+  auto issue = [&](int stage) {
+    const GemmSeg G = segs[ls];
+    // op(A)[i, p]: A[i + p*lda] as stored, A[p + i*lda] transposed
+    pipe_load_tile(As + stage * PTILE, G.A, G.lda, G.transA != 0, pipe_vec_ok(G.A, G.lda), row0, m, lk0, G.k,
+                   tid);
+    // op(B)[p, j]: B[p + j*ldb] as stored (k-contiguous), B[j + p*ldb] transposed
+    pipe_load_tile(Bs + stage * PTILE, G.B, G.ldb, G.transB == 0, pipe_vec_ok(G.B, G.ldb), col0, n, lk0, G.k,
+                   tid);
+    if (tid == 0) {
+      salpha[stage] = G.alpha;
+      sflags[stage] = (G.transA != 0 ? 1 : 0) | (G.transB == 0 ? 2 : 0);
+    }
+    lk0 += BK;
+    if (lk0 >= G.k) {
+      ++ls;
+      while (ls < send && segs[ls].k <= 0) ++ls;
+      lk0 = 0;
+    }
+  };
+#pragma unroll
+  for (int st = 0; st < S - 1; ++st) {
+    if (st < nk) issue(st);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<S - 2>();
+    __syncthreads();
+    const int nxt = kt + S - 1;
+    if (nxt < nk) issue(nxt % S);
+    cp_async_commit();
+    const int stg = kt % S;
+    const double* as = As + stg * PTILE;
+    const double* bs = Bs + stg * PTILE;
+    const double alpha = salpha[stg];
+    const int fl = sflags[stg];
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      double a[4], b[4];
+      if (fl & 1) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = as[pipe_kofs(wm + i * 8 + g, kk + tq)];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = as[(kk + tq) * PLD_MN + wm + i * 8 + g];
+      }
+      if (fl & 2) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = bs[pipe_kofs(wn + j * 8 + g, kk + tq)];
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = bs[(kk + tq) * PLD_MN + wn + j * 8 + g];
+      }
+      if (alpha != 1.0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] *= alpha;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+  }
+  cp_async_wait<0>();
+
+  const double beta = P.beta;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = row0 + wm + i * 8 + g;
+    if (r >= m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = col0 + wn + j * 8 + 2 * tq + h;
+        if (c < n) {
+          double* dst = P.C + (size_t)c * P.ldc + r;
+          const double v = acc[i][j][h];
+          if (ks > 1) atomicAdd(dst, v);
+          else *dst = (beta == 0.0) ? v : v + beta * (*dst);
+        }
+      }
+    }
+  }
+}
+
+template <int S>
+constexpr size_t pipe_smem() { return 2 * (size_t)S * PTILE * sizeof(double); }
+
+// Stage count of the pipelined kernel, 3 by default (measured on B200 at
+// 28-29 TF/s on grouped 2048^3 problems and 21 TF/s on 256^3 ones, against
+// 25-28 and 17-19 TF/s of the register-staged kernel, in all four transpose
+// combinations).  NRGB_GEMM_PIPE=4 selects four stages, NRGB_GEMM_PIPE=0 the
+// register-staged kernel; read once per process.
+int gemm_pipe_stages() {
+  static const int s = [] {
+    const char* e = getenv("NRGB_GEMM_PIPE");
+    if (!e || !*e) return 3;
+    const int v = atoi(e);
+    return (v == 0 || v == 3 || v == 4) ? v : 3;
+  }();
+  return s;
+}
+
+template <int S>
+cudaError_t pipe_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs, int total_tiles,
+                        cudaStream_t stream, const char* tag) {
+  static std::atomic<bool> attr[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 64 || !attr[dev].load(std::memory_order_acquire)) {
+    const cudaError_t e = cudaFuncSetAttribute(gemm_grouped_pipe_kernel<S>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<S>());
+    if (e != cudaSuccess) return e;
+    if (dev < 64) attr[dev].store(true, std::memory_order_release);
+  }
+  NRGB_LAUNCH(tag, stream,
+              gemm_grouped_pipe_kernel<S><<<total_tiles, NT, pipe_smem<S>(), stream>>>(d_probs, nprob, d_segs));
+  return cudaGetLastError();
+}
 // The 128x128 cp.async variant is used only where the device's schedule
 // (schedule.cuh, set by the autotuner's measurements) says it wins: by
 // default never (measured on B200 at first: 21-25 TF/s against 25-28 TF/s
@@ -429,6 +685,9 @@ cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSe
                 gemm_grouped_large_kernel<<<total_stiles, LNT, LSMEM, stream>>>(d_probs, nprob, d_segs));
     return cudaGetLastError();
   }
+  const int stages = gemm_pipe_stages();
+  if (stages == 3) return pipe_launch<3>(d_probs, nprob, d_segs, total_tiles, stream, tag);
+  if (stages == 4) return pipe_launch<4>(d_probs, nprob, d_segs, total_tiles, stream, tag);
   NRGB_LAUNCH(tag, stream, gemm_grouped_kernel<<<total_tiles, NT, 0, stream>>>(d_probs, nprob, d_segs));
   return cudaGetLastError();
 }

@@ -62,6 +62,57 @@ def test_gemm_grouped_segments_and_transposes(ctx):
         assert err <= 1e-13 * scale * 50
 
 
+def test_gemm_grouped_unaligned_views(ctx):
+    """Operands at odd element offsets (base addresses not 16-byte aligned),
+    even leading dimensions above odd row counts (element pairs that cross
+    the matrix edge) and odd K, in all four transpose combinations."""
+    import nrgb
+    rng = np.random.default_rng(11)
+    dev = "cuda:0"
+    outs, terms, refs, keep = [], [], [], []
+    for (m, n, k, off) in [(65, 67, 33, 1), (130, 129, 63, 0), (257, 96, 100, 3), (64, 64, 17, 1)]:
+        for ta in (0, 1):
+            for tb in (0, 1):
+                ra, ca = (k, m) if ta else (m, k)
+                rb, cb = (n, k) if tb else (k, n)
+                lda, ldb = ra + 2 - (ra & 1), rb + 2 - (rb & 1)      # even, above the row count
+                bufA = torch.tensor(rng.standard_normal(off + lda * ca), device=dev)
+                bufB = torch.tensor(rng.standard_normal(off + ldb * cb), device=dev)
+                Asto = bufA[off:].view(ca, lda).t()[:ra]              # column-major ra x ca
+                Bsto = bufB[off:].view(cb, ldb).t()[:rb]
+                A = Asto.t() if ta else Asto
+                B = Bsto.t() if tb else Bsto
+                C0 = torch.tensor(rng.standard_normal((m, n)), device=dev)
+                Cc = _col(C0)
+                keep += [bufA, bufB]
+                t0 = len(terms)
+                terms.append(nrgb.GemmTerm(bufA.data_ptr() + 8 * off, bufB.data_ptr() + 8 * off,
+                                           lda, ldb, k, ta, tb, -0.5))
+                outs.append(nrgb.GemmOut(Cc.data_ptr(), m, m, n, 1.0, t0, 1))
+                refs.append((Cc, C0 - 0.5 * (A @ B)))
+    ctx.gemm_grouped_dev(outs, terms)
+    torch.cuda.synchronize()
+    for Cc, ref in refs:
+        err = (Cc.t() - ref).abs().max().item()
+        assert err <= 1e-13 * (ref.abs().max().item() + 1.0) * 50
+
+
+@pytest.mark.parametrize("stages", ["0", "3", "4"])
+def test_gemm_pipelined_variants(stages):
+    """The grouped GEMM's register-staged kernel (NRGB_GEMM_PIPE=0) and its
+    cp.async-pipelined form with 3 or 4 stages (the switch is read once per
+    process, so each runs the GEMM tests in a child process)."""
+    import subprocess
+    import sys
+    env = dict(os.environ, NRGB_GEMM_PIPE=stages)
+    here = os.path.dirname(os.path.abspath(__file__))
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-p", "no:cacheprovider",
+                        os.path.join(here, "test_kernels_gpu.py"), "-k",
+                        "gemm_grouped_segments or gemm_grouped_unaligned"],
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+
+
 def _random_sym(n, rng, kind):
     if kind == "gauss":
         A = rng.standard_normal((n, n))
