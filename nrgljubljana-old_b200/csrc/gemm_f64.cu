@@ -3,7 +3,8 @@
 //
 // Tile: 64x64 per CTA, 4 warps of 32x32, K staged 16 at a time through
 // shared memory laid out so that the DMMA fragment loads are bank-conflict
-// free: by default a 3-stage cp.async ring (gemm_grouped_pipe_kernel), else
+// free: by default a cp.async ring of two K steps of 32
+// (gemm_grouped_pipe_kernel<2, 32>), else
 // register-staged double buffering (gemm_grouped_kernel; also the kernel of
 // the allocation-free entry point) or 128x128 tiles where the schedule picks
 // them.  mma.sync.m8n8k4.f64 (the m16n8k4/k8/k16 f64 shapes run at the same
@@ -385,12 +386,12 @@ __global__ void __launch_bounds__(LNT) gemm_grouped_large_kernel(const GemmProb*
 constexpr size_t LSMEM = 2 * (size_t)LSTAGES * BK * LLDS * sizeof(double);
 
 // ---------------------------------------------------------------------------
-// Pipelined variant: the same 64x64 tile, 4 warps of 32x32 and K step of 16,
-// with the operands copied by cp.async into an S-stage ring (no register
-// staging, S-1 K tiles in flight).  Each operand tile keeps the direction in
+// Pipelined variant: the same 64x64 tile and 4 warps of 32x32, with the
+// operands copied by cp.async into an S-stage ring of K steps of KB (no
+// register staging, S-1 K tiles in flight).  Each operand tile keeps the direction in
 // which it is contiguous in global memory:
-//   mn-contiguous (A as stored, B transposed): [BK][64 + 4]
-//   k-contiguous  (A transposed, B as stored): [64][BK], the 16-byte pairs of
+//   mn-contiguous (A as stored, B transposed): [KB][64 + 4]
+//   k-contiguous  (A transposed, B as stored): [64][KB], the 16-byte pairs of
 //     row r at pair index (p/2) ^ (2r mod 8)
 // and both are read bank-conflict free by the fragment loads (within a
 // half-warp, lanes g, t hit double offsets 4t + g, resp. 2((k/2 + t/2) ^ 2g)
@@ -400,11 +401,15 @@ constexpr size_t LSMEM = 2 * (size_t)LSTAGES * BK * LLDS * sizeof(double);
 // any other segment element by element.
 // ---------------------------------------------------------------------------
 constexpr int PLD_MN = BM + 4;        // 68
-constexpr int PTILE = BK * PLD_MN;    // 1088 doubles >= BM * BK = 1024
 
-// offset of element (row r, K index p) in a k-contiguous tile
+// doubles per operand tile of K step KB: KB * 68 >= 64 * KB
+template <int KB>
+__host__ __device__ constexpr int ptile() { return KB * PLD_MN; }
+
+// offset of element (row r, K index p) in a k-contiguous tile of K step KB
+template <int KB>
 __device__ __forceinline__ int pipe_kofs(int r, int p) {
-  return r * BK + ((((p >> 1) ^ (2 * r)) & 7) << 1) + (p & 1);
+  return r * KB + (((p >> 1) ^ ((2 * r) & 7)) << 1) + (p & 1);
 }
 
 __device__ __forceinline__ void cp_async16(double* smem, const double* gmem, int bytes) {
@@ -412,15 +417,16 @@ __device__ __forceinline__ void cp_async16(double* smem, const double* gmem, int
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
 }
 
-// Copy one 64 x BK operand tile: rows mn0 .. mn0+63 (< mnlim) and K columns
-// k0 .. k0+15 (< klim) of a matrix whose element (mn, k) sits at
+// Copy one 64 x KB operand tile: rows mn0 .. mn0+63 (< mnlim) and K columns
+// k0 .. k0+KB-1 (< klim) of a matrix whose element (mn, k) sits at
 // base[mn + k*ld] (mn-contiguous) or base[k + mn*ld] (k-contiguous).
+template <int KB>
 __device__ __forceinline__ void pipe_load_tile(double* dst, const double* base, int ld, bool kcontig,
                                                bool vec, int mn0, int mnlim, int k0, int klim, int tid) {
   if (!kcontig) {
     if (vec) {
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
+      for (int r = 0; r < KB / 4; ++r) {
         const int c = tid + NT * r, p = c >> 5, i = 2 * (c & 31);
         const int gi = mn0 + i, gp = k0 + p;
         const int bytes = gp < klim ? (gi + 1 < mnlim ? 16 : (gi < mnlim ? 8 : 0)) : 0;
@@ -428,7 +434,7 @@ __device__ __forceinline__ void pipe_load_tile(double* dst, const double* base, 
       }
     } else {
 #pragma unroll
-      for (int r = 0; r < 8; ++r) {
+      for (int r = 0; r < KB / 2; ++r) {
         const int e = tid + NT * r, p = e >> 6, i = e & 63;
         const int gi = mn0 + i, gp = k0 + p;
         const bool ok = gi < mnlim && gp < klim;
@@ -438,19 +444,19 @@ __device__ __forceinline__ void pipe_load_tile(double* dst, const double* base, 
   } else {
     if (vec) {
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int c = tid + NT * r, i = c >> 3, p = 2 * (c & 7);
+      for (int r = 0; r < KB / 4; ++r) {
+        const int c = tid + NT * r, i = c / (KB / 2), p = 2 * (c % (KB / 2));
         const int gi = mn0 + i, gp = k0 + p;
         const int bytes = gi < mnlim ? (gp + 1 < klim ? 16 : (gp < klim ? 8 : 0)) : 0;
-        cp_async16(dst + pipe_kofs(i, p), bytes ? base + (size_t)gi * ld + gp : base, bytes);
+        cp_async16(dst + pipe_kofs<KB>(i, p), bytes ? base + (size_t)gi * ld + gp : base, bytes);
       }
     } else {
 #pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        const int e = tid + NT * r, i = e >> 4, p = e & 15;
+      for (int r = 0; r < KB / 2; ++r) {
+        const int e = tid + NT * r, i = e / KB, p = e % KB;
         const int gi = mn0 + i, gp = k0 + p;
         const bool ok = gi < mnlim && gp < klim;
-        cp_async8(dst + pipe_kofs(i, p), ok ? base + (size_t)gi * ld + gp : base, ok);
+        cp_async8(dst + pipe_kofs<KB>(i, p), ok ? base + (size_t)gi * ld + gp : base, ok);
       }
     }
   }
@@ -460,13 +466,15 @@ __device__ __forceinline__ bool pipe_vec_ok(const double* p, int ld) {
   return ((reinterpret_cast<uintptr_t>(p) & 15) == 0) && ((ld & 1) == 0);
 }
 
-// 128 registers at most, so that four CTAs (16 warps) share an SM with the
-// 3-stage ring (52 KB of shared memory each)
-template <int S>
+// 128 registers at most, so that shared memory alone sets the CTAs per SM:
+// four with KB = 16 and 3 stages (52 KB each), three with KB = 32 and 2
+// stages (70 KB each)
+template <int S, int KB>
 __global__ void __launch_bounds__(NT, 4) gemm_grouped_pipe_kernel(const GemmProb* __restrict__ probs,
                                                                int nprob,
                                                                const GemmSeg* __restrict__ segs) {
   extern __shared__ __align__(16) double psm[];
+  constexpr int PTILE = ptile<KB>();
   double* As = psm;                  // [S][PTILE]
   double* Bs = psm + S * PTILE;      // [S][PTILE]
   __shared__ double salpha[S];
@@ -501,7 +509,7 @@ __global__ void __launch_bounds__(NT, 4) gemm_grouped_pipe_kernel(const GemmProb
   // this CTA's share of the flattened (segment, K tile) sequence
   const int send = P.seg0 + P.nseg;
   int ktot = 0;
-  for (int q = P.seg0; q < send; ++q) ktot += segs[q].k > 0 ? (segs[q].k + BK - 1) / BK : 0;
+  for (int q = P.seg0; q < send; ++q) ktot += segs[q].k > 0 ? (segs[q].k + KB - 1) / KB : 0;
   const int per = (ktot + ks - 1) / ks;
   const int kt0 = kc * per;
   const int nk = max(0, min(ktot, kt0 + per) - kt0);
@@ -509,26 +517,26 @@ __global__ void __launch_bounds__(NT, 4) gemm_grouped_pipe_kernel(const GemmProb
   {
     int kt = 0;
     while (ls < send) {
-      const int nt = segs[ls].k > 0 ? (segs[ls].k + BK - 1) / BK : 0;
+      const int nt = segs[ls].k > 0 ? (segs[ls].k + KB - 1) / KB : 0;
       if (kt + nt > kt0) break;
       kt += nt;
       ++ls;
     }
-    lk0 = (kt0 - kt) * BK;
+    lk0 = (kt0 - kt) * KB;
   }
   auto issue = [&](int stage) {
     const GemmSeg G = segs[ls];
     // op(A)[i, p]: A[i + p*lda] as stored, A[p + i*lda] transposed
-    pipe_load_tile(As + stage * PTILE, G.A, G.lda, G.transA != 0, pipe_vec_ok(G.A, G.lda), row0, m, lk0, G.k,
+    pipe_load_tile<KB>(As + stage * PTILE, G.A, G.lda, G.transA != 0, pipe_vec_ok(G.A, G.lda), row0, m, lk0, G.k,
                    tid);
     // op(B)[p, j]: B[p + j*ldb] as stored (k-contiguous), B[j + p*ldb] transposed
-    pipe_load_tile(Bs + stage * PTILE, G.B, G.ldb, G.transB == 0, pipe_vec_ok(G.B, G.ldb), col0, n, lk0, G.k,
+    pipe_load_tile<KB>(Bs + stage * PTILE, G.B, G.ldb, G.transB == 0, pipe_vec_ok(G.B, G.ldb), col0, n, lk0, G.k,
                    tid);
     if (tid == 0) {
       salpha[stage] = G.alpha;
       sflags[stage] = (G.transA != 0 ? 1 : 0) | (G.transB == 0 ? 2 : 0);
     }
-    lk0 += BK;
+    lk0 += KB;
     if (lk0 >= G.k) {
       ++ls;
       while (ls < send && segs[ls].k <= 0) ++ls;
@@ -552,18 +560,18 @@ __global__ void __launch_bounds__(NT, 4) gemm_grouped_pipe_kernel(const GemmProb
     const double alpha = salpha[stg];
     const int fl = sflags[stg];
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
+    for (int kk = 0; kk < KB; kk += 4) {
       double a[4], b[4];
       if (fl & 1) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = as[pipe_kofs(wm + i * 8 + g, kk + tq)];
+        for (int i = 0; i < 4; ++i) a[i] = as[pipe_kofs<KB>(wm + i * 8 + g, kk + tq)];
       } else {
 #pragma unroll
         for (int i = 0; i < 4; ++i) a[i] = as[(kk + tq) * PLD_MN + wm + i * 8 + g];
       }
       if (fl & 2) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = bs[pipe_kofs(wn + j * 8 + g, kk + tq)];
+        for (int j = 0; j < 4; ++j) b[j] = bs[pipe_kofs<KB>(wn + j * 8 + g, kk + tq)];
       } else {
 #pragma unroll
         for (int j = 0; j < 4; ++j) b[j] = bs[(kk + tq) * PLD_MN + wn + j * 8 + g];
@@ -601,38 +609,41 @@ __global__ void __launch_bounds__(NT, 4) gemm_grouped_pipe_kernel(const GemmProb
   }
 }
 
-template <int S>
-constexpr size_t pipe_smem() { return 2 * (size_t)S * PTILE * sizeof(double); }
+template <int S, int KB>
+constexpr size_t pipe_smem() { return 2 * (size_t)S * ptile<KB>() * sizeof(double); }
 
-// Stage count of the pipelined kernel, 3 by default (measured on B200 at
-// 28-29 TF/s on grouped 2048^3 problems and 21 TF/s on 256^3 ones, against
-// 25-28 and 17-19 TF/s of the register-staged kernel, in all four transpose
-// combinations).  NRGB_GEMM_PIPE=4 selects four stages, NRGB_GEMM_PIPE=0 the
-// register-staged kernel; read once per process.
+// Form of the grouped GEMM: the pipelined kernel with K step 32 and 2 stages
+// by default (232; measured on B200 at 28.7-30.2 TF/s on grouped 2048^3
+// problems and 20.4-20.7 TF/s on 256^3 ones, against 28.0-29.2 and 20.5-20.9
+// with K step 16 and 3 stages, and 24.8-28.2 and 14.5-19.0 for the
+// register-staged kernel, over the four transpose combinations).
+// NRGB_GEMM_PIPE selects another: 3 or 4 (K step 16 with 3 or 4 stages), 332
+// (K step 32, 3 stages) or 0 (the register-staged kernel); read once per
+// process.
 int gemm_pipe_stages() {
   static const int s = [] {
     const char* e = getenv("NRGB_GEMM_PIPE");
-    if (!e || !*e) return 3;
+    if (!e || !*e) return 232;
     const int v = atoi(e);
-    return (v == 0 || v == 3 || v == 4) ? v : 3;
+    return (v == 0 || v == 3 || v == 4 || v == 232 || v == 332) ? v : 232;
   }();
   return s;
 }
 
-template <int S>
+template <int S, int KB>
 cudaError_t pipe_launch(const GemmProb* d_probs, int nprob, const GemmSeg* d_segs, int total_tiles,
                         cudaStream_t stream, const char* tag) {
   static std::atomic<bool> attr[64];
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !attr[dev].load(std::memory_order_acquire)) {
-    const cudaError_t e = cudaFuncSetAttribute(gemm_grouped_pipe_kernel<S>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<S>());
+    const cudaError_t e = cudaFuncSetAttribute(gemm_grouped_pipe_kernel<S, KB>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipe_smem<S, KB>());
     if (e != cudaSuccess) return e;
     if (dev < 64) attr[dev].store(true, std::memory_order_release);
   }
   NRGB_LAUNCH(tag, stream,
-              gemm_grouped_pipe_kernel<S><<<total_tiles, NT, pipe_smem<S>(), stream>>>(d_probs, nprob, d_segs));
+              gemm_grouped_pipe_kernel<S, KB><<<total_tiles, NT, pipe_smem<S, KB>(), stream>>>(d_probs, nprob, d_segs));
   return cudaGetLastError();
 }
 // The 128x128 cp.async variant is used only where the device's schedule
@@ -686,8 +697,10 @@ cudaError_t gemm_grouped_launch(const GemmProb* d_probs, int nprob, const GemmSe
     return cudaGetLastError();
   }
   const int stages = gemm_pipe_stages();
-  if (stages == 3) return pipe_launch<3>(d_probs, nprob, d_segs, total_tiles, stream, tag);
-  if (stages == 4) return pipe_launch<4>(d_probs, nprob, d_segs, total_tiles, stream, tag);
+  if (stages == 3) return pipe_launch<3, 16>(d_probs, nprob, d_segs, total_tiles, stream, tag);
+  if (stages == 4) return pipe_launch<4, 16>(d_probs, nprob, d_segs, total_tiles, stream, tag);
+  if (stages == 232) return pipe_launch<2, 32>(d_probs, nprob, d_segs, total_tiles, stream, tag);
+  if (stages == 332) return pipe_launch<3, 32>(d_probs, nprob, d_segs, total_tiles, stream, tag);
   NRGB_LAUNCH(tag, stream, gemm_grouped_kernel<<<total_tiles, NT, 0, stream>>>(d_probs, nprob, d_segs));
   return cudaGetLastError();
 }

@@ -97,11 +97,12 @@ def test_gemm_grouped_unaligned_views(ctx):
         assert err <= 1e-13 * (ref.abs().max().item() + 1.0) * 50
 
 
-@pytest.mark.parametrize("stages", ["0", "3", "4"])
+@pytest.mark.parametrize("stages", ["0", "3", "4", "232", "332"])
 def test_gemm_pipelined_variants(stages):
     """The grouped GEMM's register-staged kernel (NRGB_GEMM_PIPE=0) and its
-    cp.async-pipelined form with 3 or 4 stages (the switch is read once per
-    process, so each runs the GEMM tests in a child process)."""
+    cp.async-pipelined forms: K step 16 with 3 or 4 stages, K step 32 with 2
+    or 3 stages (232, 332).  The switch is read once per process, so each
+    form runs the GEMM tests in a child process."""
     import subprocess
     import sys
     env = dict(os.environ, NRGB_GEMM_PIPE=stages)
