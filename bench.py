@@ -803,7 +803,7 @@ def run_gemm_micro():
 
     forms = {"0": "register-staged", "3": "pipelined, K step 16, 3 stages", "4": "pipelined, K step 16, 4 stages",
              "232": "pipelined, K step 32, 2 stages", "332": "pipelined, K step 32, 3 stages"}
-    out = {"kernel": forms.get(os.environ.get("NRGB_GEMM_PIPE") or "232", "pipelined, K step 32, 2 stages")}
+    out = {"kernel": forms.get(os.environ.get("NRGB_GEMM_PIPE") or "3", "pipelined, K step 16, 3 stages")}
     for edge, nprob, nseg in ((2048, 4, 1), (1024, 16, 1), (512, 64, 1), (384, 64, 3), (256, 128, 2)):
         for ta, tb in ((0, 0), (1, 0), (0, 1), (1, 1)):
             A = [torch.randn(edge, edge, generator=g, device=dev, dtype=torch.float64) for _ in range(nprob * nseg)]

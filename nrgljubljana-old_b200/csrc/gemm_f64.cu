@@ -3,8 +3,8 @@
 //
 // Tile: 64x64 per CTA, 4 warps of 32x32, K staged 16 at a time through
 // shared memory laid out so that the DMMA fragment loads are bank-conflict
-// free: by default a cp.async ring of two K steps of 32
-// (gemm_grouped_pipe_kernel<2, 32>), else
+// free: by default a cp.async ring of three K steps of 16
+// (gemm_grouped_pipe_kernel<3, 16>), else
 // register-staged double buffering (gemm_grouped_kernel; also the kernel of
 // the allocation-free entry point) or 128x128 tiles where the schedule picks
 // them.  mma.sync.m8n8k4.f64 (the m16n8k4/k8/k16 f64 shapes run at the same
@@ -612,20 +612,23 @@ __global__ void __launch_bounds__(NT, 4) gemm_grouped_pipe_kernel(const GemmProb
 template <int S, int KB>
 constexpr size_t pipe_smem() { return 2 * (size_t)S * ptile<KB>() * sizeof(double); }
 
-// Form of the grouped GEMM: the pipelined kernel with K step 32 and 2 stages
-// by default (232; measured on B200 at 28.7-30.2 TF/s on grouped 2048^3
-// problems and 20.4-20.7 TF/s on 256^3 ones, against 28.0-29.2 and 20.5-20.9
-// with K step 16 and 3 stages, and 24.8-28.2 and 14.5-19.0 for the
-// register-staged kernel, over the four transpose combinations).
-// NRGB_GEMM_PIPE selects another: 3 or 4 (K step 16 with 3 or 4 stages), 332
-// (K step 32, 3 stages) or 0 (the register-staged kernel); read once per
-// process.
+// Form of the grouped GEMM: the pipelined kernel with K step 16 and 3 stages
+// by default (3).  Measured on B200: 28.0-29.2 TF/s on grouped 2048^3
+// problems and 20.5-20.9 TF/s on 256^3 ones, over the four transpose
+// combinations, against 24.8-28.2 and 14.5-19.0 TF/s for the register-staged
+// kernel; over the eigensolver's own launches of a 12-block step (trailing
+// updates, merges, back-transforms, basis changes) 4 % less GEMM time than
+// either the register-staged kernel or K step 32 with 2 stages.  That last
+// form (232) is 3 % faster on large square problems but up to 50 % slower on
+// launches with short K.  NRGB_GEMM_PIPE selects another form: 4 (K step 16,
+// 4 stages), 232, 332 (K step 32, 2 or 3 stages) or 0 (register-staged);
+// read once per process.
 int gemm_pipe_stages() {
   static const int s = [] {
     const char* e = getenv("NRGB_GEMM_PIPE");
-    if (!e || !*e) return 232;
+    if (!e || !*e) return 3;
     const int v = atoi(e);
-    return (v == 0 || v == 3 || v == 4 || v == 232 || v == 332) ? v : 232;
+    return (v == 0 || v == 3 || v == 4 || v == 232 || v == 332) ? v : 3;
   }();
   return s;
 }
