@@ -14,9 +14,10 @@ namespace {
 // diag tables of coefnew/qs/qs-<P>ch-*.dat): electrons per channel on the
 // added site, site spin, In = ancestor - subspace.
 struct ComboDef {
-  int occ[2];
+  int occ[3];
   double s;
   int dq, dss;
+  int label = 0;
 };
 const ComboDef COMBOS_1CH[] = {{{0, 0}, 0.0, 1, 0}, {{1, 0}, 0.5, 0, -1}, {{1, 0}, 0.5, 0, 1}, {{2, 0}, 0.0, -1, 0}};
 const ComboDef COMBOS_2CH[] = {{{0, 0}, 0.0, 2, 0},   {{0, 1}, 0.5, 1, -1},  {{0, 1}, 0.5, 1, 1},
@@ -25,6 +26,41 @@ const ComboDef COMBOS_2CH[] = {{{0, 0}, 0.0, 2, 0},   {{0, 1}, 0.5, 1, -1},  {{0
                                {{1, 1}, 1.0, 0, 0},   {{1, 1}, 1.0, 0, 2},   {{1, 2}, 0.5, -1, -1},
                                {{1, 2}, 0.5, -1, 1},  {{2, 1}, 0.5, -1, -1}, {{2, 1}, 0.5, -1, 1},
                                {{2, 2}, 0.0, -2, 0}};
+
+// Three channels (coefnew/qs/qs-3ch-In2.dat, QN, diag); label 1 marks the
+// second spin-1/2 multiplet with one electron per channel.
+const ComboDef COMBOS_3CH[] = {
+    {{0, 0, 0}, 0.0, 3, 0}, {{0, 0, 1}, 0.5, 2, -1}, {{0, 0, 1}, 0.5, 2, 1}, {{0, 1, 0}, 0.5, 2, -1},
+    {{0, 1, 0}, 0.5, 2, 1}, {{1, 0, 0}, 0.5, 2, -1}, {{1, 0, 0}, 0.5, 2, 1}, {{0, 0, 2}, 0.0, 1, 0},
+    {{0, 1, 1}, 0.0, 1, 0}, {{1, 0, 1}, 0.0, 1, 0}, {{0, 2, 0}, 0.0, 1, 0}, {{1, 1, 0}, 0.0, 1, 0},
+    {{2, 0, 0}, 0.0, 1, 0}, {{0, 1, 1}, 1.0, 1, -2}, {{0, 1, 1}, 1.0, 1, 0}, {{0, 1, 1}, 1.0, 1, 2},
+    {{1, 0, 1}, 1.0, 1, -2}, {{1, 0, 1}, 1.0, 1, 0}, {{1, 0, 1}, 1.0, 1, 2}, {{1, 1, 0}, 1.0, 1, -2},
+    {{1, 1, 0}, 1.0, 1, 0}, {{1, 1, 0}, 1.0, 1, 2}, {{0, 1, 2}, 0.5, 0, -1}, {{0, 1, 2}, 0.5, 0, 1},
+    {{1, 0, 2}, 0.5, 0, -1}, {{1, 0, 2}, 0.5, 0, 1}, {{0, 2, 1}, 0.5, 0, -1}, {{0, 2, 1}, 0.5, 0, 1},
+    {{1, 1, 1}, 0.5, 0, -1}, {{1, 1, 1}, 0.5, 0, 1}, {{2, 0, 1}, 0.5, 0, -1}, {{2, 0, 1}, 0.5, 0, 1},
+    {{1, 1, 1}, 0.5, 0, -1, 1}, {{1, 1, 1}, 0.5, 0, 1, 1}, {{1, 2, 0}, 0.5, 0, -1}, {{1, 2, 0}, 0.5, 0, 1},
+    {{2, 1, 0}, 0.5, 0, -1}, {{2, 1, 0}, 0.5, 0, 1}, {{1, 1, 1}, 1.5, 0, -3}, {{1, 1, 1}, 1.5, 0, -1},
+    {{1, 1, 1}, 1.5, 0, 1}, {{1, 1, 1}, 1.5, 0, 3}, {{0, 2, 2}, 0.0, -1, 0}, {{1, 1, 2}, 0.0, -1, 0},
+    {{2, 0, 2}, 0.0, -1, 0}, {{1, 2, 1}, 0.0, -1, 0}, {{2, 1, 1}, 0.0, -1, 0}, {{2, 2, 0}, 0.0, -1, 0},
+    {{1, 1, 2}, 1.0, -1, -2}, {{1, 1, 2}, 1.0, -1, 0}, {{1, 1, 2}, 1.0, -1, 2}, {{1, 2, 1}, 1.0, -1, -2},
+    {{1, 2, 1}, 1.0, -1, 0}, {{1, 2, 1}, 1.0, -1, 2}, {{2, 1, 1}, 1.0, -1, -2}, {{2, 1, 1}, 1.0, -1, 0},
+    {{2, 1, 1}, 1.0, -1, 2}, {{1, 2, 2}, 0.5, -2, -1}, {{1, 2, 2}, 0.5, -2, 1}, {{2, 1, 2}, 0.5, -2, -1},
+    {{2, 1, 2}, 0.5, -2, 1}, {{2, 2, 1}, 0.5, -2, -1}, {{2, 2, 1}, 0.5, -2, 1}, {{2, 2, 2}, 0.0, -3, 0},
+};
+
+// Three-channel site multiplets with the opposite phase: electrons per
+// channel, 2s, label.
+struct SignDef {
+  int occ[3];
+  int twos, label;
+};
+const SignDef NEGATIVE_3CH[] = {
+    {{0, 0, 2}, 0, 0}, {{0, 1, 1}, 2, 0}, {{0, 1, 2}, 1, 0}, {{0, 2, 0}, 0, 0},
+    {{0, 2, 1}, 1, 0}, {{1, 0, 1}, 2, 0}, {{1, 0, 2}, 1, 0}, {{1, 1, 0}, 2, 0},
+    {{1, 1, 1}, 1, 0}, {{1, 1, 1}, 1, 1}, {{1, 1, 1}, 3, 0}, {{1, 1, 2}, 0, 0},
+    {{1, 2, 0}, 1, 0}, {{1, 2, 1}, 0, 0}, {{2, 0, 0}, 0, 0}, {{2, 0, 1}, 1, 0},
+    {{2, 1, 0}, 1, 0}, {{2, 1, 1}, 0, 0}, {{2, 2, 2}, 0, 0},
+};
 
 // The same for SPSU2 (no charge: every In is (0, dss)), in the order of
 // coefnew/spsu2/spsu2-<P>ch-In2.dat: site singlets, doublets, the triplet.
@@ -37,9 +73,15 @@ const ComboDef SPSU2_2CH[] = {{{0, 0}, 0.0, 0, 0},  {{0, 2}, 0.0, 0, 0},  {{1, 1
 // Phase of each site multiplet relative to the highest-weight state whose
 // first nonzero amplitude (bit k = mode k = 2*channel + spin, up first) is
 // positive: the reference's conventions.
-double site_sign(int P, const std::vector<int>& occ, double s) {
+double site_sign(int P, const std::vector<int>& occ, double s, int label) {
   const int twos = (int)lround(2 * s);
   if (P == 1) return (occ[0] == 2) ? -1.0 : 1.0;
+  if (P == 3) {
+    for (const SignDef& d : NEGATIVE_3CH)
+      if (d.occ[0] == occ[0] && d.occ[1] == occ[1] && d.occ[2] == occ[2] && d.twos == twos && d.label == label)
+        return -1.0;
+    return 1.0;
+  }
   const int a = occ[0], b = occ[1];
   if ((a == 2 && b == 0) || (a == 0 && b == 2)) return -1.0;
   if (a == 1 && b == 1 && twos == 2) return -1.0;
@@ -71,14 +113,18 @@ double clebsch_gordan(double j1, double m1, double j2, double m2, double J, doub
 }
 
 QSCoupling::QSCoupling(int channels, bool spsu2) : P_(channels), spsu2_(spsu2) {
-  if (channels != 1 && channels != 2) throw std::runtime_error("QS symmetry: tables for 1 and 2 channels");
+  if (channels < 1 || channels > (spsu2 ? 2 : 3))
+    throw std::runtime_error(spsu2 ? "SPSU2 symmetry: tables for 1 and 2 channels"
+                                   : "QS symmetry: tables for 1, 2 and 3 channels");
   dim_ = 1 << (2 * P_);
-  const ComboDef* defs = spsu2 ? (P_ == 1 ? SPSU2_1CH : SPSU2_2CH) : (P_ == 1 ? COMBOS_1CH : COMBOS_2CH);
-  const int n = P_ == 1 ? 4 : 16;
+  const ComboDef* defs = spsu2 ? (P_ == 1 ? SPSU2_1CH : SPSU2_2CH)
+                               : (P_ == 1 ? COMBOS_1CH : P_ == 2 ? COMBOS_2CH : COMBOS_3CH);
+  const int n = 1 << (2 * P_);
   for (int i = 0; i < n; ++i) {
     Combo c;
     c.occ.assign(defs[i].occ, defs[i].occ + P_);
     c.s = defs[i].s;
+    c.label = defs[i].label;
     c.In = {defs[i].dq, defs[i].dss};
     combos_.push_back(c);
     in_.push_back(c.In);
@@ -94,11 +140,26 @@ QSCoupling::QSCoupling(int channels, bool spsu2) : P_(channels), spsu2_(spsu2) {
       if (!((b >> k) & 1)) M[(size_t)(b | (1 << k)) * dim_ + b] = (popcount(b & ((1u << k) - 1)) & 1) ? -1.0 : 1.0;
     cd_.push_back(M);
   }
+  // S+ = sum_ch c^dag_{ch up} c_{ch dn}
+  sp_.assign((size_t)dim_ * dim_, 0.0);
+  for (int ch = 0; ch < P_; ++ch) {
+    const Vec& up = cd_[2 * ch];
+    const Vec& dn = cd_[2 * ch + 1];
+    for (int r = 0; r < dim_; ++r)
+      for (int c = 0; c < dim_; ++c) {
+        double t = 0.0;
+        for (int k = 0; k < dim_; ++k) t += up[(size_t)r * dim_ + k] * dn[(size_t)c * dim_ + k];  // up * dn^T
+        sp_[(size_t)r * dim_ + c] += t;
+      }
+  }
   for (const Combo& c : combos_) {
-    int key = 0;
-    for (int ch = 0; ch < P_; ++ch) key = key * 3 + c.occ[ch];
-    const std::pair<int, int> k2{key, (int)lround(2 * c.s)};
-    if (!mult_.count(k2)) mult_[k2] = multiplet(c.occ, c.s, site_sign(P_, c.occ, c.s));
+    const std::pair<int, int> k2 = mult_key(c);
+    if (mult_.count(k2)) continue;
+    const double sign = site_sign(P_, c.occ, c.s, c.label);
+    if (P_ == 3 && c.occ == std::vector<int>{1, 1, 1} && c.twos() == 1)
+      mult_[k2] = coupled_doublet(c.label, sign);
+    else
+      mult_[k2] = multiplet(c.occ, c.s, sign);
   }
   // the site's pairing operator f^dag_up f^dag_dn + h.c. per channel (SPSU2)
   if (spsu2)
@@ -160,18 +221,7 @@ std::map<int, QSCoupling::Vec> QSCoupling::multiplet(const std::vector<int>& occ
   std::vector<int> idx;
   for (int b = 0; b < dim_; ++b)
     if (occ_ok(b) && sz2(b) == twos) idx.push_back(b);
-  // S+ = sum_ch c^dag_{ch up} c_{ch dn}
-  Vec Sp((size_t)dim_ * dim_, 0.0);
-  for (int ch = 0; ch < P_; ++ch) {
-    const Vec& up = cd_[2 * ch];
-    const Vec& dn = cd_[2 * ch + 1];
-    for (int r = 0; r < dim_; ++r)
-      for (int c = 0; c < dim_; ++c) {
-        double t = 0.0;
-        for (int k = 0; k < dim_; ++k) t += up[(size_t)r * dim_ + k] * dn[(size_t)c * dim_ + k];  // up * dn^T
-        Sp[(size_t)r * dim_ + c] += t;
-      }
-  }
+  const Vec& Sp = sp_;
   // null space of the columns idx of S+: orthonormal basis of the row space
   // (restricted to idx), then the first unit vector with a residual
   const int m = (int)idx.size();
@@ -230,13 +280,44 @@ std::map<int, QSCoupling::Vec> QSCoupling::multiplet(const std::vector<int>& occ
   return out;
 }
 
+// The three-channel spin-1/2 multiplet with one electron per channel whose
+// channels 0 and 1 couple to spin s01 = label (0 or 1):
+//   |1/2 1/2> = sum <s01 m01; 1/2 mc|1/2 1/2> c^dag_{2,mc} |s01 m01>,
+//   |s01 m01> = sum <1/2 ma; 1/2 mb|s01 m01> c^dag_{0,ma} c^dag_{1,mb} |0>,
+// normalised and multiplied by `sign`; then S- for M = -1/2.
+std::map<int, QSCoupling::Vec> QSCoupling::coupled_doublet(int label, double sign) const {
+  const double s01 = label;
+  Vec vac(dim_, 0.0);
+  vac[0] = 1.0;
+  auto cdag = [&](int ch, double m, const Vec& v) { return apply(cd_[2 * ch + (m > 0 ? 0 : 1)], v); };
+  Vec hw(dim_, 0.0);
+  for (double m01 = -s01; m01 <= s01 + 1e-9; m01 += 1.0) {
+    Vec pair(dim_, 0.0);
+    for (double ma : {0.5, -0.5}) {
+      const double g = clebsch_gordan(0.5, ma, 0.5, m01 - ma, s01, m01);
+      if (g == 0.0) continue;
+      const Vec v = cdag(0, ma, cdag(1, m01 - ma, vac));
+      for (int t = 0; t < dim_; ++t) pair[t] += g * v[t];
+    }
+    const double g = clebsch_gordan(s01, m01, 0.5, 0.5 - m01, 0.5, 0.5);
+    if (g == 0.0) continue;
+    const Vec v = cdag(2, 0.5 - m01, pair);
+    for (int t = 0; t < dim_; ++t) hw[t] += g * v[t];
+  }
+  double nrm = 0.0;
+  for (double x : hw) nrm += x * x;
+  for (double& x : hw) x *= sign / sqrt(nrm);
+  std::map<int, Vec> out;
+  out[1] = hw;
+  out[-1] = apply_t(sp_, hw);  // S- |1/2 1/2> = |1/2 -1/2>
+  return out;
+}
+
 bool QSCoupling::state(int i, double S, double M, State& out) const {
   const Combo& c = combos_[i];
   const double Sa = S + c.In.second / 2.0;
   if (Sa < -1e-9 || S < fabs(Sa - c.s) - 1e-9 || S > Sa + c.s + 1e-9) return false;
-  int key = 0;
-  for (int ch = 0; ch < P_; ++ch) key = key * 3 + c.occ[ch];
-  const auto& ms = mult_.at({key, (int)lround(2 * c.s)});
+  const auto& ms = mult_.at(mult_key(c));
   out.parts.clear();
   out.Sa = Sa;
   for (const auto& kv : ms) {
@@ -369,7 +450,7 @@ std::vector<RecalcRow> QSCoupling::chain_op(const Invar& I1, const Invar& Ip, do
   std::vector<RecalcRow> rows;
   for (int i1 = 0; i1 < combs(); ++i1)
     for (int ip = 0; ip < combs(); ++ip) {
-      if (combos_[i1].occ != combos_[ip].occ || combos_[i1].s != combos_[ip].s) continue;
+      if (mult_key(combos_[i1]) != mult_key(combos_[ip])) continue;
       if (anc(i1, I1).second < 1 || anc(ip, Ip).second < 1) continue;
       const double v = reduced(I1, Ip, rank, [&](double q, double S1, double Sp, double M2) {
         return elem(i1, S1, S1, ip, Sp, M2, rank, q, nullptr, false, odd);

@@ -1,4 +1,4 @@
-// QS coefficient tables derived from spin coupling, for 1 and 2 channels.
+// QS coefficient tables derived from spin coupling, for 1, 2 and 3 channels.
 //
 // The reference ships these tables as Mathematica output (coefnew/qs/
 // qs-<P>ch-*.dat, included by src/sym-QS.cc and src/nrg-recalc-QS.cc).
@@ -6,15 +6,19 @@
 //   * a subspace I = (Q, SS) of step N+1 is spanned, for each combination i,
 //     by  sum_{m_a, m_s} <S_a m_a; s_i m_s | S M> |site_i m_s> |anc_i m_a>,
 //     anc_i = I + In[i] a subspace of step N and site_i a spin multiplet of
-//     the added site with fixed electron numbers per channel;
+//     the added site with fixed electron numbers per channel (three channels
+//     have two spin-1/2 multiplets with one electron per channel, told apart
+//     by the spin to which channels 0 and 1 couple);
 //   * the added site's fermion operators stand to the left of the chain's,
 //     so an odd chain operator picks up (-1)^(electrons on the site);
 //   * chain operators enter through reduced matrix elements in the
 //     Wigner-Eckart normalisation <S1 M1|T^k_q|S2 M2> = <S2 M2; k q|S1 M1> R.
-// Every entry is a matrix element in the site's Fock space (4 or 16 states)
+// Every entry is a matrix element in the site's Fock space (4, 16 or 64 states)
 // divided by the Clebsch-Gordan coefficient of the Wigner-Eckart theorem.
 // The phases of the site multiplets are the reference's conventions.
 #pragma once
+#include <math.h>
+
 #include <map>
 #include <vector>
 
@@ -54,6 +58,8 @@ class QSCoupling {
     std::vector<int> occ;  // electrons per channel on the site
     double s;              // site spin
     Invar In;              // ancestor = I + In
+    int label = 0;         // which of equal (occ, s) multiplets
+    int twos() const { return (int)lround(2 * s); }
   };
   using Vec = std::vector<double>;
   // |state> = sum over 2 m_a of (site vector) |anc m_a>
@@ -67,13 +73,20 @@ class QSCoupling {
   std::vector<Combo> combos_;
   std::vector<Invar> in_, qn_;
   std::vector<Vec> cd_;                 // creation operators, dim x dim, row-major
-  std::map<std::pair<int, int>, std::map<int, Vec>> mult_;  // (occupations, 2s) -> 2M -> state
+  Vec sp_;                              // total S+ of the site
+  std::map<std::pair<int, int>, std::map<int, Vec>> mult_;  // (occupations and label, 2s) -> 2M -> state
   std::map<int, std::vector<OffdiagTerm>> off_;
   std::map<Invar, std::vector<RecalcTable>> rf_, dbl_, trp_;
 
   Vec apply(const Vec& op, const Vec& v) const;
   Vec apply_t(const Vec& op, const Vec& v) const;  // transpose
   std::map<int, Vec> multiplet(const std::vector<int>& occ, double s, double sign) const;
+  std::map<int, Vec> coupled_doublet(int label, double sign) const;
+  std::pair<int, int> mult_key(const Combo& c) const {
+    int key = 0;
+    for (int ch = 0; ch < P_; ++ch) key = key * 3 + c.occ[ch];
+    return {key * 2 + c.label, c.twos()};
+  }
   bool state(int i, double S, double M, State& out) const;
   Invar anc(int i, const Invar& I) const { return {I.first + combos_[i].In.first, I.second + combos_[i].In.second}; }
   int nsite(int i) const;

@@ -72,13 +72,13 @@ class Symmetry {
 class SymmetryQS : public Symmetry {
  public:
   explicit SymmetryQS(int channels) : nch_(channels) {
-    if (channels == 2) {
-      cpl_.reset(new QSCoupling(2));
+    if (channels == 2 || channels == 3) {
+      cpl_.reset(new QSCoupling(channels));
       in_ = cpl_->In();
       qn_ = cpl_->QN();
       return;
     }
-    if (channels != 1) throw std::runtime_error("QS symmetry: this build provides the 1- and 2-channel tables");
+    if (channels != 1) throw std::runtime_error("QS symmetry: this build provides the 1-, 2- and 3-channel tables");
     in_ = {{1, 0}, {0, -1}, {0, 1}, {-1, 0}};
     qn_ = {{-1, 1}, {0, 2}, {0, 2}, {1, 1}};
   }

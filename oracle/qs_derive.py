@@ -1,5 +1,5 @@
 """QS coefficient tables derived from spin coupling (the oracle's restatement
-of coefnew/qs/qs-<P>ch-*.dat for P = 1, 2 channels).
+of coefnew/qs/qs-<P>ch-*.dat for P = 1, 2, 3 channels).
 
 Test infrastructure: part of the CPU checker for the CUDA path, imported only
 by tests, smoke() and the bench's CPU baseline.
@@ -19,7 +19,7 @@ computed from their definition instead:
   Wigner-Eckart normalisation  <S1 M1|T^k_q|S2 M2> = <S2 M2; k q|S1 M1> <S1||T||S2>.
 
 Each table entry is then a matrix element computed numerically in the
-16-state (two channels) or 4-state (one channel) Fock space of the site,
+64-, 16- or 4-state Fock space of the site (three, two or one channels),
 divided by the Clebsch-Gordan coefficient of the Wigner-Eckart theorem.  The
 phases of the site multiplets are conventions; SITE_SIGNS fixes them to the
 reference's.  tests/test_qs_tables.py checks every entry against the
@@ -33,22 +33,66 @@ import math
 import numpy as np
 
 # Combinations of a new subspace (1-based index = position + 1):
-# (electrons per channel on the site, site spin, In = ancestor - subspace)
+# (electrons per channel on the site, site spin, In = ancestor - subspace[,
+# label]).  With three channels the site has two spin-1/2 multiplets with one
+# electron in each channel: label 0 couples channels 0 and 1 to spin 0, label
+# 1 to spin 1, and either with channel 2 to spin 1/2 (the reference's basis;
+# its tables of coefnew/qs/qs-3ch-*.dat fix it).
 COMBOS = {
     1: [((0,), 0.0, (1, 0)), ((1,), 0.5, (0, -1)), ((1,), 0.5, (0, 1)), ((2,), 0.0, (-1, 0))],
     2: [((0, 0), 0.0, (2, 0)), ((0, 1), 0.5, (1, -1)), ((0, 1), 0.5, (1, 1)), ((1, 0), 0.5, (1, -1)),
         ((1, 0), 0.5, (1, 1)), ((0, 2), 0.0, (0, 0)), ((1, 1), 0.0, (0, 0)), ((2, 0), 0.0, (0, 0)),
         ((1, 1), 1.0, (0, -2)), ((1, 1), 1.0, (0, 0)), ((1, 1), 1.0, (0, 2)), ((1, 2), 0.5, (-1, -1)),
         ((1, 2), 0.5, (-1, 1)), ((2, 1), 0.5, (-1, -1)), ((2, 1), 0.5, (-1, 1)), ((2, 2), 0.0, (-2, 0))],
+    3: [
+        ((0, 0, 0), 0.0, (3, 0)), ((0, 0, 1), 0.5, (2, -1)), ((0, 0, 1), 0.5, (2, 1)),
+        ((0, 1, 0), 0.5, (2, -1)), ((0, 1, 0), 0.5, (2, 1)), ((1, 0, 0), 0.5, (2, -1)),
+        ((1, 0, 0), 0.5, (2, 1)), ((0, 0, 2), 0.0, (1, 0)), ((0, 1, 1), 0.0, (1, 0)),
+        ((1, 0, 1), 0.0, (1, 0)), ((0, 2, 0), 0.0, (1, 0)), ((1, 1, 0), 0.0, (1, 0)),
+        ((2, 0, 0), 0.0, (1, 0)), ((0, 1, 1), 1.0, (1, -2)), ((0, 1, 1), 1.0, (1, 0)),
+        ((0, 1, 1), 1.0, (1, 2)), ((1, 0, 1), 1.0, (1, -2)), ((1, 0, 1), 1.0, (1, 0)),
+        ((1, 0, 1), 1.0, (1, 2)), ((1, 1, 0), 1.0, (1, -2)), ((1, 1, 0), 1.0, (1, 0)),
+        ((1, 1, 0), 1.0, (1, 2)), ((0, 1, 2), 0.5, (0, -1)), ((0, 1, 2), 0.5, (0, 1)),
+        ((1, 0, 2), 0.5, (0, -1)), ((1, 0, 2), 0.5, (0, 1)), ((0, 2, 1), 0.5, (0, -1)),
+        ((0, 2, 1), 0.5, (0, 1)), ((1, 1, 1), 0.5, (0, -1)), ((1, 1, 1), 0.5, (0, 1)),
+        ((2, 0, 1), 0.5, (0, -1)), ((2, 0, 1), 0.5, (0, 1)), ((1, 1, 1), 0.5, (0, -1), 1),
+        ((1, 1, 1), 0.5, (0, 1), 1), ((1, 2, 0), 0.5, (0, -1)), ((1, 2, 0), 0.5, (0, 1)),
+        ((2, 1, 0), 0.5, (0, -1)), ((2, 1, 0), 0.5, (0, 1)), ((1, 1, 1), 1.5, (0, -3)),
+        ((1, 1, 1), 1.5, (0, -1)), ((1, 1, 1), 1.5, (0, 1)), ((1, 1, 1), 1.5, (0, 3)),
+        ((0, 2, 2), 0.0, (-1, 0)), ((1, 1, 2), 0.0, (-1, 0)), ((2, 0, 2), 0.0, (-1, 0)),
+        ((1, 2, 1), 0.0, (-1, 0)), ((2, 1, 1), 0.0, (-1, 0)), ((2, 2, 0), 0.0, (-1, 0)),
+        ((1, 1, 2), 1.0, (-1, -2)), ((1, 1, 2), 1.0, (-1, 0)), ((1, 1, 2), 1.0, (-1, 2)),
+        ((1, 2, 1), 1.0, (-1, -2)), ((1, 2, 1), 1.0, (-1, 0)), ((1, 2, 1), 1.0, (-1, 2)),
+        ((2, 1, 1), 1.0, (-1, -2)), ((2, 1, 1), 1.0, (-1, 0)), ((2, 1, 1), 1.0, (-1, 2)),
+        ((1, 2, 2), 0.5, (-2, -1)), ((1, 2, 2), 0.5, (-2, 1)), ((2, 1, 2), 0.5, (-2, -1)),
+        ((2, 1, 2), 0.5, (-2, 1)), ((2, 2, 1), 0.5, (-2, -1)), ((2, 2, 1), 0.5, (-2, 1)),
+        ((2, 2, 2), 0.0, (-3, 0)),
+    ],
 }
 
 # Sign of each site multiplet relative to the highest-weight state whose first
 # nonzero amplitude (occupation bit order: channel-major, spin up first) is
-# positive, with c^dag operators applied in increasing mode order.
+# positive, with c^dag operators applied in increasing mode order; for the two
+# coupled doublets of three channels, relative to the coupled state
+# sum <S01 m01; 1/2 mc|1/2 1/2> c^dag_{2,mc} |S01 m01> with
+# |S01 m01> = sum <1/2 ma; 1/2 mb|S01 m01> c^dag_{0,ma} c^dag_{1,mb} |0>.
+# Three-channel keys carry the label.
 SITE_SIGNS = {
     1: {((2,), 0.0): -1.0},
     2: {((2, 0), 0.0): -1.0, ((0, 2), 0.0): -1.0, ((1, 1), 1.0): -1.0, ((1, 2), 0.5): -1.0,
         ((2, 1), 0.5): -1.0},
+    3: {
+        ((0, 0, 2), 0.0, 0): -1.0, ((0, 1, 1), 1.0, 0): -1.0,
+        ((0, 1, 2), 0.5, 0): -1.0, ((0, 2, 0), 0.0, 0): -1.0,
+        ((0, 2, 1), 0.5, 0): -1.0, ((1, 0, 1), 1.0, 0): -1.0,
+        ((1, 0, 2), 0.5, 0): -1.0, ((1, 1, 0), 1.0, 0): -1.0,
+        ((1, 1, 1), 0.5, 0): -1.0, ((1, 1, 1), 0.5, 1): -1.0,
+        ((1, 1, 1), 1.5, 0): -1.0, ((1, 1, 2), 0.0, 0): -1.0,
+        ((1, 2, 0), 0.5, 0): -1.0, ((1, 2, 1), 0.0, 0): -1.0,
+        ((2, 0, 0), 0.0, 0): -1.0, ((2, 0, 1), 0.5, 0): -1.0,
+        ((2, 1, 0), 0.5, 0): -1.0, ((2, 1, 1), 0.0, 0): -1.0,
+        ((2, 2, 2), 0.0, 0): -1.0,
+    },
 }
 
 
@@ -115,20 +159,52 @@ class _Site:
             out[m] = v
         return out
 
+    def coupled_doublet(self, s01, sign):
+        """{M: state} of the three-channel spin-1/2 multiplet with one electron
+        per channel whose channels 0 and 1 couple to spin s01."""
+        vac = np.zeros(self.dim)
+        vac[0] = 1.0
+
+        def cdag(ch, m):
+            return self.cd[2 * ch + (0 if m > 0 else 1)]
+        hw = np.zeros(self.dim)
+        for m01 in np.arange(-s01, s01 + 0.5, 1.0):
+            pair = np.zeros(self.dim)
+            for ma in (0.5, -0.5):
+                c = cg(0.5, ma, 0.5, m01 - ma, s01, m01)
+                if c:
+                    pair += c * (cdag(0, ma) @ cdag(1, m01 - ma) @ vac)
+            g = cg(s01, m01, 0.5, 0.5 - m01, 0.5, 0.5)
+            if g:
+                hw += g * (cdag(2, 0.5 - m01) @ pair)
+        hw = hw / np.linalg.norm(hw) * sign
+        return {0.5: hw, -0.5: self.Sp.T @ hw}
+
+
+def _key(c):
+    """Site multiplet of a combination: (occupations, spin, label)."""
+    return (c[0], c[1], c[3] if len(c) > 3 else 0)
+
 
 class Tables:
     """All QS tables for P channels."""
 
     def __init__(self, P):
         if P not in COMBOS:
-            raise NotImplementedError("QS tables are derived for 1 and 2 channels")
+            raise NotImplementedError("QS tables are derived for 1, 2 and 3 channels")
         self.P = P
         self.combos = COMBOS[P]
         self.site = _Site(P)
         self.mult = {}
-        for occ, s, _ in self.combos:
-            if (occ, s) not in self.mult:
-                self.mult[(occ, s)] = self.site.multiplet(occ, s, SITE_SIGNS[P].get((occ, s), 1.0))
+        for c in self.combos:
+            k = _key(c)
+            if k in self.mult:
+                continue
+            sign = SITE_SIGNS[P].get(k if P == 3 else k[:2], 1.0)
+            if P == 3 and c[0] == (1, 1, 1) and c[1] == 0.5:
+                self.mult[k] = self.site.coupled_doublet(float(k[2]), sign)
+            else:
+                self.mult[k] = self.site.multiplet(c[0], c[1], sign)
 
     # ---- helpers ----
     def anc(self, i, I):
@@ -139,12 +215,12 @@ class Tables:
         return sum(self.combos[i][0])
 
     def _state(self, i, S, M):
-        occ, s, In = self.combos[i]
+        s, In = self.combos[i][1], self.combos[i][2]
         Sa = S + In[1] / 2.0
         if Sa < -1e-9 or not (abs(Sa - s) - 1e-9 <= S <= Sa + s + 1e-9):
             return None
         out = {}
-        for ms, vec in self.mult[(occ, s)].items():
+        for ms, vec in self.mult[_key(self.combos[i])].items():
             ma = M - ms
             if abs(ma) > Sa + 1e-9:
                 continue
@@ -232,7 +308,7 @@ class Tables:
         rows = []
         for i1 in range(len(self.combos)):
             for ip in range(len(self.combos)):
-                if self.combos[i1][:2] != self.combos[ip][:2]:
+                if _key(self.combos[i1]) != _key(self.combos[ip]):
                     continue
                 if self.anc(i1, I1)[1] < 1 or self.anc(ip, Ip)[1] < 1:
                     continue

@@ -1,5 +1,6 @@
-"""Generate tests/golden/qs_tables.json and qs_tables_2ch.json from the
-reference's QS coefficient tables (coefnew/qs/qs-1ch-*.dat, qs-2ch-*.dat),
+"""Generate tests/golden/qs_tables.json, qs_tables_2ch.json and
+qs_tables_3ch.json from the reference's QS coefficient tables
+(coefnew/qs/qs-1ch-*.dat, qs-2ch-*.dat, qs-3ch-*.dat),
 evaluated numerically for a range of spin multiplicities.  Run in a container that has the reference checkout:
 
     python tests/golden/make_qs_tables.py /root/reference
@@ -22,6 +23,7 @@ FILES = ["offdiag", "diag", "spinupa", "spindowna", "doubletp", "doubletm",
 def _ns(**kw):
     ns = {"sqrt": lambda x: math.sqrt(x) if x >= 0 else float("nan"),
           "Power": lambda a, b: a ** b,
+          "pow": lambda a, b: a ** b,
           "S": lambda ss: (ss - 1) / 2.0,
           "Invar": lambda *a: tuple(a)}
     ns.update(kw)
@@ -58,11 +60,13 @@ def _split_args(s):
 
 FILES_2CH = ["offdiag", "diag", "spinupa", "spinupb", "spindowna", "spindownb", "doubletp", "doubletm",
              "triplets", "tripletp", "tripletm", "In2", "QN"]
+FILES_3CH = ["offdiag", "diag", "spinupa", "spinupb", "spinupc", "spindowna", "spindownb", "spindownc",
+             "doubletp", "doubletm", "triplets", "tripletp", "tripletm", "In2", "QN"]
 
 
-def main(refroot, out, channels=1, files=FILES, indent=1):
+def main(refroot, out, channels=1, files=FILES, indent=1, ss_max=40):
     base = os.path.join(refroot, "coefnew", "qs")
-    result = {"ss_range": [1, 40], "tables": {}}
+    result = {"ss_range": [1, ss_max], "tables": {}}
     for name in files:
         path = os.path.join(base, "qs-%dch-%s.dat" % (channels, name))
         rows = []
@@ -77,7 +81,7 @@ def main(refroot, out, channels=1, files=FILES, indent=1):
                     continue
                 if name == "offdiag":
                     args = _split_args(line[line.index("(") + 1:line.rindex(")")])
-                    vals = {ss: _eval(args[3], ss=ss) for ss in range(1, 41)}
+                    vals = {ss: _eval(args[3], ss=ss) for ss in range(1, ss_max + 1)}
                     rows.append({"i": int(args[0]), "j": int(args[1]), "ch": int(args[2]), "factor": vals})
                     continue
                 if name == "diag":
@@ -86,10 +90,10 @@ def main(refroot, out, channels=1, files=FILES, indent=1):
                     continue
                 args = _split_args(line[line.index("{") + 1:line.rindex("}")])
                 if name.startswith("spinup") or name.startswith("spindown"):
-                    vals = {ss: _eval(args[2], ssp=ss) for ss in range(1, 41)}
+                    vals = {ss: _eval(args[2], ssp=ss) for ss in range(1, ss_max + 1)}
                     rows.append({"i1": int(args[0]), "ip": int(args[1]), "factor": vals})
                 else:
-                    vals = {ss: _eval(args[4], ss1=ss, q1=0) for ss in range(1, 41)}
+                    vals = {ss: _eval(args[4], ss1=ss, q1=0) for ss in range(1, ss_max + 1)}
                     in1 = _eval(args[2], ss1=10, q1=0)
                     inp = _eval(args[3], ss1=10, q1=0)
                     rows.append({"i1": int(args[0]), "ip": int(args[1]),
@@ -105,3 +109,4 @@ if __name__ == "__main__":
     here = os.path.dirname(os.path.abspath(__file__))
     main(ref, os.path.join(here, "qs_tables.json"))
     main(ref, os.path.join(here, "qs_tables_2ch.json"), channels=2, files=FILES_2CH, indent=None)
+    main(ref, os.path.join(here, "qs_tables_3ch.json"), channels=3, files=FILES_3CH, indent=None, ss_max=14)

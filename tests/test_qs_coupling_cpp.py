@@ -2,7 +2,7 @@
 the GPU path) agrees entry by entry with the oracle's Python derivation
 (oracle/qs_derive.py), which tests/test_qs_tables*.py check against the
 reference's tables: diagonal and off-diagonal Hamiltonian terms, <f>
-recalculation, doublet and triplet operator tables, 1 and 2 channels.
+recalculation, doublet and triplet operator tables, 1, 2 and 3 channels.
 
 tests/qs_coupling_dump.cc prints the C++ tables; it is compiled here with
 the host compiler (no device needed)."""
@@ -45,7 +45,7 @@ def _same(cpp, py):
     return len(a)
 
 
-@pytest.mark.parametrize("P", [1, 2])
+@pytest.mark.parametrize("P", [1, 2, 3])
 def test_cpp_tables_match_python_derivation(dump, P):
     n = 0
     for rec in dump(P):
@@ -66,4 +66,4 @@ def test_cpp_tables_match_python_derivation(dump, P):
                 py = {(tuple(Ip), 0, i1, ip): v for Ip, rows in fn(P, I) for i1, ip, v in rows}
                 cpp = {(k[0], 0, k[2], k[3]): v for k, v in cpp.items()}
             n += _same(cpp, py)
-    assert n > (300 if P == 1 else 3000)
+    assert n > {1: 300, 2: 3000, 3: 15000}[P]

@@ -260,3 +260,54 @@ def test_qsz_three_channels_symmetric_spectra(tmp_path):
                 dz = dict(zip(z[:, 0], z[:, 1]))
                 err = max(abs(dr.get(k, 0.0) - dz.get(k, 0.0)) for k in set(dr) | set(dz))
                 assert err <= 1e-8 * wmax, (typ, ch, spin, err / wmax)
+
+
+def test_qs_three_channels_matches_qsz(tmp_path):
+    """Three-channel Kondo model with unequal couplings in QS (tables derived
+    by spin coupling, host/qs_coupling.cc) and in QSZ (Fock-state
+    combinations, pinned above to exact diagonalisation): under an energy
+    cutoff both keep the same states, so the shared thermodynamic columns
+    agree, every QS multiplet appears with its SS spin projections in QSZ,
+    and the f spectral function of every channel (a doublet operator, whose
+    recalculation runs through the doublet tables) equals each QSZ spin
+    component."""
+    import nrgb
+    params = {"keep": 100000, "keepenergy": 3.0, "keepmin": 1, "T": 1e-3, "fdm": True, "dmnrg": True,
+              "specd": "A_f0-A_f0 A_f1-A_f1 A_f2-A_f2", "bins": 30, "savebins": True, "broaden": False,
+              "dumpannotated": 100000, "dumpgroups": False, "prec_td": 16, "dumpprecision": 16}
+    out = {}
+    ctx = nrgb.Context(0)
+    try:
+        for sym in ("QS", "QSZ"):
+            wd = str(tmp_path / ("in" + sym))
+            inputgen.make_kondo(wd, [0.3, 0.2, 0.1], 3.0, 5, symtype=sym, params=dict(params))
+            od = str(tmp_path / ("out" + sym))
+            os.makedirs(od)
+            ctx.run(wd, od)
+            out[sym] = od
+    finally:
+        ctx.close()
+    tq = cases.read_table(os.path.join(out["QS"], "td"))
+    tz = cases.read_table(os.path.join(out["QSZ"], "td"))
+    assert tq.shape[0] == tz.shape[0]
+    shared_z = tz[:, [0, 1, 3, 4, 5, 6, 7, 8, 9]]
+    assert np.all(np.abs(shared_z - tq) <= 1e-8 * np.abs(tq) + 1e-11), float(np.max(np.abs(shared_z - tq)))
+    aq = cases.read_annotated(os.path.join(out["QS"], "annotated.dat"))
+    az = cases.read_annotated(os.path.join(out["QSZ"], "annotated.dat"))
+    assert len(aq) == len(az)
+    for sq, sz in zip(aq, az):
+        eq = np.sort(np.concatenate([[e] * int(lab[0].split()[1]) for e, lab, _ in sq]))
+        ez = np.sort(np.array([e for e, _, _ in sz]))
+        assert eq.shape == ez.shape
+        assert np.max(np.abs(eq - ez)) <= 1e-9 * max(1.0, np.max(np.abs(eq)))
+    for ch in range(3):
+        for typ in ("DMNRG", "FDM"):
+            q = cases.read_bins(os.path.join(out["QS"], "spec_%s_dens_A_f%d-A_f%d.bin" % (typ, ch, ch)))
+            dq = dict(zip(q[:, 0], q[:, 1]))
+            wmax = max(abs(v) for v in dq.values())
+            assert wmax > 0
+            for spin in ("u", "d"):
+                z = cases.read_bins(os.path.join(out["QSZ"], "spec_%s_dens_A_f%d-A_f%d-%s.bin" % (typ, ch, ch, spin)))
+                dz = dict(zip(z[:, 0], z[:, 1]))
+                err = max(abs(dq.get(k, 0.0) - dz.get(k, 0.0)) for k in set(dq) | set(dz))
+                assert err <= 1e-8 * wmax, (ch, typ, spin, err / wmax)
