@@ -70,9 +70,10 @@ class Tables(qd.Tables):
         self.combos = COMBOS[P]
         self.site = qd._Site(P)
         self.mult = {}
-        for occ, s, _ in self.combos:
-            if (occ, s) not in self.mult:
-                self.mult[(occ, s)] = self.site.multiplet(occ, s, SITE_SIGNS[P].get((occ, s), 1.0))
+        for c in self.combos:
+            k = qd._key(c)
+            if k not in self.mult:
+                self.mult[k] = self.site.multiplet(c[0], c[1], SITE_SIGNS[P].get(k[:2], 1.0))
 
     def _pairs(self, ss, site_ops):
         """Ordered pairs (i, j) and channels with sum over (c, op, q) of
