@@ -1593,7 +1593,7 @@ struct NrgDriver::Impl {
         throw std::runtime_error("symmetry type QSZ: only the spectral functions of doublet operators are built");
       sym.reset(new SymmetryQSZ(D.channels));
     } else if (D.symtype == "SPSU2") {
-      if (D.channels != 1 && D.channels != 2) throw std::runtime_error("symmetry type SPSU2: 1 and 2 channels are built");
+      if (D.channels < 1 || D.channels > 3) throw std::runtime_error("symmetry type SPSU2: 1 to 3 channels are built");
       sym.reset(new SymmetrySPSU2(D.channels));
     } else {
       throw std::runtime_error("symmetry type " + D.symtype + " is not built (QS, QSZ, SPSU2)");

@@ -70,6 +70,28 @@ const ComboDef SPSU2_2CH[] = {{{0, 0}, 0.0, 0, 0},  {{0, 2}, 0.0, 0, 0},  {{1, 1
                               {{1, 0}, 0.5, 0, 1},  {{1, 2}, 0.5, 0, -1}, {{1, 2}, 0.5, 0, 1},  {{2, 1}, 0.5, 0, -1},
                               {{2, 1}, 0.5, 0, 1},  {{1, 1}, 1.0, 0, -2}, {{1, 1}, 1.0, 0, 0},  {{1, 1}, 1.0, 0, 2}};
 
+// Three channels: site singlets, doublets, quartet in the order of
+// coefnew/spsu2/spsu2-3ch-In2.dat, QN and diag; label 1 marks the second
+// spin-1/2 multiplet with one electron per channel.
+const ComboDef SPSU2_3CH[] = {
+    {{0, 0, 0}, 0.0, 0, 0}, {{0, 0, 2}, 0.0, 0, 0}, {{0, 1, 1}, 0.0, 0, 0}, {{1, 0, 1}, 0.0, 0, 0},
+    {{0, 2, 0}, 0.0, 0, 0}, {{1, 1, 0}, 0.0, 0, 0}, {{2, 0, 0}, 0.0, 0, 0}, {{0, 2, 2}, 0.0, 0, 0},
+    {{1, 1, 2}, 0.0, 0, 0}, {{2, 0, 2}, 0.0, 0, 0}, {{1, 2, 1}, 0.0, 0, 0}, {{2, 1, 1}, 0.0, 0, 0},
+    {{2, 2, 0}, 0.0, 0, 0}, {{2, 2, 2}, 0.0, 0, 0}, {{0, 0, 1}, 0.5, 0, -1}, {{0, 0, 1}, 0.5, 0, 1},
+    {{0, 1, 0}, 0.5, 0, -1}, {{0, 1, 0}, 0.5, 0, 1}, {{1, 0, 0}, 0.5, 0, -1}, {{1, 0, 0}, 0.5, 0, 1},
+    {{0, 1, 2}, 0.5, 0, -1}, {{0, 1, 2}, 0.5, 0, 1}, {{1, 0, 2}, 0.5, 0, -1}, {{1, 0, 2}, 0.5, 0, 1},
+    {{0, 2, 1}, 0.5, 0, -1}, {{0, 2, 1}, 0.5, 0, 1}, {{1, 1, 1}, 0.5, 0, -1}, {{1, 1, 1}, 0.5, 0, 1},
+    {{2, 0, 1}, 0.5, 0, -1}, {{2, 0, 1}, 0.5, 0, 1}, {{1, 1, 1}, 0.5, 0, -1, 1}, {{1, 1, 1}, 0.5, 0, 1, 1},
+    {{1, 2, 0}, 0.5, 0, -1}, {{1, 2, 0}, 0.5, 0, 1}, {{2, 1, 0}, 0.5, 0, -1}, {{2, 1, 0}, 0.5, 0, 1},
+    {{1, 2, 2}, 0.5, 0, -1}, {{1, 2, 2}, 0.5, 0, 1}, {{2, 1, 2}, 0.5, 0, -1}, {{2, 1, 2}, 0.5, 0, 1},
+    {{2, 2, 1}, 0.5, 0, -1}, {{2, 2, 1}, 0.5, 0, 1}, {{0, 1, 1}, 1.0, 0, -2}, {{0, 1, 1}, 1.0, 0, 0},
+    {{0, 1, 1}, 1.0, 0, 2}, {{1, 0, 1}, 1.0, 0, -2}, {{1, 0, 1}, 1.0, 0, 0}, {{1, 0, 1}, 1.0, 0, 2},
+    {{1, 1, 0}, 1.0, 0, -2}, {{1, 1, 0}, 1.0, 0, 0}, {{1, 1, 0}, 1.0, 0, 2}, {{1, 1, 2}, 1.0, 0, -2},
+    {{1, 1, 2}, 1.0, 0, 0}, {{1, 1, 2}, 1.0, 0, 2}, {{1, 2, 1}, 1.0, 0, -2}, {{1, 2, 1}, 1.0, 0, 0},
+    {{1, 2, 1}, 1.0, 0, 2}, {{2, 1, 1}, 1.0, 0, -2}, {{2, 1, 1}, 1.0, 0, 0}, {{2, 1, 1}, 1.0, 0, 2},
+    {{1, 1, 1}, 1.5, 0, -3}, {{1, 1, 1}, 1.5, 0, -1}, {{1, 1, 1}, 1.5, 0, 1}, {{1, 1, 1}, 1.5, 0, 3},
+};
+
 // Phase of each site multiplet relative to the highest-weight state whose
 // first nonzero amplitude (bit k = mode k = 2*channel + spin, up first) is
 // positive: the reference's conventions.
@@ -113,11 +135,11 @@ double clebsch_gordan(double j1, double m1, double j2, double m2, double J, doub
 }
 
 QSCoupling::QSCoupling(int channels, bool spsu2) : P_(channels), spsu2_(spsu2) {
-  if (channels < 1 || channels > (spsu2 ? 2 : 3))
-    throw std::runtime_error(spsu2 ? "SPSU2 symmetry: tables for 1 and 2 channels"
+  if (channels < 1 || channels > 3)
+    throw std::runtime_error(spsu2 ? "SPSU2 symmetry: tables for 1, 2 and 3 channels"
                                    : "QS symmetry: tables for 1, 2 and 3 channels");
   dim_ = 1 << (2 * P_);
-  const ComboDef* defs = spsu2 ? (P_ == 1 ? SPSU2_1CH : SPSU2_2CH)
+  const ComboDef* defs = spsu2 ? (P_ == 1 ? SPSU2_1CH : P_ == 2 ? SPSU2_2CH : SPSU2_3CH)
                                : (P_ == 1 ? COMBOS_1CH : P_ == 2 ? COMBOS_2CH : COMBOS_3CH);
   const int n = 1 << (2 * P_);
   for (int i = 0; i < n; ++i) {
@@ -407,16 +429,16 @@ const std::vector<OffdiagTerm>& QSCoupling::offdiag(int ss) {
         }
       }
     // on-site pairing between combinations of one ancestor, in units of
-    // 2 delta; the reference writes the pairing of every channel after the
-    // first with the opposite sign along the chain and its tables with the
-    // opposite sign to match (initial.m, bcsgap section).  The element does
-    // not depend on the subspace; it is taken at S = 2.
+    // 2 delta; the reference writes the pairing of the odd channels with the
+    // opposite sign along the chain and its tables with the opposite sign to
+    // match (initial.m, bcsgap section).  The element does not depend on the
+    // subspace; it is taken at S = 2.
     for (int ch = 0; ch < P_; ++ch)
       for (int i = 0; i < n; ++i)
         for (int j = i + 1; j < n; ++j) {
           if (combos_[i].In != combos_[j].In) continue;
           const double v = elem(i, 2.0, 2.0, j, 2.0, 2.0, -1.0, 0.0, &pair_[ch], false, false);
-          if (fabs(v) > 1e-13) out.push_back({i + 1, j + 1, ch, (ch == 0 ? 0.5 : -0.5) * v, 2});
+          if (fabs(v) > 1e-13) out.push_back({i + 1, j + 1, ch, (ch % 2 == 0 ? 0.5 : -0.5) * v, 2});
         }
   }
   return off_[ss] = out;

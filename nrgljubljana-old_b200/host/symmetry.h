@@ -213,17 +213,18 @@ class SymmetryQS : public Symmetry {
 // Thermodynamics column <Sz^2> (calculate_TD, src/sym-SPSU2.cc:81-94).
 class SymmetrySPSU2 : public Symmetry {
  public:
-  // One channel: the closed forms below; two channels: the tables derived by
-  // QSCoupling in its SPSU2 mode (16 combinations of coefnew/spsu2/
-  // spsu2-2ch-In2.dat), checked against the reference's by the tests.
+  // One channel: the closed forms below; two and three channels: the tables
+  // derived by QSCoupling in its SPSU2 mode (the 16 or 64 combinations of
+  // coefnew/spsu2/spsu2-<P>ch-In2.dat), checked against the reference's by
+  // the tests.
   explicit SymmetrySPSU2(int channels = 1) {
-    if (channels == 2) {
-      cpl_.reset(new QSCoupling(2, true));
+    if (channels == 2 || channels == 3) {
+      cpl_.reset(new QSCoupling(channels, true));
       in_ = cpl_->In();
       qn_ = cpl_->QN();
       return;
     }
-    if (channels != 1) throw std::runtime_error("SPSU2 symmetry: this build provides the 1- and 2-channel tables");
+    if (channels != 1) throw std::runtime_error("SPSU2 symmetry: this build provides the 1-, 2- and 3-channel tables");
     in_ = {{0, 0}, {0, 0}, {0, -1}, {0, 1}};
     qn_ = {{0, 1}, {0, 1}, {0, 2}, {0, 2}};
   }

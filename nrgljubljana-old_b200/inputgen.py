@@ -709,7 +709,7 @@ def decompose_spsu2(m: ClusterModel, tol: float = 1e-9) -> List[Subspace]:
 def write_data_spsu2(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: int,
                      xi: np.ndarray, zeta: np.ndarray, delta: np.ndarray, kappa: np.ndarray,
                      discretization: str = "Y") -> dict:
-    """Write a version-9 `data` file of the SPSU2 symmetry (one or two
+    """Write a version-9 `data` file of the SPSU2 symmetry (one to three
     channels): subspaces labelled by SS alone, reduced matrix elements
     <SS1||a^dag||SS2> of f_0 of each channel and of the doublet operators for
     |SS1 - SS2| = 1 in the Wigner-Eckart normalisation of QS
@@ -718,8 +718,8 @@ def write_data_spsu2(path: str, m: ClusterModel, Lambda: float, z: float, Nmax: 
     hopping; src/nrg.cc:3383-3386), each the same for every channel or given
     per channel (one row per channel)."""
     nch = len(m.f_orbitals)
-    if nch not in (1, 2):
-        raise ValueError("SPSU2 data: one or two channels")
+    if nch not in (1, 2, 3):
+        raise ValueError("SPSU2 data: one to three channels")
     F = m.fock
     subs = decompose_spsu2(m)
     smap = {s.SS: s for s in subs}

@@ -1,6 +1,6 @@
 """SPSU2 coefficient tables (spin SU(2), charge not conserved) derived from
 spin coupling: the oracle's restatement of coefnew/spsu2/spsu2-<P>ch-*.dat
-for P = 1, 2 channels (src/sym-SPSU2.cc, src/nrg-recalc-SPSU2.cc).
+for P = 1, 2, 3 channels (src/sym-SPSU2.cc, src/nrg-recalc-SPSU2.cc).
 
 Test infrastructure: part of the CPU checker for the CUDA path, imported only
 by tests.
@@ -16,9 +16,11 @@ one channel:
   3: site singly occ.  (s = 1/2), ancestor SS - 1
   4: site singly occ.  (s = 1/2), ancestor SS + 1
 
-and for two channels the five singlets, the four doublets (two ancestors
-each) and the triplet (three ancestors) of the 16-state site, in the
-reference's order (COMBOS).  Because the charge is not conserved, three kinds
+for two channels the five singlets, the four doublets (two ancestors each)
+and the triplet (three ancestors) of the 16-state site, and for three
+channels the 64 combinations of the 64-state site, in the reference's order
+(COMBOS; the two spin-1/2 multiplets with one electron per channel are those
+of qs_derive.py, told apart by a label).  Because the charge is not conserved, three kinds
 of coupling between the chain's last site N and the added site N+1 enter
 the Hamiltonian, per channel:
 
@@ -27,11 +29,11 @@ the Hamiltonian, per channel:
                       - f^dag_{N,dn} f^dag_{N+1,up} + h.c.)    (ANOMALOUS)
   on-site   delta_{N+1} (f^dag_{N+1,up} f^dag_{N+1,dn} + h.c.)  (ISOSPINX)
 
-The reference's input generator writes the on-site pairing of every channel
-after the first with the opposite sign along the chain (initial.m, the
-"sign for isospin is inverted for f_1" of its bcsgap section), and its
-ISOSPINX tables for those channels carry the opposite sign to match; the
-tables here follow that convention.
+The reference's input generator writes the on-site pairing of the odd
+channels with the opposite sign along the chain (initial.m, the "sign for
+isospin is inverted for f_1" of its bcsgap section), and its ISOSPINX tables
+for those channels carry the opposite sign to match (channels 1 of two, and
+1 but not 2 of three); the tables here follow that convention.
 
 Each table entry is a matrix element in the site's Fock space times a
 Clebsch-Gordan recoupling, divided by the coefficient of the Wigner-Eckart
@@ -52,6 +54,30 @@ COMBOS = {
         ((2, 2), 0.0, (0, 0)), ((0, 1), 0.5, (0, -1)), ((0, 1), 0.5, (0, 1)), ((1, 0), 0.5, (0, -1)),
         ((1, 0), 0.5, (0, 1)), ((1, 2), 0.5, (0, -1)), ((1, 2), 0.5, (0, 1)), ((2, 1), 0.5, (0, -1)),
         ((2, 1), 0.5, (0, 1)), ((1, 1), 1.0, (0, -2)), ((1, 1), 1.0, (0, 0)), ((1, 1), 1.0, (0, 2))],
+    3: [
+        ((0, 0, 0), 0.0, (0, 0)), ((0, 0, 2), 0.0, (0, 0)), ((0, 1, 1), 0.0, (0, 0)),
+        ((1, 0, 1), 0.0, (0, 0)), ((0, 2, 0), 0.0, (0, 0)), ((1, 1, 0), 0.0, (0, 0)),
+        ((2, 0, 0), 0.0, (0, 0)), ((0, 2, 2), 0.0, (0, 0)), ((1, 1, 2), 0.0, (0, 0)),
+        ((2, 0, 2), 0.0, (0, 0)), ((1, 2, 1), 0.0, (0, 0)), ((2, 1, 1), 0.0, (0, 0)),
+        ((2, 2, 0), 0.0, (0, 0)), ((2, 2, 2), 0.0, (0, 0)), ((0, 0, 1), 0.5, (0, -1)),
+        ((0, 0, 1), 0.5, (0, 1)), ((0, 1, 0), 0.5, (0, -1)), ((0, 1, 0), 0.5, (0, 1)),
+        ((1, 0, 0), 0.5, (0, -1)), ((1, 0, 0), 0.5, (0, 1)), ((0, 1, 2), 0.5, (0, -1)),
+        ((0, 1, 2), 0.5, (0, 1)), ((1, 0, 2), 0.5, (0, -1)), ((1, 0, 2), 0.5, (0, 1)),
+        ((0, 2, 1), 0.5, (0, -1)), ((0, 2, 1), 0.5, (0, 1)), ((1, 1, 1), 0.5, (0, -1)),
+        ((1, 1, 1), 0.5, (0, 1)), ((2, 0, 1), 0.5, (0, -1)), ((2, 0, 1), 0.5, (0, 1)),
+        ((1, 1, 1), 0.5, (0, -1), 1), ((1, 1, 1), 0.5, (0, 1), 1), ((1, 2, 0), 0.5, (0, -1)),
+        ((1, 2, 0), 0.5, (0, 1)), ((2, 1, 0), 0.5, (0, -1)), ((2, 1, 0), 0.5, (0, 1)),
+        ((1, 2, 2), 0.5, (0, -1)), ((1, 2, 2), 0.5, (0, 1)), ((2, 1, 2), 0.5, (0, -1)),
+        ((2, 1, 2), 0.5, (0, 1)), ((2, 2, 1), 0.5, (0, -1)), ((2, 2, 1), 0.5, (0, 1)),
+        ((0, 1, 1), 1.0, (0, -2)), ((0, 1, 1), 1.0, (0, 0)), ((0, 1, 1), 1.0, (0, 2)),
+        ((1, 0, 1), 1.0, (0, -2)), ((1, 0, 1), 1.0, (0, 0)), ((1, 0, 1), 1.0, (0, 2)),
+        ((1, 1, 0), 1.0, (0, -2)), ((1, 1, 0), 1.0, (0, 0)), ((1, 1, 0), 1.0, (0, 2)),
+        ((1, 1, 2), 1.0, (0, -2)), ((1, 1, 2), 1.0, (0, 0)), ((1, 1, 2), 1.0, (0, 2)),
+        ((1, 2, 1), 1.0, (0, -2)), ((1, 2, 1), 1.0, (0, 0)), ((1, 2, 1), 1.0, (0, 2)),
+        ((2, 1, 1), 1.0, (0, -2)), ((2, 1, 1), 1.0, (0, 0)), ((2, 1, 1), 1.0, (0, 2)),
+        ((1, 1, 1), 1.5, (0, -3)), ((1, 1, 1), 1.5, (0, -1)), ((1, 1, 1), 1.5, (0, 1)),
+        ((1, 1, 1), 1.5, (0, 3)),
+    ],
 }
 # phases of the site multiplets (those of QS: qs_derive.SITE_SIGNS)
 SITE_SIGNS = qd.SITE_SIGNS
@@ -59,21 +85,26 @@ SITE_SIGNS = qd.SITE_SIGNS
 
 def iso_sign(ch):
     """The reference's sign of the on-site pairing table of channel ch."""
-    return 1.0 if ch == 0 else -1.0
+    return 1.0 if ch % 2 == 0 else -1.0
 
 
 class Tables(qd.Tables):
     def __init__(self, P=1):
         if P not in COMBOS:
-            raise NotImplementedError("SPSU2 tables are derived for 1 and 2 channels")
+            raise NotImplementedError("SPSU2 tables are derived for 1, 2 and 3 channels")
         self.P = P
         self.combos = COMBOS[P]
         self.site = qd._Site(P)
         self.mult = {}
         for c in self.combos:
             k = qd._key(c)
-            if k not in self.mult:
-                self.mult[k] = self.site.multiplet(c[0], c[1], SITE_SIGNS[P].get(k[:2], 1.0))
+            if k in self.mult:
+                continue
+            sign = SITE_SIGNS[P].get(k if P == 3 else k[:2], 1.0)
+            if P == 3 and c[0] == (1, 1, 1) and c[1] == 0.5:
+                self.mult[k] = self.site.coupled_doublet(float(k[2]), sign)
+            else:
+                self.mult[k] = self.site.multiplet(c[0], c[1], sign)
 
     def _pairs(self, ss, site_ops):
         """Ordered pairs (i, j) and channels with sum over (c, op, q) of

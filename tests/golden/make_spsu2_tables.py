@@ -22,11 +22,12 @@ from make_qs_tables import _eval, _split_args  # noqa: E402
 FILES = ["offdiag", "anomalous", "isospinx", "diag", "spinupa", "spindowna", "doubletp", "doubletm",
          "triplets", "tripletp", "tripletm", "singlet", "In2", "QN"]
 FILES_2CH = FILES + ["spinupb", "spindownb"]
+FILES_3CH = FILES_2CH + ["spinupc", "spindownc"]
 
 
-def main(refroot, out, channels=1, files=FILES):
+def main(refroot, out, channels=1, files=FILES, ss_max=40):
     base = os.path.join(refroot, "coefnew", "spsu2")
-    result = {"ss_range": [1, 40], "tables": {}}
+    result = {"ss_range": [1, ss_max], "tables": {}}
     for name in files:
         rows = []
         with open(os.path.join(base, "spsu2-%dch-%s.dat" % (channels, name))) as fh:
@@ -40,7 +41,7 @@ def main(refroot, out, channels=1, files=FILES):
                     continue
                 if name in ("offdiag", "anomalous", "isospinx"):
                     args = _split_args(line[line.index("(") + 1:line.rindex(")")])
-                    vals = {ss: _eval(args[3], ss=ss) for ss in range(1, 41)}
+                    vals = {ss: _eval(args[3], ss=ss) for ss in range(1, ss_max + 1)}
                     rows.append({"i": int(args[0]), "j": int(args[1]), "ch": int(args[2]), "factor": vals})
                     continue
                 if name == "diag":
@@ -49,10 +50,10 @@ def main(refroot, out, channels=1, files=FILES):
                     continue
                 args = _split_args(line[line.index("{") + 1:line.rindex("}")])
                 if name.startswith("spinup") or name.startswith("spindown"):
-                    vals = {ss: _eval(args[2], ssp=ss) for ss in range(1, 41)}
+                    vals = {ss: _eval(args[2], ssp=ss) for ss in range(1, ss_max + 1)}
                     rows.append({"i1": int(args[0]), "ip": int(args[1]), "factor": vals})
                 else:
-                    vals = {ss: _eval(args[4], ss1=ss) for ss in range(1, 41)}
+                    vals = {ss: _eval(args[4], ss1=ss) for ss in range(1, ss_max + 1)}
                     rows.append({"i1": int(args[0]), "ip": int(args[1]),
                                  "IN1_at_ss10": list(_eval(args[2], ss1=10)),
                                  "INp_at_ss10": list(_eval(args[3], ss1=10)), "factor": vals})
@@ -66,3 +67,4 @@ if __name__ == "__main__":
     here = os.path.dirname(os.path.abspath(__file__))
     main(ref, os.path.join(here, "spsu2_tables.json"))
     main(ref, os.path.join(here, "spsu2_tables_2ch.json"), channels=2, files=FILES_2CH)
+    main(ref, os.path.join(here, "spsu2_tables_3ch.json"), channels=3, files=FILES_3CH, ss_max=12)

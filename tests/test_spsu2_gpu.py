@@ -182,3 +182,49 @@ def test_spsu2_two_channels_matches_qs(tmp_path):
         wmax = max(abs(v) for v in dq.values())
         err = max(abs(dq.get(k, 0.0) - ds.get(k, 0.0)) for k in set(dq) | set(ds))
         assert err <= 1e-8 * wmax, (fname, err / wmax)
+
+
+def test_spsu2_three_channels_matches_qs(tmp_path):
+    """Three-channel Kondo model with unequal couplings (no pairing) in SPSU2
+    and in QS, both with tables derived for 64 combinations: thermodynamics,
+    energy flow and the f spectral function of every channel (doublet
+    operators) agree."""
+    import nrgb
+    params = {"keep": 100000, "keepenergy": 3.0, "keepmin": 1, "T": 1e-3, "fdm": True, "dmnrg": True,
+              "specd": "A_f0-A_f0 A_f1-A_f1 A_f2-A_f2", "bins": 30, "savebins": True, "broaden": False,
+              "dumpannotated": 100000, "prec_td": 16, "dumpprecision": 16}
+    out = {}
+    ctx = nrgb.Context(0)
+    try:
+        for sym in ("QS", "SPSU2"):
+            wd = str(tmp_path / ("in" + sym))
+            inputgen.make_kondo(wd, [0.3, 0.2, 0.1], 3.0, 5, symtype=sym, params=dict(params))
+            od = str(tmp_path / ("out" + sym))
+            os.makedirs(od)
+            ctx.run(wd, od)
+            out[sym] = od
+    finally:
+        ctx.close()
+    nq, tq = _td(os.path.join(out["QS"], "td"))
+    ns, ts = _td(os.path.join(out["SPSU2"], "td"))
+    assert tq.shape[0] == ts.shape[0]
+    for name in ("T", "<Sz^2>", "<E>", "<E^2>", "C", "F", "S"):
+        a, b = tq[:, nq.index(name)], ts[:, ns.index(name)]
+        assert np.all(np.abs(a - b) <= 1e-8 * np.abs(a) + 1e-11), (name, float(np.max(np.abs(a - b))))
+    aq = cases.read_annotated(os.path.join(out["QS"], "annotated.dat"))
+    as_ = cases.read_annotated(os.path.join(out["SPSU2"], "annotated.dat"))
+    assert len(aq) == len(as_)
+    for sq, ss in zip(aq, as_):
+        lq, ls = _levels(sq), _levels(ss)
+        assert lq.shape == ls.shape
+        assert np.max(np.abs(lq - ls)) <= 1e-9 * max(1.0, np.max(np.abs(lq)))
+    for ch in range(3):
+        for typ in ("FDM", "DMNRG"):
+            fname = "spec_%s_dens_A_f%d-A_f%d.bin" % (typ, ch, ch)
+            q = cases.read_bins(os.path.join(out["QS"], fname))
+            s = cases.read_bins(os.path.join(out["SPSU2"], fname))
+            dq, ds = dict(zip(q[:, 0], q[:, 1])), dict(zip(s[:, 0], s[:, 1]))
+            wmax = max(abs(v) for v in dq.values())
+            assert wmax > 0
+            err = max(abs(dq.get(k, 0.0) - ds.get(k, 0.0)) for k in set(dq) | set(ds))
+            assert err <= 1e-8 * wmax, (fname, err / wmax)

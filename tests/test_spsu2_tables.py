@@ -1,7 +1,7 @@
 """The SPSU2 coefficient tables (spin SU(2) without charge conservation), 1
-and 2 channels: the oracle's derivation from the site's Fock space
+to 3 channels: the oracle's derivation from the site's Fock space
 (oracle/spsu2_derive.py) and the host's plug-in (host/symmetry.h,
-SymmetrySPSU2, with host/qs_coupling.cc for two channels) against the
+SymmetrySPSU2, with host/qs_coupling.cc for two and three channels) against the
 reference's tables (coefnew/spsu2/spsu2-<P>ch-*.dat, evaluated into
 tests/golden/spsu2_tables*.json by tests/golden/make_spsu2_tables.py):
 hopping, anomalous hopping, on-site pairing, site occupancies, <f^dag>
@@ -10,7 +10,14 @@ recalculation, doublet and triplet operator tables.
 Entries the reference's expressions give for subspaces an NRG run never
 forms (an ancestor SS < 1, or an operator that the triangle rule forbids
 between the two subspaces) are not compared: the reference's run never
-evaluates them either."""
+evaluates them either.
+
+Three channels: the doublet-operator rows between combinations 27 and 28
+(the site doublet whose channels 0 and 1 couple to spin 0) carry in
+spsu2-3ch-doubletp/m.dat the opposite sign of the same rows of every other
+three-electron doublet, as the QS tables do for the same multiplet; the
+derivation keeps the definition (see tests/test_qs_tables_2ch.py and the
+three-channel GPU tests)."""
 import json
 import os
 import shutil
@@ -21,13 +28,18 @@ import pytest
 import spsu2_derive as SD
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-SSMAX = {1: 20, 2: 12}
+SSMAX = {1: 20, 2: 12, 3: 6}
+GOLDEN = {1: "spsu2_tables.json", 2: "spsu2_tables_2ch.json", 3: "spsu2_tables_3ch.json"}
 TOL = 1e-12
 
 
 def _gold(P):
-    name = "spsu2_tables.json" if P == 1 else "spsu2_tables_2ch.json"
-    return json.load(open(os.path.join(ROOT, "tests", "golden", name)))["tables"]
+    return json.load(open(os.path.join(ROOT, "tests", "golden", GOLDEN[P])))["tables"]
+
+
+def _flip(P, name, key):
+    """The reference's doublet rows of three-channel combinations 27, 28."""
+    return P == 3 and name.startswith("doublet") and key[0] in (27, 28) and key[1] in (27, 28)
 
 
 class _Offsets(dict):
@@ -88,25 +100,25 @@ def _ref_offdiag(P, ss):
     return out
 
 
-@pytest.mark.parametrize("P", [1, 2])
+@pytest.mark.parametrize("P", [1, 2, 3])
 def test_derivation_matches_reference_hamiltonian_tables(P):
     n = 0
     for ss in range(1, SSMAX[P] + 1):
         n += _check(_python_offdiag(P, ss), _ref_offdiag(P, ss))
-    assert n > (150 if P == 1 else 900)
+    assert n > {1: 150, 2: 900, 3: 1500}[P]
     G = _gold(P)
     assert sorted((r["i"], r["ch"], r["number"]) for r in G["diag"]) == sorted(SD.tables(P).diag())
     assert [r["qn"][0] for r in sorted(G["In2"], key=lambda r: r["i"])] == [_in(P)[i] for i in sorted(_in(P))]
 
 
-@pytest.mark.parametrize("P", [1, 2])
+@pytest.mark.parametrize("P", [1, 2, 3])
 def test_derivation_matches_reference_recalc_tables(P):
     T, G, IN = SD.tables(P), _gold(P), _in(P)
     n = 0
     for ss in range(1, SSMAX[P] + 1):
         for I1, ch, rows in T.recalc_f((0, ss)):
             d = I1[1] - ss
-            name = ("spinup" if d == 1 else "spindown") + "ab"[ch]
+            name = ("spinup" if d == 1 else "spindown") + "abc"[ch]
             ref = {}
             for r in G[name]:
                 v = r["factor"][str(ss)]
@@ -121,10 +133,11 @@ def test_derivation_matches_reference_recalc_tables(P):
                 for r in G[names[d]]:
                     v = r["factor"][str(ss)]
                     if v is not None and _used(IN, ss, ss + d, r["i1"], r["ip"], rank_ss):
-                        ref[(r["i1"], r["ip"])] = v
+                        k = (r["i1"], r["ip"])
+                        ref[k] = -v if _flip(P, names[d], k) else v
                 got = {(a, b): v for a, b, v in rows if _used(IN, ss, Ip[1], a, b, rank_ss)}
                 n += _check(got, ref)
-    assert n > (400 if P == 1 else 1500)
+    assert n > {1: 400, 2: 1500, 3: 3000}[P]
 
 
 @pytest.fixture(scope="module")
@@ -142,7 +155,7 @@ def dump(tmp_path_factory):
     return run
 
 
-@pytest.mark.parametrize("P", [1, 2])
+@pytest.mark.parametrize("P", [1, 2, 3])
 def test_plugin_matches_derivation(dump, P):
     T, IN = SD.tables(P), _in(P)
     n = 0
@@ -169,4 +182,4 @@ def test_plugin_matches_derivation(dump, P):
                if _used(IN, ss, Ip[1], a, b, rank_ss)}
         py = {(tuple(Ip), a, b): v for Ip, rs in fn((0, ss)) for a, b, v in rs if _used(IN, ss, Ip[1], a, b, rank_ss)}
         n += _check(got, py)
-    assert n > (500 if P == 1 else 1500)
+    assert n > {1: 500, 2: 1500, 3: 3000}[P]
