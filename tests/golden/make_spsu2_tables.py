@@ -1,5 +1,6 @@
-"""Generate tests/golden/spsu2_tables.json and spsu2_tables_2ch.json from the
-reference's 1- and 2-channel SPSU2 coefficient tables
+"""Generate tests/golden/spsu2_tables.json, spsu2_tables_2ch.json and
+spsu2_tables_3ch.json (SS up to 12) from the reference's 1-, 2- and
+3-channel SPSU2 coefficient tables
 (coefnew/spsu2/spsu2-<P>ch-*.dat, included by src/sym-SPSU2.cc:35-58 and
 :120-138 and src/nrg-recalc-SPSU2.cc), evaluated numerically for a range of
 spin multiplicities.  Run in a container that has
