@@ -8,11 +8,12 @@ the QSZ energy flow must be the QS one with each level repeated over its
 spin projections, and each spin component of the QSZ spectral function
 (spec_*_dens_A_d-A_d-u / -d, DM-NRG and FDM) must equal the QS one.
 
-Three channels (no QS tables to compare with): with every state kept, the
-levels and (Q, SSZ) labels of the initial cluster and of step 0 equal the
-exact diagonalisation of the impurity spin and two sites of each channel;
-under truncation, the channel-symmetric model gives the same spectral
-function for the f operator of every channel and both spins."""
+Three channels: with every state kept, the levels and (Q, SSZ) labels of
+the initial cluster and of step 0 equal the exact diagonalisation of the
+impurity spin and two sites of each channel; under truncation, the
+channel-symmetric model gives the same spectral function for the f operator
+of every channel and both spins, and the model with unequal couplings agrees
+with the three-channel QS run."""
 import collections
 import os
 
