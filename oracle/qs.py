@@ -17,16 +17,18 @@ import math
 
 import qs_derive
 
-COMBS = {1: 4, 2: 16}
+COMBS = {1: 4, 2: 16, 3: 64}
 
 # In[i]: quantum-number difference between a subspace and its i-th ancestor
 # (ancestor = I + In[i]); QN[i]: quantum numbers of the states added on the
-# new site (coefnew/qs/qs-1ch-In2.dat, qs-1ch-QN.dat; for two channels the
-# combinations of qs_derive.COMBOS, which follow qs-2ch-In2.dat, qs-2ch-QN.dat).
-IN = {1: [(1, 0), (0, -1), (0, 1), (-1, 0)],
-      2: [c[2] for c in qs_derive.COMBOS[2]]}
-QN = {1: [(-1, 1), (0, 2), (0, 2), (1, 1)],
-      2: [(sum(c[0]) - 2, int(round(2 * c[1])) + 1) for c in qs_derive.COMBOS[2]]}
+# new site (coefnew/qs/qs-1ch-In2.dat, qs-1ch-QN.dat; for two and three
+# channels the combinations of qs_derive.COMBOS, which follow
+# qs-<P>ch-In2.dat, qs-<P>ch-QN.dat).
+IN = {1: [(1, 0), (0, -1), (0, 1), (-1, 0)]}
+QN = {1: [(-1, 1), (0, 2), (0, 2), (1, 1)]}
+for _P in (2, 3):
+    IN[_P] = [c[2] for c in qs_derive.COMBOS[_P]]
+    QN[_P] = [(sum(c[0]) - _P, int(round(2 * c[1])) + 1) for c in qs_derive.COMBOS[_P]]
 
 SINGLET = (0, 1)   # InvarSinglet
 DOUBLET = (1, 2)   # Invar_f: quantum numbers of f^dag
@@ -61,11 +63,12 @@ def inverse(A):
 def offdiag_terms(nch, ss):
     """Hopping blocks of H_{N+1} in subspace with multiplicity ss:
     (i, j, ch, factor) adds factor*xi_N/SCALE(N+1) * <In[i]||f^dag_ch||In[j]>
-    to block (i, j) (qs-1ch-offdiag.dat; two channels: derived, qs_derive)."""
-    if nch == 2:
-        return qs_derive.offdiag(2, ss)
+    to block (i, j) (qs-1ch-offdiag.dat; two and three channels: derived,
+    qs_derive)."""
+    if nch in (2, 3):
+        return qs_derive.offdiag(nch, ss)
     if nch != 1:
-        raise NotImplementedError("QS tables for 1 and 2 channels")
+        raise NotImplementedError("QS tables for 1 to 3 channels")
     return [(1, 2, 0, 1.0),
             (1, 3, 0, 1.0),
             (2, 4, 0, -math.sqrt((ss - 1) / ss)),
@@ -75,8 +78,8 @@ def offdiag_terms(nch, ss):
 def diag_terms(nch):
     """(i, ch, number): electrons added in channel ch by combination i
     (qs-1ch-diag.dat)."""
-    if nch == 2:
-        return qs_derive.tables(2).diag()
+    if nch in (2, 3):
+        return qs_derive.tables(nch).diag()
     if nch != 1:
         raise NotImplementedError
     return [(1, 0, 0), (2, 0, 1), (3, 0, 1), (4, 0, 2)]
@@ -85,8 +88,8 @@ def diag_terms(nch):
 def recalc_f_tables(nch, Ip):
     """<I1||f^dag_ch||Ip> of the new site: list of (I1, ch, [(i1, ip, factor)])
     (qs-1ch-spinupa.dat, qs-1ch-spindowna.dat; src/nrg-recalc-QS.cc:210-458)."""
-    if nch == 2:
-        return qs_derive.recalc_f(2, tuple(Ip))
+    if nch in (2, 3):
+        return qs_derive.recalc_f(nch, tuple(Ip))
     if nch != 1:
         raise NotImplementedError
     qp, ssp = Ip
@@ -102,8 +105,8 @@ def recalc_f_tables(nch, Ip):
 def doublet_tables(nch, I1):
     """Recalculation of a doublet operator: list of (Ip, [(i1, ip, factor)])
     (qs-1ch-doubletp.dat, qs-1ch-doubletm.dat; src/nrg-recalc-QS.cc:34-203)."""
-    if nch == 2:
-        return qs_derive.doublet(2, tuple(I1))
+    if nch in (2, 3):
+        return qs_derive.doublet(nch, tuple(I1))
     if nch != 1:
         raise NotImplementedError
     q1, ss1 = I1
@@ -118,8 +121,8 @@ def doublet_tables(nch, I1):
 def triplet_tables(nch, I1):
     """Recalculation of a triplet (spin) operator: list of (Ip, rows)
     (qs-1ch-triplets.dat, tripletp.dat, tripletm.dat; src/nrg-recalc-QS.cc:497-697)."""
-    if nch == 2:
-        return qs_derive.triplet(2, tuple(I1))
+    if nch in (2, 3):
+        return qs_derive.triplet(nch, tuple(I1))
     if nch != 1:
         raise NotImplementedError
     q1, ss1 = I1

@@ -102,3 +102,43 @@ def test_chain_operator_tables(P, ss1):
         # the operator's rank cannot connect the two spins: every block is empty
         forbidden = not (abs(ss1 - Ip[1]) <= rank <= ss1 + Ip[1] - 2)
         _compare(mine, ref, lambda k: forbidden or not (_exists(T, k[0] - 1, I1) and _exists(T, k[1] - 1, Ip)))
+
+
+def test_three_channel_doublet_row_sign_matters(tmp_path):
+    """The sign of the reference's doublet rows between three-channel
+    combinations 29 and 30 (which the derivation does not follow) is not
+    immaterial: the oracle's f spectrum of a three-channel Kondo run changes
+    when those rows take the reference's sign, while the derived sign
+    reproduces the QSZ plug-in on the GPU (tests/test_qsz_gpu.py)."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                    "nrgljubljana-old_b200"))
+    import inputgen
+    import nrg_cases as cases
+    import nrg_oracle as O
+    params = {"keep": 80, "keepenergy": 2.5, "keepmin": 1, "T": 1e-2, "fdm": True, "dmnrg": False,
+              "specd": "A_f0-A_f0", "bins": 20, "savebins": True, "broaden": False}
+    wd = str(tmp_path / "in")
+    inputgen.make_kondo(wd, [0.3, 0.2, 0.1], 3.0, 2, symtype="QS", params=params)
+    spectra = []
+    derived = QD.doublet
+    try:
+        for flip in (False, True):
+            QD.doublet.cache_clear()
+            if flip:
+                def reference_sign(P, I1, _d=derived.__wrapped__):
+                    return [(Ip, [(a, b, -v if a in (29, 30) and b in (29, 30) else v) for a, b, v in rows])
+                            for Ip, rows in _d(P, I1)]
+                QD.doublet = reference_sign
+            od = str(tmp_path / ("out%d" % flip))
+            os.makedirs(od)
+            O.Oracle(wd).run(od)
+            b = cases.read_bins(os.path.join(od, "spec_FDM_dens_A_f0-A_f0.bin"))
+            spectra.append(dict(zip(b[:, 0], b[:, 1])))
+    finally:
+        QD.doublet = derived
+        QD.doublet.cache_clear()
+    a, b = spectra
+    assert abs(sum(a.values()) - 1.0) < 1e-9 and abs(sum(b.values()) - 1.0) < 1e-9
+    wmax = max(abs(v) for v in a.values())
+    assert max(abs(a.get(k, 0.0) - b.get(k, 0.0)) for k in set(a) | set(b)) > 1e-2 * wmax
