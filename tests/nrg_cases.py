@@ -44,6 +44,13 @@ CASES = {
                      params={"keep": 300, "dmnrg": True, "fdm": True, "T": 1e-3, "spect": "SZd-SZd",
                              "specd": "A_f0-A_f0", "bins": 30, "savebins": True, "broaden": False,
                              "dumpannotated": 1, "dumpgroups": False}),
+    # three-channel Kondo model with unequal couplings (QS tables derived for
+    # 64 combinations, the oracle's and the host's derivations): spin and f
+    # spectra of channels 0 and 2, DM-NRG and FDM
+    "kondo3ch": dict(model="kondo", J=[0.3, 0.2, 0.1], Lambda=3.0, Nmax=3,
+                     params={"keep": 150, "keepenergy": 2.5, "dmnrg": True, "fdm": True, "T": 1e-2,
+                             "spect": "SZd-SZd", "specd": "A_f0-A_f0 A_f2-A_f2", "bins": 20, "savebins": True,
+                             "broaden": False, "dumpannotated": 1, "dumpgroups": False}),
     # one run of the served z-averaging workload (z = 5/8, Nmax = 40, T = 1e-6),
     # at its smallest Nkeep: FDM A(omega)
     "siam_zshift": dict(model="siam", U=0.2, eps_d=-0.1, Gamma=0.02, Lambda=2.0, Nmax=40, z=0.625,
